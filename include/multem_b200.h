@@ -1,0 +1,273 @@
+/*
+ * multem_b200 — C ABI of a B200-native multislice engine.
+ *
+ * This is the drop-in boundary for MULTEM's plain multislice loop. It replaces the reference's
+ * entry points:
+ *   - mexFunction / run_multislice           mex_files_multem/ilc_multem.cu:484-546
+ *   - read_input_multislice (field parsing)  mex_files_multem/ilc_multem.cu:38-379
+ *   - set_struct_multislice (output packing) mex_files_multem/ilc_multem.cu:382-481
+ *   - mt_run_multislice / mt_stop_multislice / mt_niter / mt_iter   gui_multem/multem.cu:28-138
+ *   - Multislice<T,dev>::set_input_data + operator()                src/tem_simulation.cuh:51-97
+ *   - the operator-level MEX entries ilc_projected_potential, ilc_transmission_function,
+ *     ilc_propagate, ilc_incident_wave (mex_files_multem/ilc_*.cu)
+ *
+ * Conventions kept identical to the reference so a thin MATLAB/Python shim maps 1:1:
+ *   - field names follow the MATLAB input class matlab_functions/+multem_input/parameters.m;
+ *   - enum codes are the reference's (src/types.cuh:137-310), e.g. simulation_type 11 = STEM,
+ *     52 = EWRS; potential_type 6 = Lobato; potential_slicing 1 = planes, 2 = dz_Proj;
+ *     pn_model 3 = frozen phonon; pn_dim 110 = x,y;
+ *   - units are the MATLAB input's: lengths in Angstrom, E_0 in keV, theta/phi and lens azimuths in
+ *     degrees, apertures and detector angles in mrad, c_30/c_50 in mm;
+ *   - 2-D arrays are column-major (MATLAB order, element (iy, ix) at ix*ny + iy);
+ *   - spec_atoms is the reference's n x 8 column-major matrix [Z x y z sigma occ region charge]
+ *     (src/atomic_data_mt.hpp:769-787); fewer columns use the reference's defaults.
+ *
+ * Every call returns an mt_status; mt_last_error() gives a message for the calling thread.
+ * Inputs are never modified. Handles are independent and may be used from different threads.
+ */
+#ifndef MULTEM_B200_H
+#define MULTEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MT_ABI_VERSION 1
+
+typedef enum mt_status {
+    MT_OK = 0,
+    MT_ERR_INVALID_ARG = 1,  /* bad or inconsistent input */
+    MT_ERR_OOM = 2,          /* device or host allocation failed */
+    MT_ERR_CUDA = 3,         /* CUDA runtime error */
+    MT_ERR_CANCELLED = 4,    /* mt_multislice_cancel() was called */
+    MT_ERR_TIMEOUT = 5,      /* a bounded device wait ran out */
+    MT_ERR_UNSUPPORTED = 6,  /* valid reference input outside what this engine implements */
+    MT_ERR_INTERNAL = 7
+} mt_status;
+
+/* Simulation types (src/types.cuh eTEM_Sim_Type). */
+enum { MT_SIM_STEM = 11, MT_SIM_ISTEM = 12, MT_SIM_CBED = 21, MT_SIM_CBEI = 22, MT_SIM_ED = 31,
+       MT_SIM_HRTEM = 32, MT_SIM_PED = 41, MT_SIM_HCTEM = 42, MT_SIM_EWFS = 51, MT_SIM_EWRS = 52,
+       MT_SIM_EELS = 61, MT_SIM_EFTEM = 62, MT_SIM_IWFS = 71, MT_SIM_IWRS = 72, MT_SIM_PPFS = 81,
+       MT_SIM_PPRS = 82, MT_SIM_TFFS = 91, MT_SIM_TFRS = 92, MT_SIM_PROPFS = 101, MT_SIM_PROPRS = 102 };
+
+/* System configuration: mirrors System_Configuration (src/types.cuh:4447-4520) and the MATLAB
+ * system_conf struct read by read_system_conf (src/matlab_mex.cuh:263-288).
+ * precision 1 = float, 2 = double; device 1 = host, 2 = device (GPU). This engine computes the
+ * multislice loop in FP32 on the GPU; precision 2 or device 1 are rejected (MT_ERR_UNSUPPORTED). */
+typedef struct mt_system_conf {
+    int precision;
+    int device;
+    int cpu_nthread;
+    int gpu_device;
+} mt_system_conf;
+
+/* Lens parameters: cond_lens_* / obj_lens_* fields of the MATLAB input
+ * (read at mex_files_multem/ilc_multem.cu:155-268; Lens<T> in src/types.cuh:2824-3296). */
+typedef struct mt_lens {
+    int m;
+    double c_10, c_12, phi_12;
+    double c_21, phi_21, c_23, phi_23;
+    double c_30, c_32, phi_32, c_34, phi_34;
+    double c_41, phi_41, c_43, phi_43, c_45, phi_45;
+    double c_50, c_52, phi_52, c_54, phi_54, c_56, phi_56;
+    double inner_aper_ang, outer_aper_ang;
+    double ti_a, ti_sigma, ti_beta;
+    int ti_npts;
+    double si_a, si_sigma, si_beta;
+    int si_rad_npts, si_azm_npts;
+    int zero_defocus_type;       /* 1 first, 2 middle, 3 last, 4 user defined */
+    double zero_defocus_plane;
+} mt_lens;
+
+/* Input: the fields of Input_Multislice that the plain multislice path reads
+ * (src/input_multislice.cuh:456-535, filled by mex_files_multem/ilc_multem.cu:38-379). */
+typedef struct mt_input_multislice {
+    int simulation_type;
+    int interaction_model;       /* 1 multislice, 2 phase object, 3 weak phase object */
+    int potential_type;          /* 6 Lobato (0-12) */
+    int operation_mode;
+    int reverse_multislice;
+
+    int pn_model;                /* 1 still atom, 2 absorptive, 3 frozen phonon */
+    int pn_coh_contrib;
+    int pn_single_conf;
+    int pn_nconf;
+    int pn_dim;                  /* 110, 111, ... */
+    int pn_seed;
+
+    const double* spec_atoms;    /* column-major spec_atoms_rows x spec_atoms_cols */
+    int spec_atoms_rows;
+    int spec_atoms_cols;
+    double spec_lx, spec_ly, spec_lz, spec_dz;
+    int spec_cryst_na, spec_cryst_nb, spec_cryst_nc;
+    double spec_cryst_a, spec_cryst_b, spec_cryst_c, spec_cryst_x0, spec_cryst_y0;
+    int spec_amorp_n;            /* amorphous layers (z_0, z_e, dz), spec_amorp_n entries each */
+    const double* spec_amorp_z_0;
+    const double* spec_amorp_z_e;
+    const double* spec_amorp_dz;
+    double spec_rot_theta;       /* degrees */
+    double spec_rot_u0[3];
+    int spec_rot_center_type;
+    double spec_rot_center_p[3];
+
+    int thick_type;              /* 1 whole specimen, 2 through thickness, 3 through slices */
+    const double* thick;
+    int n_thick;
+
+    int potential_slicing;       /* 1 planes, 2 dz_Proj */
+
+    int nx, ny;
+    int bwl;
+
+    int iw_type;                 /* 1 plane, 2 convergent, 3 user defined, 4 auto */
+    const double* iw_psi;        /* user-defined wave: interleaved (re, im), column-major ny x nx */
+    const double* iw_x;
+    const double* iw_y;
+    int n_iw_xy;
+
+    double E_0;                  /* keV */
+    double theta, phi;           /* degrees */
+
+    int illumination_model;
+    int temporal_spatial_incoh;
+
+    mt_lens cond_lens;
+    mt_lens obj_lens;
+
+    int scanning_type;           /* 1 line, 2 area */
+    int scanning_periodic;
+    int scanning_square_pxs;
+    int scanning_ns;
+    double scanning_x0, scanning_y0, scanning_xe, scanning_ye;
+
+    int detector_type;           /* 1 circular */
+    int n_detector;
+    const double* detector_inner_ang;   /* mrad */
+    const double* detector_outer_ang;   /* mrad */
+
+    int output_area_ix_0, output_area_iy_0, output_area_ix_e, output_area_iy_e;  /* 1-based */
+} mt_input_multislice;
+
+/* Output sizes, from mt_output_query(). */
+typedef struct mt_output_dims {
+    int n_thick;                 /* thicknesses reported */
+    int n_detector;              /* STEM detectors (0 otherwise) */
+    int nx, ny;                  /* output image size (scan raster for STEM, output area otherwise) */
+    int has_image_tot;           /* STEM: image_tot[ithk][idet][ny*nx] */
+    int has_image_coh;           /* STEM with pn_coh_contrib */
+    int has_m2psi_tot;           /* EW/HRTEM-like: m2psi_tot[ithk][ny*nx] */
+    int has_psi_coh;             /* EW: psi_coh[ithk][ny*nx] complex */
+    int n_x, n_y;                /* lengths of the x and y coordinate arrays: the output grid's
+                                    axes, or every scan position for a STEM area scan (as the
+                                    reference's output x/y, src/output_multislice.hpp:1207-1245) */
+} mt_output_dims;
+
+/* Output buffers, caller-owned, sized from mt_output_dims (set_struct_multislice,
+ * mex_files_multem/ilc_multem.cu:382-481). Unused pointers may be NULL. Images are double, like
+ * the MATLAB output; psi_coh is interleaved (re, im). */
+typedef struct mt_output_multislice {
+    double dx, dy;
+    double* x;                   /* n_x */
+    double* y;                   /* n_y */
+    double* thick;               /* n_thick */
+    double* image_tot;           /* n_thick * n_detector * ny * nx */
+    double* image_coh;           /* n_thick * n_detector * ny * nx */
+    double* m2psi_tot;           /* n_thick * ny * nx */
+    double* psi_coh;             /* n_thick * ny * nx * 2 */
+} mt_output_multislice;
+
+typedef struct mt_engine mt_engine;
+
+/* ---- version / errors ---- */
+int mt_abi_version(void);
+const char* mt_last_error(void);
+
+/* ---- whole simulation (ilc_multem / mt_run_multislice) ---- */
+
+/* Sizes of the output a run of `in` produces (Output_Multislice::set_input_data,
+ * src/output_multislice.hpp:415-520). Validates the input like validate_parameters
+ * (src/input_multislice.cuh:622-796). */
+mt_status mt_output_query(const mt_input_multislice* in, mt_output_dims* dims);
+
+/* One-shot run: create an engine on conf->gpu_device, run, copy results to `out`, destroy.
+ * Equivalent of mt_run_multislice (gui_multem/multem.cu:28-50) / run_multislice
+ * (mex_files_multem/ilc_multem.cu:484-518). */
+mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislice* in,
+                            mt_output_multislice* out);
+
+/* Handle-based form: set-up once (tables, specimen, buffers), run many times.
+ * mt_engine_create = Multislice::set_input_data (src/tem_simulation.cuh:51-69). */
+mt_status mt_engine_create(const mt_system_conf* conf, const mt_input_multislice* in, mt_engine** eng);
+/* Run all phonon configurations [fp_iconf_0, pn_nconf] (Multislice::operator(),
+ * src/tem_simulation.cuh:71-97) and write the output. */
+mt_status mt_engine_run(mt_engine* eng, mt_output_multislice* out);
+/* Run a subset of phonon configurations [iconf_0, iconf_e] (1-based, inclusive) and accumulate
+ * their weighted detector sums into the engine's FP64 accumulators without writing output. Used to
+ * shard configurations over GPUs; mt_engine_read_stem() then returns the partial sums. */
+mt_status mt_engine_run_confs(mt_engine* eng, int iconf_0, int iconf_e);
+/* Zero the engine's accumulators. */
+mt_status mt_engine_reset(mt_engine* eng);
+/* STEM: copy the FP64 accumulators image_tot[ithk][idet][ny*nx] to host memory. */
+mt_status mt_engine_read_stem(mt_engine* eng, double* image_tot, size_t n);
+/* Cancel a run in progress from another thread (mt_stop_multislice, gui_multem/multem.cu:56-75).
+ * The run returns MT_ERR_CANCELLED between launches. */
+mt_status mt_engine_cancel(mt_engine* eng);
+/* Progress counters (mt_niter / mt_iter, gui_multem/multem.cu:98-138): iterations are
+ * (configuration, probe batch) pairs. */
+mt_status mt_engine_progress(mt_engine* eng, int* iter, int* niter);
+/* Device-resident hot path for timing and sharding: run configurations [iconf_0, iconf_e] with all
+ * specimen data already on the device (displaced atoms and slicing generated by
+ * mt_engine_prepare_confs). No host<->device copies inside. */
+mt_status mt_engine_prepare_confs(mt_engine* eng, int iconf_0, int iconf_e);
+mt_status mt_engine_run_prepared(mt_engine* eng, int iconf_0, int iconf_e);
+/* Number of kernel launches the last run issued (own kernels only). */
+mt_status mt_engine_launch_count(mt_engine* eng, long long* n);
+mt_status mt_engine_destroy(mt_engine* eng);
+
+/* ---- operator-level entries (ilc_projected_potential, ilc_transmission_function,
+ *      ilc_propagate, ilc_incident_wave) ---- */
+
+/* Projected potential of slice `islice` (0-based) of phonon configuration `iconf` (1-based):
+ * V[ny*nx] column-major in the reference's stored layout, which is fft-shifted: pixel (iy, ix)
+ * holds the potential at ((ix - nx/2) dx, (iy - ny/2) dy) modulo the box, exactly what
+ * ilc_projected_potential returns (mex_files_multem/ilc_projected_potential.cu:134-160;
+ * Projected_Potential::operator(), src/projected_potential.cuh:127-167). */
+mt_status mt_projected_potential(const mt_system_conf* conf, const mt_input_multislice* in,
+                                 int iconf, int islice, double* V);
+/* Transmission function exp(i*sigma*V) of slice `islice`, same layout as V
+ * (ilc_transmission_function.cu:152; Transmission_Function::trans,
+ * src/transmission_function.cuh:54-85). trans: interleaved complex. */
+mt_status mt_transmission_function(const mt_system_conf* conf, const mt_input_multislice* in,
+                                   int iconf, int islice, double* trans);
+/* Propagate the user wave in->iw_psi by distance z (ilc_propagate.cu:125; Propagator::operator(),
+ * src/propagator.cuh:34-86). space 1 = real, 2 = reciprocal. psi_out: interleaved complex. */
+mt_status mt_propagate(const mt_system_conf* conf, const mt_input_multislice* in, int space,
+                       double z, double* psi_out);
+/* Incident wave at in->iw_x/iw_y (ilc_incident_wave.cu:154; Incident_Wave::operator(),
+ * src/incident_wave.cuh:44-116). space 1 = real, 2 = reciprocal. psi_out: interleaved complex. */
+mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space,
+                           double* psi_out);
+
+/* ---- specimen host logic, exposed for parity checks ---- */
+
+/* Number of atoms kept after validation and the slice count for configuration `iconf`. */
+mt_status mt_specimen_info(const mt_input_multislice* in, int iconf, int* n_atoms, int* n_slice,
+                           int* n_thick);
+/* Displaced, z-sorted atoms of configuration `iconf` (Spec::move_atoms, src/spec.hpp:85-127):
+ * Z[n], xyz[3n] as (x, y, z) triples, in the working precision of the engine (float) widened to
+ * double. */
+mt_status mt_specimen_atoms(const mt_input_multislice* in, int iconf, int* Z, double* xyz, int n);
+/* Slices of configuration `iconf` (Slicing::calculate, src/slicing.hpp:93-100):
+ * z_0, z_e, iatom_0, iatom_e, ithk per slice. */
+mt_status mt_specimen_slices(const mt_input_multislice* in, int iconf, double* z_0, double* z_e,
+                             int* iatom_0, int* iatom_e, int* ithk, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MULTEM_B200_H */

@@ -1,0 +1,199 @@
+"""MATLAB-style entry points over the C ABI (the `ilc_*` methods of multem_input.parameters,
+matlab_functions/+multem_input/parameters.m:241-305).
+
+    out = multem_b200.ilc_multem(system_conf, params)
+
+returns a dict shaped like the MATLAB output struct of ilc_multem (set_struct_multislice,
+mex_files_multem/ilc_multem.cu:382-481): dx, dy, x, y, thick and `data`, a list over thicknesses
+of {"image_tot": [image per detector]} (STEM) or {"psi_coh", "m2psi_tot"} (exit wave). Images are
+numpy arrays in MATLAB (ny, nx) orientation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .input import Parameters, SystemConf
+
+
+def _dp(a):
+    return a.ctypes.data_as(capi.P_double)
+
+
+def _conf(system_conf):
+    return (system_conf or SystemConf()).to_c()
+
+
+def output_dims(params: Parameters) -> capi.MtOutputDims:
+    lib = capi.load()
+    s, keep = params.to_c()
+    d = capi.MtOutputDims()
+    capi.check(lib.mt_output_query(C.byref(s), C.byref(d)))
+    return d
+
+
+class OutputBuffers:
+    """Host buffers for mt_output_multislice sized from mt_output_dims."""
+
+    def __init__(self, d: capi.MtOutputDims):
+        self.d = d
+        nxy = d.nx * d.ny
+        self.x = np.zeros(max(1, d.n_x))
+        self.y = np.zeros(max(1, d.n_y))
+        self.thick = np.zeros(max(1, d.n_thick))
+        self.image_tot = np.zeros(max(1, d.n_thick * d.n_detector * nxy)) if d.has_image_tot else None
+        self.m2psi_tot = np.zeros(max(1, d.n_thick * nxy)) if d.has_m2psi_tot else None
+        self.psi_coh = np.zeros(max(1, 2 * d.n_thick * nxy)) if d.has_psi_coh else None
+        o = capi.MtOutputMultislice()
+        o.x, o.y, o.thick = _dp(self.x), _dp(self.y), _dp(self.thick)
+        if self.image_tot is not None:
+            o.image_tot = _dp(self.image_tot)
+        if self.m2psi_tot is not None:
+            o.m2psi_tot = _dp(self.m2psi_tot)
+        if self.psi_coh is not None:
+            o.psi_coh = _dp(self.psi_coh)
+        self.c = o
+
+    def to_dict(self):
+        d = self.d
+        nx, ny = d.nx, d.ny
+        res = {"dx": self.c.dx, "dy": self.c.dy, "x": self.x[:d.n_x].copy(), "y": self.y[:d.n_y].copy(),
+               "thick": self.thick[:d.n_thick].copy(), "data": []}
+        for it in range(d.n_thick):
+            e = {}
+            if self.image_tot is not None:
+                imgs = self.image_tot.reshape(d.n_thick, d.n_detector, nx, ny)[it]
+                e["image_tot"] = [imgs[k].T.copy() for k in range(d.n_detector)]
+            if self.m2psi_tot is not None:
+                e["m2psi_tot"] = self.m2psi_tot.reshape(d.n_thick, nx, ny)[it].T.copy()
+            if self.psi_coh is not None:
+                r = self.psi_coh.reshape(d.n_thick, nx, ny, 2)[it]
+                e["psi_coh"] = (r[..., 0] + 1j * r[..., 1]).T.copy()
+            res["data"].append(e)
+        return res
+
+
+def ilc_multem(system_conf: SystemConf | None, params: Parameters) -> dict:
+    """Run a full simulation (mexFunction of mex_files_multem/ilc_multem.cu:520-546)."""
+    lib = capi.load()
+    d = output_dims(params)
+    buf = OutputBuffers(d)
+    s, keep = params.to_c()
+    conf = _conf(system_conf)
+    capi.check(lib.mt_multislice_run(C.byref(conf), C.byref(s), C.byref(buf.c)))
+    return buf.to_dict()
+
+
+class Engine:
+    """Handle-based engine: set-up once, run configurations, read FP64 accumulators."""
+
+    def __init__(self, params: Parameters, system_conf: SystemConf | None = None):
+        self.lib = capi.load()
+        self.params = params
+        self._s, self._keep = params.to_c()
+        conf = _conf(system_conf)
+        h = C.c_void_p()
+        capi.check(self.lib.mt_engine_create(C.byref(conf), C.byref(self._s), C.byref(h)))
+        self.h = h
+        self.dims = output_dims(params)
+
+    def close(self):
+        if self.h:
+            self.lib.mt_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self) -> dict:
+        buf = OutputBuffers(self.dims)
+        capi.check(self.lib.mt_engine_run(self.h, C.byref(buf.c)))
+        return buf.to_dict()
+
+    def reset(self):
+        capi.check(self.lib.mt_engine_reset(self.h))
+
+    def run_confs(self, c0: int, c1: int):
+        capi.check(self.lib.mt_engine_run_confs(self.h, c0, c1))
+
+    def prepare_confs(self, c0: int, c1: int):
+        capi.check(self.lib.mt_engine_prepare_confs(self.h, c0, c1))
+
+    def run_prepared(self, c0: int, c1: int):
+        capi.check(self.lib.mt_engine_run_prepared(self.h, c0, c1))
+
+    def read_stem(self) -> np.ndarray:
+        d = self.dims
+        a = np.zeros(d.n_thick * d.n_detector * d.nx * d.ny)
+        capi.check(self.lib.mt_engine_read_stem(self.h, _dp(a), a.size))
+        return a.reshape(d.n_thick, d.n_detector, d.nx, d.ny)
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        capi.check(self.lib.mt_engine_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def cancel(self):
+        capi.check(self.lib.mt_engine_cancel(self.h))
+
+    def progress(self):
+        i, n = C.c_int(), C.c_int()
+        capi.check(self.lib.mt_engine_progress(self.h, C.byref(i), C.byref(n)))
+        return i.value, n.value
+
+
+def ilc_projected_potential(system_conf, params: Parameters, iconf: int, islice: int) -> np.ndarray:
+    lib = capi.load()
+    s, keep = params.to_c()
+    V = np.zeros(params.nx * params.ny)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_projected_potential(C.byref(conf), C.byref(s), iconf, islice, _dp(V)))
+    return V.reshape(params.nx, params.ny).T
+
+
+def ilc_transmission_function(system_conf, params: Parameters, iconf: int, islice: int) -> np.ndarray:
+    lib = capi.load()
+    s, keep = params.to_c()
+    t = np.zeros(2 * params.nx * params.ny)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_transmission_function(C.byref(conf), C.byref(s), iconf, islice, _dp(t)))
+    return (t[0::2] + 1j * t[1::2]).reshape(params.nx, params.ny).T
+
+
+def ilc_incident_wave(system_conf, params: Parameters, space: int = 1) -> np.ndarray:
+    lib = capi.load()
+    s, keep = params.to_c()
+    t = np.zeros(2 * params.nx * params.ny)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_incident_wave(C.byref(conf), C.byref(s), space, _dp(t)))
+    return (t[0::2] + 1j * t[1::2]).reshape(params.nx, params.ny).T
+
+
+def specimen_atoms(params: Parameters, iconf: int):
+    """Displaced z-sorted atoms of configuration iconf (host logic, no GPU)."""
+    lib = capi.load()
+    s, keep = params.to_c()
+    na, ns, nt = C.c_int(), C.c_int(), C.c_int()
+    capi.check(lib.mt_specimen_info(C.byref(s), iconf, C.byref(na), C.byref(ns), C.byref(nt)))
+    Z = np.zeros(na.value, np.int32)
+    xyz = np.zeros(3 * na.value)
+    capi.check(lib.mt_specimen_atoms(C.byref(s), iconf, Z.ctypes.data_as(capi.P_int), _dp(xyz), na.value))
+    return Z, xyz.reshape(-1, 3)
+
+
+def specimen_slices(params: Parameters, iconf: int):
+    lib = capi.load()
+    s, keep = params.to_c()
+    na, ns, nt = C.c_int(), C.c_int(), C.c_int()
+    capi.check(lib.mt_specimen_info(C.byref(s), iconf, C.byref(na), C.byref(ns), C.byref(nt)))
+    n = ns.value
+    z0, ze = np.zeros(n), np.zeros(n)
+    i0, ie, it = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    capi.check(lib.mt_specimen_slices(C.byref(s), iconf, _dp(z0), _dp(ze), i0.ctypes.data_as(capi.P_int),
+                                      ie.ctypes.data_as(capi.P_int), it.ctypes.data_as(capi.P_int), n))
+    return {"z_0": z0, "z_e": ze, "iatom_0": i0, "iatom_e": ie, "ithk": it}

@@ -1,0 +1,250 @@
+// extern "C" entry points declared in include/multem_b200.h.
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+
+#include "common.hpp"
+#include "engine.hpp"
+#include "multem_b200.h"
+
+struct mt_engine {
+    std::unique_ptr<mtb::Engine> eng;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+mt_status guarded(F fn) {
+    try {
+        fn();
+        g_last_error.clear();
+        return MT_OK;
+    } catch (const mtb::Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return MT_ERR_OOM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return MT_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return MT_ERR_INTERNAL;
+    }
+}
+
+mt_system_conf default_conf() {
+    mt_system_conf c{};
+    c.precision = 1;
+    c.device = 2;
+    c.cpu_nthread = 1;
+    c.gpu_device = 0;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_abi_version(void) { return MT_ABI_VERSION; }
+
+const char* mt_last_error(void) { return g_last_error.c_str(); }
+
+mt_status mt_output_query(const mt_input_multislice* in, mt_output_dims* dims) {
+    return guarded([&] {
+        if (!dims) mtb::fail(MT_ERR_INVALID_ARG, "dims is NULL");
+        *dims = mtb::output_dims(mtb::build_model(in));
+    });
+}
+
+mt_status mt_engine_create(const mt_system_conf* conf, const mt_input_multislice* in, mt_engine** eng) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        *eng = nullptr;
+        mt_system_conf c = conf ? *conf : default_conf();
+        auto h = std::unique_ptr<mt_engine>(new mt_engine);
+        h->eng.reset(new mtb::Engine(&c, in));
+        *eng = h.release();
+    });
+}
+
+mt_status mt_engine_destroy(mt_engine* eng) {
+    return guarded([&] { delete eng; });
+}
+
+mt_status mt_engine_run(mt_engine* eng, mt_output_multislice* out) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        auto& e = *eng->eng;
+        e.reset();
+        e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
+        e.write_output(out);
+    });
+}
+
+mt_status mt_engine_run_confs(mt_engine* eng, int iconf_0, int iconf_e) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->run_confs(iconf_0, iconf_e);
+    });
+}
+
+mt_status mt_engine_reset(mt_engine* eng) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->reset();
+    });
+}
+
+mt_status mt_engine_read_stem(mt_engine* eng, double* image_tot, size_t n) {
+    return guarded([&] {
+        if (!eng || !image_tot) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        eng->eng->read_stem(image_tot, n);
+    });
+}
+
+mt_status mt_engine_cancel(mt_engine* eng) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->cancel();
+    });
+}
+
+mt_status mt_engine_progress(mt_engine* eng, int* iter, int* niter) {
+    return guarded([&] {
+        if (!eng || !iter || !niter) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        eng->eng->progress(iter, niter);
+    });
+}
+
+mt_status mt_engine_prepare_confs(mt_engine* eng, int iconf_0, int iconf_e) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->prepare_confs(iconf_0, iconf_e);
+    });
+}
+
+mt_status mt_engine_run_prepared(mt_engine* eng, int iconf_0, int iconf_e) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->run_prepared(iconf_0, iconf_e);
+    });
+}
+
+mt_status mt_engine_launch_count(mt_engine* eng, long long* n) {
+    return guarded([&] {
+        if (!eng || !n) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        *n = eng->eng->launches();
+    });
+}
+
+mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislice* in, mt_output_multislice* out) {
+    return guarded([&] {
+        mt_system_conf c = conf ? *conf : default_conf();
+        mtb::Engine e(&c, in);
+        e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
+        e.write_output(out);
+    });
+}
+
+mt_status mt_projected_potential(const mt_system_conf* conf, const mt_input_multislice* in, int iconf, int islice,
+                                 double* V) {
+    return guarded([&] {
+        if (!V) mtb::fail(MT_ERR_INVALID_ARG, "V is NULL");
+        mt_system_conf c = conf ? *conf : default_conf();
+        mtb::Engine e(&c, in);
+        e.projected_potential(iconf, islice, V, nullptr);
+    });
+}
+
+mt_status mt_transmission_function(const mt_system_conf* conf, const mt_input_multislice* in, int iconf, int islice,
+                                   double* trans) {
+    return guarded([&] {
+        if (!trans) mtb::fail(MT_ERR_INVALID_ARG, "trans is NULL");
+        mt_system_conf c = conf ? *conf : default_conf();
+        mtb::Engine e(&c, in);
+        e.projected_potential(iconf, islice, nullptr, trans);
+    });
+}
+
+mt_status mt_propagate(const mt_system_conf* conf, const mt_input_multislice* in, int space, double z,
+                       double* psi_out) {
+    return guarded([&] {
+        mt_system_conf c = conf ? *conf : default_conf();
+        mtb::Engine e(&c, in);
+        e.propagate(space, z, psi_out);
+    });
+}
+
+mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space, double* psi_out) {
+    return guarded([&] {
+        if (!psi_out) mtb::fail(MT_ERR_INVALID_ARG, "psi_out is NULL");
+        mt_system_conf c = conf ? *conf : default_conf();
+        mtb::Engine e(&c, in);
+        e.incident_wave(space, psi_out);
+    });
+}
+
+// Host-only parity helpers: no GPU needed.
+namespace {
+struct HostSpec {
+    mtb::Model m;
+    std::unique_ptr<mtb::Specimen> spec;
+    explicit HostSpec(const mt_input_multislice* in) : m(mtb::build_model(in)) {
+        std::vector<float> rmax(103, 0.0f);
+        for (int Zr : m.atoms_in.Z) {
+            int Z = Zr % 1000;
+            if (rmax[Z - 1] == 0.0f) rmax[Z - 1] = (float)mtb::element_head(Z, m.grid.dR_min(), m.Vrl).R_max;
+        }
+        spec.reset(new mtb::Specimen(m, rmax));
+    }
+};
+}  // namespace
+
+mt_status mt_specimen_info(const mt_input_multislice* in, int iconf, int* n_atoms, int* n_slice, int* n_thick) {
+    return guarded([&] {
+        HostSpec h(in);
+        h.spec->move_atoms(iconf);
+        if (n_atoms) *n_atoms = (int)h.spec->atoms().size();
+        if (n_slice) *n_slice = (int)h.spec->slices().size();
+        if (n_thick) *n_thick = (int)h.spec->thicks().size();
+    });
+}
+
+mt_status mt_specimen_atoms(const mt_input_multislice* in, int iconf, int* Z, double* xyz, int n) {
+    return guarded([&] {
+        HostSpec h(in);
+        h.spec->move_atoms(iconf);
+        const auto& A = h.spec->atoms();
+        if (n < (int)A.size()) mtb::fail(MT_ERR_INVALID_ARG, "buffer too small");
+        for (size_t i = 0; i < A.size(); i++) {
+            Z[i] = A.Z[i];
+            xyz[3 * i] = A.x[i];
+            xyz[3 * i + 1] = A.y[i];
+            xyz[3 * i + 2] = A.z[i];
+        }
+    });
+}
+
+mt_status mt_specimen_slices(const mt_input_multislice* in, int iconf, double* z_0, double* z_e, int* iatom_0,
+                             int* iatom_e, int* ithk, int n) {
+    return guarded([&] {
+        HostSpec h(in);
+        h.spec->move_atoms(iconf);
+        const auto& S = h.spec->slices();
+        if (n < (int)S.size()) mtb::fail(MT_ERR_INVALID_ARG, "buffer too small");
+        for (size_t i = 0; i < S.size(); i++) {
+            z_0[i] = S[i].z_0;
+            z_e[i] = S[i].z_e;
+            iatom_0[i] = S[i].iatom_0;
+            iatom_e[i] = S[i].iatom_e;
+            ithk[i] = S[i].ithk;
+        }
+    });
+}
+
+}  // extern "C"

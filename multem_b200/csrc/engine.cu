@@ -1,0 +1,607 @@
+// Multislice engine: the batched slice loop on the device.
+//
+// Control flow follows Multislice::STEM_ISTEM / EWFS_EWRS (src/tem_simulation.cuh:101-200,
+// 304-325): for every frozen-phonon configuration, displace the atoms (host), build the
+// transmission functions of all slices (device splat), then push the incident waves through the
+// slices and reduce them at every requested thickness. The reference does one probe at a time,
+// four launches per slice and a host round trip per detector and thickness; here a batch of probes
+// advances slice by slice together (two passes per slice over the whole batch, the transmission
+// function of a slice shared from L2 by all probes), and detector sums stay on the device in FP64
+// until the end of the run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "common.hpp"
+#include "engine.hpp"
+
+namespace mtb {
+
+namespace {
+
+bool is_zero_f(float a) {
+    float d = std::fabs(a);
+    return d <= 1e-5f;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return v ? std::atoi(v) : dflt;
+}
+
+}  // namespace
+
+Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
+    if (conf) {
+        if (conf->precision != 1)
+            fail(MT_ERR_UNSUPPORTED, "this engine computes in FP32 (system_conf.precision must be 1)");
+        if (conf->device != 2) fail(MT_ERR_UNSUPPORTED, "this engine runs on the GPU (system_conf.device must be 2)");
+        device_ = conf->gpu_device;
+    }
+    int ndev = 0;
+    MTB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device_ < 0 || device_ >= ndev) fail(MT_ERR_INVALID_ARG, "gpu_device out of range");
+    MTB_CUDA(cudaSetDevice(device_));
+    MTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+    m_ = build_model(in);
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    auto pow2 = [](int n) { return n >= 64 && n <= 2048 && (n & (n - 1)) == 0; };
+    if (!pow2(nx) || !pow2(ny)) fail(MT_ERR_UNSUPPORTED, "nx and ny must be powers of two in [64, 2048]");
+    if (m_.is_EW() && !m_.is_plane_wave()) fail(MT_ERR_UNSUPPORTED, "EW simulations need a plane incident wave");
+
+    gdev_.nx = nx;
+    gdev_.ny = ny;
+    gdev_.nxh = m_.grid.nxh;
+    gdev_.nyh = m_.grid.nyh;
+    gdev_.lx = m_.grid.lx;
+    gdev_.ly = m_.grid.ly;
+    gdev_.dRx = m_.grid.dRx;
+    gdev_.dRy = m_.grid.dRy;
+    gdev_.Rx_0 = m_.grid.Rx_0;
+    gdev_.Ry_0 = m_.grid.Ry_0;
+    gdev_.dgx = m_.grid.dgx;
+    gdev_.dgy = m_.grid.dgy;
+
+    build_types();
+    std::vector<float> rmax_of_Z(103, 0.0f);
+    for (size_t t = 0; t < Z_of_type_.size(); t++) rmax_of_Z[Z_of_type_[t] - 1] = R_max_f_[t];
+    spec_.reset(new Specimen(m_, rmax_of_Z));
+
+    const size_t nxy = (size_t)nx * ny;
+    const int n_thk = (int)m_.thick.size();
+    if (m_.is_STEM()) {
+        int bmax = env_int("MTB_BATCH", std::max(1, (int)((size_t)1 << 26) / (int)nxy));
+        batch_ = std::max(1, std::min(bmax, m_.n_scan()));
+        const int n_det = (int)m_.det_g_inner.size();
+        d_image_.alloc((size_t)n_thk * n_det * m_.n_scan());
+        const int tiles = col_tiles(nx, ny);
+        d_partial_.alloc((size_t)n_thk * batch_ * tiles * n_det);
+        std::vector<float2> beam(m_.n_scan());
+        std::vector<int> idx(m_.n_scan());
+        for (int i = 0; i < m_.n_scan(); i++) {
+            beam[i] = make_float2(m_.grid.exp_factor_Rx(m_.scan_x[i]), m_.grid.exp_factor_Ry(m_.scan_y[i]));
+            idx[i] = i;
+        }
+        d_beam_.upload(beam.data(), beam.size(), stream_);
+        d_scan_idx_.upload(idx.data(), idx.size(), stream_);
+        // probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
+        // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
+        // aperture's pixel count (aperture test in the kernel's float arithmetic).
+        const LensF& L = m_.cond_lens;
+        double count = 0;
+        for (int ix = 0; ix < nx; ix++) {
+            float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx + m_.gx_0();
+            for (int iy = 0; iy < ny; iy++) {
+                float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy + m_.gy_0();
+                float g2 = gx * gx + gy * gy;
+                if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
+            }
+        }
+        if (count <= 0) fail(MT_ERR_INVALID_ARG, "condenser aperture contains no Fourier pixel");
+        probe_norm_ = (float)std::sqrt(1.0 / (double)(float)count);
+        niter_ = m_.n_scan() * m_.number_conf();
+    } else {
+        batch_ = 1;
+        const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
+        d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
+        d_ew_m2_.alloc((size_t)n_thk * onxy);
+        d_tmp_.alloc(nxy);
+        niter_ = m_.number_conf();
+    }
+    d_psi_.alloc((size_t)batch_ * nxy);
+    d_trans_.alloc((size_t)spec_->slices().size() * nxy);
+    reset();
+}
+
+Engine::~Engine() {
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+}
+
+void Engine::synchronize() { MTB_CUDA(cudaStreamSynchronize(stream_)); }
+
+void Engine::reset() {
+    if (d_image_.p) MTB_CUDA(cudaMemsetAsync(d_image_.p, 0, sizeof(double) * d_image_.n, stream_));
+    if (d_ew_psi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_psi_.p, 0, sizeof(double) * d_ew_psi_.n, stream_));
+    if (d_ew_m2_.p) MTB_CUDA(cudaMemsetAsync(d_ew_m2_.p, 0, sizeof(double) * d_ew_m2_.n, stream_));
+    iter_ = 0;
+    cancel_ = false;
+    synchronize();
+}
+
+// Element spline tables for the elements present (Spec::set_input_data builds all 103,
+// src/spec.hpp:49-55; only the present ones are ever read).
+void Engine::build_types() {
+    type_of_Z_.assign(103, -1);
+    Z_of_type_.clear();
+    for (int Zr : m_.atoms_in.Z) {
+        int Z = Zr % 1000;
+        if (type_of_Z_[Z - 1] < 0) {
+            type_of_Z_[Z - 1] = (int)Z_of_type_.size();
+            Z_of_type_.push_back(Z);
+        }
+    }
+    if ((int)Z_of_type_.size() > kMaxTypes) fail(MT_ERR_UNSUPPORTED, "more than 16 elements in one specimen");
+    d_tab_.alloc((size_t)Z_of_type_.size() * 5 * m_.nR);
+    heads_.clear();
+    for (int Z : Z_of_type_) heads_.push_back(element_head(Z, m_.grid.dR_min(), m_.Vrl));
+    build_tables(Z_of_type_, heads_, m_.nR, d_tab_.p, stream_);
+    R_max_f_.resize(Z_of_type_.size());
+    for (size_t t = 0; t < Z_of_type_.size(); t++) R_max_f_[t] = (float)heads_[t].R_max;
+    d_Rmax_.upload(R_max_f_.data(), R_max_f_.size(), stream_);
+    synchronize();
+}
+
+// Fresnel propagator factors for distance dz, separable in x and y:
+// P(ix, iy) = exp(i*w*(gx^2 + gy^2))/N, w = -pi*lambda*dz (propagate, src/cgpu_fcns.cuh:1837-1845;
+// get_propagator_factor, src/input_multislice.cuh:909-912). Phases in double, stored as float.
+void Engine::prop_tables(float dz, float2* px, float2* py) const {
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const double w = (double)m_.propagator_factor(dz);
+    const double m = (double)(1.0f / (float)(nx * ny));
+    const double gx0 = m_.gx_0(), gy0 = m_.gy_0();
+    for (int ix = 0; ix < nx; ix++) {
+        double gx = (double)((float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx) - gx0;
+        double th = w * gx * gx;
+        px[ix] = make_float2((float)(m * std::cos(th)), (float)(m * std::sin(th)));
+    }
+    for (int iy = 0; iy < ny; iy++) {
+        double gy = (double)((float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy) - gy0;
+        double th = w * gy * gy;
+        py[iy] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+}
+
+ProbeDev Engine::probe_params(float c_c_10, int nz_c10) const {
+    const LensF& L = m_.cond_lens;
+    ProbeDev p{};
+    p.c_c_10 = c_c_10;
+    p.nz_c10 = nz_c10;
+    p.c_c_30 = L.c_c_30;
+    p.nz_c30 = !is_zero_f(L.c_30);
+    p.c_c_50 = L.c_c_50;
+    p.nz_c50 = !is_zero_f(L.c_50);
+    p.g2_min = L.g2_min;
+    p.g2_max = L.g2_max;
+    p.gxu = m_.gx_0();
+    p.gyu = m_.gy_0();
+    p.norm = probe_norm_;
+    p.phi_required = L.is_phi_required();
+    p.m = L.m;
+    p.c_c_12 = L.c_c_12; p.phi_12 = L.phi_12;
+    p.c_c_21 = L.c_c_21; p.phi_21 = L.phi_21;
+    p.c_c_23 = L.c_c_23; p.phi_23 = L.phi_23;
+    p.c_c_32 = L.c_c_32; p.phi_32 = L.phi_32;
+    p.c_c_34 = L.c_c_34; p.phi_34 = L.phi_34;
+    p.c_c_41 = L.c_c_41; p.phi_41 = L.phi_41;
+    p.c_c_43 = L.c_c_43; p.phi_43 = L.phi_43;
+    p.c_c_45 = L.c_c_45; p.phi_45 = L.phi_45;
+    p.c_c_52 = L.c_c_52; p.phi_52 = L.phi_52;
+    p.c_c_54 = L.c_c_54; p.phi_54 = L.phi_54;
+    p.c_c_56 = L.c_c_56; p.phi_56 = L.phi_56;
+    return p;
+}
+
+// Host part of one configuration: Spec::move_atoms, slicing, tables; uploads on the stream.
+void Engine::prepare_conf(ConfData& cd, int iconf) {
+    spec_->move_atoms(iconf);
+    const auto& A = spec_->atoms();
+    const auto& S = spec_->slices();
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    cd.iconf = iconf;
+    cd.n_slice = (int)S.size();
+    std::vector<float4> at(A.size());
+    for (size_t i = 0; i < A.size(); i++) {
+        int t = type_of_Z_[(A.Z[i] % 1000) - 1];
+        float tf;
+        std::memcpy(&tf, &t, sizeof(float));
+        at[i] = make_float4(A.x[i], A.y[i], A.occ[i], tf);
+    }
+    std::vector<int2> rg(S.size());
+    cd.slice_ithk.resize(S.size());
+    cd.last_slice = -1;
+    for (size_t k = 0; k < S.size(); k++) {
+        rg[k] = make_int2(S[k].iatom_0, S[k].iatom_e);
+        cd.slice_ithk[k] = S[k].ithk;
+        if (S[k].ithk >= 0) cd.last_slice = (int)k;
+    }
+    if (cd.last_slice < 0) fail(MT_ERR_INTERNAL, "no slice carries a thickness");
+    const auto& TH = spec_->thicks();
+    cd.thick_z_back_prop.resize(TH.size());
+    for (size_t t = 0; t < TH.size(); t++) cd.thick_z_back_prop[t] = TH[t].z_back_prop;
+    const size_t pl = (size_t)nx + ny;
+    std::vector<float2> prop((S.size() + TH.size()) * pl);
+    for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), &prop[k * pl], &prop[k * pl + nx]);
+    for (size_t t = 0; t < TH.size(); t++)
+        prop_tables(TH[t].z_back_prop, &prop[(S.size() + t) * pl], &prop[(S.size() + t) * pl + nx]);
+    // incident-wave defocus relative to the first slice (Incident_Wave::operator(),
+    // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0))
+    const float z_init = (float)(0.5 * (S[0].z_0 + S[0].z_e));
+    const float f_s = m_.cond_lens.c_10 - (m_.cond_lens.zero_defocus_plane - z_init);
+    LensF L = m_.cond_lens;
+    L.set_defocus(f_s);
+    cd.probe_c_c_10 = L.c_c_10;
+    cd.probe_nz_c10 = !is_zero_f(f_s);
+    cd.atoms.upload(at.data(), at.size(), stream_);
+    cd.ranges.upload(rg.data(), rg.size(), stream_);
+    cd.prop.upload(prop.data(), prop.size(), stream_);
+    synchronize();  // host vectors go out of scope
+}
+
+ConfData* Engine::find_conf(int iconf) {
+    for (auto& c : confs_)
+        if (c.iconf == iconf) return &c;
+    return nullptr;
+}
+
+void Engine::prepare_confs(int c0, int c1) {
+    for (int c = c0; c <= c1; c++) {
+        if (find_conf(c)) continue;
+        confs_.emplace_back();
+        prepare_conf(confs_.back(), c);
+    }
+}
+
+void Engine::check_cancel() {
+    if (cancel_) {
+        synchronize();
+        fail(MT_ERR_CANCELLED, "run cancelled");
+    }
+}
+
+void Engine::run_prepared(int c0, int c1) {
+    if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
+    long long l0 = launches_issued();
+    for (int c = c0; c <= c1; c++) {
+        ConfData* cd = find_conf(c);
+        if (!cd) fail(MT_ERR_INVALID_ARG, "configuration not prepared");
+        run_conf(*cd);
+    }
+    launches_ = launches_issued() - l0;
+}
+
+void Engine::run_confs(int c0, int c1) {
+    if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
+    long long l0 = launches_issued();
+    for (int c = c0; c <= c1; c++) {
+        ConfData cd;
+        prepare_conf(cd, c);
+        run_conf(cd);
+    }
+    launches_ = launches_issued() - l0;
+    synchronize();
+}
+
+void Engine::run_conf(ConfData& cd) {
+    // transmission functions of the slices up to the last output thickness
+    SplatArgs sa{};
+    sa.g = gdev_;
+    sa.atoms = cd.atoms.p;
+    sa.slice_range = cd.ranges.p;
+    sa.tab = d_tab_.p;
+    sa.R_max = d_Rmax_.p;
+    sa.n_types = (int)Z_of_type_.size();
+    sa.nR = m_.nR;
+    sa.w = m_.Vr_factor();
+    sa.wpo = (m_.interaction_model == 3);
+    sa.trans = d_trans_.p;
+    sa.V = nullptr;
+    launch_splat(sa, 0, cd.last_slice + 1, stream_);
+    if (m_.is_STEM()) run_stem(cd); else run_ew(cd);
+}
+
+void Engine::run_stem(ConfData& cd) {
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const size_t nxy = (size_t)nx * ny;
+    const int n_det = (int)m_.det_g_inner.size();
+    const int n_scan = m_.n_scan();
+    const int n_thk = (int)m_.thick.size();
+    const int tiles = col_tiles(nx, ny);
+    const size_t pl = (size_t)nx + ny;
+    const double w = (double)m_.phonon_weight();
+
+    ColArgs ca{};
+    ca.ny = ny;
+    ca.g = gdev_;
+    ca.probe = probe_params(cd.probe_c_c_10, cd.probe_nz_c10);
+    ca.n_det = n_det;
+    for (int d = 0; d < n_det; d++) {
+        // sum_square_over_Det bounds: g2 = pow(g, 2) stored as float (src/cpu_fcns.hpp:1168-1169)
+        ca.det_g2_min[d] = (float)std::pow((double)m_.det_g_inner[d], 2);
+        ca.det_g2_max[d] = (float)std::pow((double)m_.det_g_outer[d], 2);
+    }
+    ca.gx_0 = 0;
+    ca.gy_0 = 0;
+    RowArgs ra{};
+    ra.nx = nx;
+    ra.scale = 1.0f;
+
+    for (int p0 = 0; p0 < n_scan; p0 += batch_) {
+        const int nb = std::min(batch_, n_scan - p0);
+        ca.nprobe = nb;
+        ra.nprobe = nb;
+        // incident probes, generated in Fourier space and brought to the hybrid layout
+        ca.in = nullptr;
+        ca.out = d_psi_.p;
+        ca.beam = d_beam_.p + p0;
+        ca.Px = nullptr;
+        ca.Py = nullptr;
+        launch_cols(nx, COL_INVERSE | COL_STORE, ca, 0, stream_);
+        for (int k = 0; k <= cd.last_slice; k++) {
+            ra.in = d_psi_.p;
+            ra.out = d_psi_.p;
+            ra.trans = d_trans_.p + (size_t)k * nxy;
+            launch_rows(ny, ROW_STEP, ra, 0, stream_);
+            const int ithk = cd.slice_ithk[k];
+            int flags = COL_LOAD | COL_PROP;
+            if (ithk >= 0) flags |= COL_DETECT;
+            if (k < cd.last_slice) flags |= COL_INVERSE | COL_STORE;
+            ca.in = d_psi_.p;
+            ca.out = d_psi_.p;
+            ca.Px = cd.prop.p + (size_t)k * pl;
+            ca.Py = ca.Px + nx;
+            ca.det_partial = d_partial_.p + (size_t)(ithk >= 0 ? ithk : 0) * batch_ * tiles * n_det;
+            launch_cols(nx, flags, ca, 0, stream_);
+        }
+        for (int t = 0; t < n_thk; t++)
+            launch_det_reduce(d_partial_.p + (size_t)t * batch_ * tiles * n_det, nb, tiles, n_det, d_scan_idx_.p + p0, w,
+                              d_image_.p + (size_t)t * n_det * n_scan, n_scan, stream_);
+        iter_ += nb;
+        check_cancel();
+    }
+}
+
+void Engine::run_ew(ConfData& cd) {
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const size_t nxy = (size_t)nx * ny;
+    const size_t pl = (size_t)nx + ny;
+    const int ox = m_.out_ix_e - m_.out_ix_0, oy = m_.out_iy_e - m_.out_iy_0;
+    const size_t onxy = (size_t)ox * oy;
+    const double w = (double)m_.phonon_weight();
+    const bool sc = m_.is_EW_SC();
+
+    RowArgs ra{};
+    ra.nx = nx;
+    ra.nprobe = 1;
+    ra.scale = 1.0f;
+    ColArgs ca{};
+    ca.ny = ny;
+    ca.nprobe = 1;
+    ca.g = gdev_;
+    ca.n_det = 0;
+    for (int k = 0; k <= cd.last_slice; k++) {
+        ra.in = d_psi_.p;
+        ra.out = d_psi_.p;
+        ra.trans = d_trans_.p + (size_t)k * nxy;
+        launch_rows(ny, k == 0 ? ROW_FIRST_ONE : ROW_STEP, ra, 0, stream_);
+        ca.in = d_psi_.p;
+        ca.out = d_psi_.p;
+        ca.Px = cd.prop.p + (size_t)k * pl;
+        ca.Py = ca.Px + nx;
+        launch_cols(nx, COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca, 0, stream_);
+        const int ithk = cd.slice_ithk[k];
+        if (ithk < 0) continue;
+        // wave at this thickness (Wave_Function::get_psi, src/wave_function.cuh:96-105)
+        const float zbp = cd.thick_z_back_prop[ithk];
+        ColArgs cb = ca;
+        cb.in = d_psi_.p;
+        cb.out = d_tmp_.p;
+        cb.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
+        cb.Py = cb.Px + nx;
+        if (m_.is_EWRS()) {
+            RowArgs rb = ra;
+            if (zbp != 0.0f) {
+                launch_cols(nx, COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cb, 0, stream_);
+                rb.in = d_tmp_.p;
+                rb.scale = 1.0f;
+            } else {
+                rb.in = d_psi_.p;
+                rb.scale = 1.0f / (float)ny;
+            }
+            rb.out = d_tmp_.p;
+            launch_rows(ny, ROW_INVERSE, rb, 0, stream_);
+        } else {
+            launch_cols(nx, COL_LOAD | COL_PROP | COL_STORE, cb, 0, stream_);
+        }
+        launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
+                             d_ew_psi_.p + (size_t)ithk * onxy * 2, sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy,
+                             stream_);
+    }
+    iter_ += 1;
+    check_cancel();
+}
+
+mt_output_dims Engine::dims() const { return output_dims(m_); }
+
+// Output_Multislice::set_input_data sizes (src/output_multislice.hpp:415-520); host only.
+mt_output_dims output_dims(const Model& m_) {
+    mt_output_dims d{};
+    d.n_thick = (int)m_.thick.size();
+    if (m_.is_STEM()) {
+        d.n_detector = (int)m_.det_g_inner.size();
+        d.nx = m_.scan_nx;
+        d.ny = m_.scan_ny;
+        d.has_image_tot = 1;
+        d.n_x = (int)m_.scan_x.size();
+        d.n_y = (int)m_.scan_y.size();
+    } else {
+        d.nx = m_.out_ix_e - m_.out_ix_0;
+        d.ny = m_.out_iy_e - m_.out_iy_0;
+        d.has_psi_coh = 1;
+        d.has_m2psi_tot = m_.is_EW_SC() ? 0 : 1;
+        d.n_x = d.nx;
+        d.n_y = d.ny;
+    }
+    return d;
+}
+
+void Engine::read_stem(double* image_tot, size_t n) {
+    if (!m_.is_STEM()) fail(MT_ERR_INVALID_ARG, "not a STEM engine");
+    if (n < d_image_.n) fail(MT_ERR_INVALID_ARG, "image buffer too small");
+    MTB_CUDA(cudaMemcpyAsync(image_tot, d_image_.p, sizeof(double) * d_image_.n, cudaMemcpyDeviceToHost, stream_));
+    synchronize();
+}
+
+// Output_Multislice::set_output_grid + gather (src/output_multislice.hpp:1207-1245) and
+// set_struct_multislice (mex_files_multem/ilc_multem.cu:382-481).
+void Engine::write_output(mt_output_multislice* out) {
+    if (!out) return;
+    synchronize();
+    const mt_output_dims d = dims();
+    if (out->thick)
+        for (int i = 0; i < d.n_thick; i++) out->thick[i] = m_.thick[i];
+    if (m_.is_STEM()) {
+        out->dx = m_.scan_dRx;
+        out->dy = m_.scan_dRy;
+        if (out->x)
+            for (size_t i = 0; i < m_.scan_x.size(); i++) out->x[i] = m_.scan_x[i];
+        if (out->y)
+            for (size_t i = 0; i < m_.scan_y.size(); i++) out->y[i] = m_.scan_y[i];
+        if (out->image_tot)
+            MTB_CUDA(cudaMemcpy(out->image_tot, d_image_.p, sizeof(double) * d_image_.n, cudaMemcpyDeviceToHost));
+    } else {
+        const bool rs = m_.is_EWRS();
+        out->dx = rs ? m_.grid.dRx : m_.grid.dgx;
+        out->dy = rs ? m_.grid.dRy : m_.grid.dgy;
+        if (out->x)
+            for (int ix = m_.out_ix_0; ix < m_.out_ix_e; ix++)
+                out->x[ix - m_.out_ix_0] = rs ? m_.grid.Rx(ix) : m_.grid.gx(ix);
+        if (out->y)
+            for (int iy = m_.out_iy_0; iy < m_.out_iy_e; iy++)
+                out->y[iy - m_.out_iy_0] = rs ? m_.grid.Ry(iy) : m_.grid.gy(iy);
+        if (out->psi_coh)
+            MTB_CUDA(cudaMemcpy(out->psi_coh, d_ew_psi_.p, sizeof(double) * d_ew_psi_.n, cudaMemcpyDeviceToHost));
+        if (out->m2psi_tot && d.has_m2psi_tot)
+            MTB_CUDA(cudaMemcpy(out->m2psi_tot, d_ew_m2_.p, sizeof(double) * d_ew_m2_.n, cudaMemcpyDeviceToHost));
+    }
+}
+
+// Projected potential / transmission of one slice, reference stored layout.
+void Engine::projected_potential(int iconf, int islice, double* V, double* trans) {
+    ConfData cd;
+    prepare_conf(cd, iconf);
+    if (islice < 0 || islice >= cd.n_slice) fail(MT_ERR_INVALID_ARG, "islice out of range");
+    const size_t nxy = (size_t)m_.grid.nx * m_.grid.ny;
+    DevBuf<float> dV;
+    DevBuf<float2> dT;
+    dV.alloc(nxy);
+    dT.alloc(nxy);
+    SplatArgs sa{};
+    sa.g = gdev_;
+    sa.atoms = cd.atoms.p;
+    sa.slice_range = cd.ranges.p + islice;
+    sa.tab = d_tab_.p;
+    sa.R_max = d_Rmax_.p;
+    sa.n_types = (int)Z_of_type_.size();
+    sa.nR = m_.nR;
+    sa.w = m_.Vr_factor();
+    sa.wpo = (m_.interaction_model == 3);
+    sa.trans = dT.p;
+    sa.V = dV.p;
+    launch_splat(sa, 0, 1, stream_);
+    std::vector<float> hV(nxy);
+    std::vector<float2> hT(nxy);
+    MTB_CUDA(cudaMemcpyAsync(hV.data(), dV.p, sizeof(float) * nxy, cudaMemcpyDeviceToHost, stream_));
+    MTB_CUDA(cudaMemcpyAsync(hT.data(), dT.p, sizeof(float2) * nxy, cudaMemcpyDeviceToHost, stream_));
+    synchronize();
+    if (V)
+        for (size_t i = 0; i < nxy; i++) V[i] = hV[i];
+    if (trans)
+        for (size_t i = 0; i < nxy; i++) {
+            trans[2 * i] = hT[i].x;
+            trans[2 * i + 1] = hT[i].y;
+        }
+}
+
+// Incident_Wave::operator()(space, output) (src/incident_wave.cuh:98-116): convergent probe(s) at
+// iw_x/iw_y, defocus referred to z = 0; space 1 real, 2 reciprocal.
+void Engine::incident_wave(int space, double* psi) {
+    if (!m_.is_convergent_wave()) fail(MT_ERR_UNSUPPORTED, "incident_wave implements the convergent wave");
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const size_t nxy = (size_t)nx * ny;
+    const int nb = (int)m_.iw_x.size();
+    if (nb <= 0) fail(MT_ERR_INVALID_ARG, "iw_x/iw_y are empty");
+    // probe normalisation as in the STEM constructor
+    const LensF& L = m_.cond_lens;
+    double count = 0;
+    for (int ix = 0; ix < nx; ix++) {
+        float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx + m_.gx_0();
+        for (int iy = 0; iy < ny; iy++) {
+            float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy + m_.gy_0();
+            float g2 = gx * gx + gy * gy;
+            if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
+        }
+    }
+    probe_norm_ = (float)std::sqrt(1.0 / (double)(float)count);
+    const float f_s = m_.cond_lens.c_10 - (m_.cond_lens.zero_defocus_plane - 0.0f);
+    LensF Lp = m_.cond_lens;
+    Lp.set_defocus(f_s);
+    std::vector<float2> beam(nb);
+    for (int i = 0; i < nb; i++) beam[i] = make_float2(m_.grid.exp_factor_Rx(m_.iw_x[i]), m_.grid.exp_factor_Ry(m_.iw_y[i]));
+    DevBuf<float2> dbeam, dpsi;
+    dbeam.upload(beam.data(), nb, stream_);
+    dpsi.alloc(nxy * nb);
+    ColArgs ca{};
+    ca.ny = ny;
+    ca.nprobe = nb;
+    ca.g = gdev_;
+    ca.beam = dbeam.p;
+    ca.probe = probe_params(Lp.c_c_10, !is_zero_f(f_s));
+    ca.out = dpsi.p;
+    if (space == 2) {
+        launch_cols(nx, COL_STORE, ca, 0, stream_);
+    } else {
+        launch_cols(nx, COL_INVERSE | COL_STORE, ca, 0, stream_);
+        RowArgs ra{};
+        ra.in = dpsi.p;
+        ra.out = dpsi.p;
+        ra.nx = nx;
+        ra.nprobe = nb;
+        ra.scale = 1.0f;
+        launch_rows(ny, ROW_INVERSE, ra, 0, stream_);
+    }
+    std::vector<float2> h(nxy * nb);
+    MTB_CUDA(cudaMemcpyAsync(h.data(), dpsi.p, sizeof(float2) * h.size(), cudaMemcpyDeviceToHost, stream_));
+    synchronize();
+    for (size_t i = 0; i < nxy; i++) {
+        double re = 0, im = 0;
+        for (int b = 0; b < nb; b++) {
+            re += h[b * nxy + i].x;
+            im += h[b * nxy + i].y;
+        }
+        psi[2 * i] = re;
+        psi[2 * i + 1] = im;
+    }
+}
+
+void Engine::propagate(int, double, double*) {
+    fail(MT_ERR_UNSUPPORTED, "mt_propagate is not implemented yet");
+}
+
+}  // namespace mtb

@@ -1,0 +1,129 @@
+// Multislice engine: device state and the batched slice loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <memory>
+#include <vector>
+
+#include "host_model.hpp"
+#include "kernels.cuh"
+#include "multem_b200.h"
+#include "tables.hpp"
+
+namespace mtb {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept { std::swap(p, o.p); std::swap(n, o.n); return *this; }
+    ~DevBuf() { if (p) cudaFree(p); }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cuda_check(cudaMalloc(&p, sizeof(T) * (count ? count : 1)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) cuda_check(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
+    }
+};
+
+// Per phonon configuration: displaced atoms, slice ranges, propagator tables, probe defocus.
+struct ConfData {
+    int iconf = 0;
+    int n_slice = 0;
+    int last_slice = 0;             // last slice that carries a thickness
+    std::vector<int> slice_ithk;    // per slice
+    std::vector<float> thick_z_back_prop;
+    float probe_c_c_10 = 0;
+    int probe_nz_c10 = 0;
+    DevBuf<float4> atoms;
+    DevBuf<int2> ranges;
+    DevBuf<float2> prop;            // per slice: Px[nx] then Py[ny]
+};
+
+mt_output_dims output_dims(const Model& m);
+
+class Engine {
+  public:
+    Engine(const mt_system_conf* conf, const mt_input_multislice* in);
+    ~Engine();
+
+    const Model& model() const { return m_; }
+    Specimen& specimen() { return *spec_; }
+
+    mt_output_dims dims() const;
+    void reset();
+    void prepare_confs(int c0, int c1);      // host RNG + slicing + uploads
+    void run_prepared(int c0, int c1);       // device-only work for prepared confs
+    void run_confs(int c0, int c1);          // prepare + run
+    void write_output(mt_output_multislice* out);
+    void read_stem(double* image_tot, size_t n);
+    void cancel() { cancel_ = true; }
+    void progress(int* iter, int* niter) const { *iter = iter_; *niter = niter_; }
+    long long launches() const { return launches_; }
+    void synchronize();
+
+    // operator-level entries
+    void projected_potential(int iconf, int islice, double* V, double* trans);
+    void incident_wave(int space, double* psi);
+    void propagate(int space, double z, double* psi);
+
+    cudaStream_t stream() const { return stream_; }
+    int batch_size() const { return batch_; }
+
+  private:
+    Model m_;
+    std::unique_ptr<Specimen> spec_;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    std::atomic<bool> cancel_{false};
+    int iter_ = 0, niter_ = 0;
+    long long launches_ = 0;
+
+    // element tables
+    std::vector<int> type_of_Z_;     // Z-1 -> type index or -1
+    std::vector<int> Z_of_type_;
+    std::vector<float> R_max_f_;     // per type
+    std::vector<TableHead> heads_;
+    DevBuf<float> d_tab_;
+    DevBuf<float> d_Rmax_;
+
+    // wave state
+    int batch_ = 1;
+    DevBuf<float2> d_psi_;
+    DevBuf<float2> d_trans_;
+    DevBuf<float2> d_tmp_;
+    DevBuf<float2> d_beam_;          // all scan positions (exp factors)
+    DevBuf<int> d_scan_idx_;
+    DevBuf<double> d_partial_;
+    DevBuf<double> d_image_;         // [n_thk][n_det][n_scan]
+    DevBuf<double> d_ew_psi_;        // [n_thk][out_nxy][2]
+    DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
+    DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
+    std::vector<ConfData> confs_;
+    GridDev gdev_{};
+    float probe_norm_ = 1.0f;
+
+    void build_types();
+    void prepare_conf(ConfData& cd, int iconf);
+    void run_conf(ConfData& cd);
+    void run_stem(ConfData& cd);
+    void run_ew(ConfData& cd);
+    void prop_tables(float dz, float2* px, float2* py) const;
+    ProbeDev probe_params(float c_c_10, int nz_c10) const;
+    void check_cancel();
+    ConfData* find_conf(int iconf);
+};
+
+}  // namespace mtb

@@ -1,0 +1,320 @@
+// Register/shared-memory FFT building blocks for the multislice passes (sm_100a).
+//
+// A line of N complex points is transformed by TPL = N / E threads, each holding E points in
+// registers. The transform is a Stockham autosort FFT (Govindaraju et al., "High performance
+// discrete Fourier transforms on graphics processors", SC'08) over a compile-time list of radices:
+//
+//   stage with radix R, Ns = product of the earlier radices, butterflies j in [0, N/R):
+//     k = j % Ns;  v_r = in[j + r*N/R] * w^(r*k), w = exp(dir*2*pi*i/(Ns*R));  DFT_R(v);
+//     out[(j/Ns)*Ns*R + k + r*Ns] = v_r
+//
+// Thread t owns butterflies j = t + TPL*m (m in [0, E/R)) and keeps v in x[m*R + r]. Points move
+// between stages through a padded shared-memory line buffer. The first stage reads positions
+// j + r*N/R and the last stage produces positions j + r*N/R_last, so
+//   * the first stage can load straight from global memory (coalesced over t), and
+//   * an inverse transform with radices (R1..Rs) followed by a forward transform with radices
+//     (Rs..R1) needs no exchange between them: the inverse's outputs already sit in the registers
+//     the forward's first stage reads. The pointwise multiply between them (transmission
+//     function or Fresnel propagator) is applied there, in natural order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <type_traits>
+#include <utility>
+
+namespace mtb {
+
+// ---------------------------------------------------------------------------------------------
+// compile-time helpers
+
+template <int I>
+using ic = std::integral_constant<int, I>;
+
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (I < N) {
+        f(ic<I>{});
+        static_for<I + 1, N>(f);
+    }
+}
+
+// cos/sin(2*pi*k/n) at compile time: octant reduction + Taylor series on [0, pi/4].
+constexpr double cx_pi = 3.141592653589793238462643383279502884;
+
+constexpr double cx_sin_series(double x) {
+    double x2 = x * x, term = x, sum = x;
+    for (int n = 1; n < 14; ++n) {
+        term *= -x2 / ((2.0 * n) * (2.0 * n + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+
+constexpr double cx_cos_series(double x) {
+    double x2 = x * x, term = 1.0, sum = 1.0;
+    for (int n = 1; n < 14; ++n) {
+        term *= -x2 / ((2.0 * n - 1.0) * (2.0 * n));
+        sum += term;
+    }
+    return sum;
+}
+
+// returns cos (c=true) or sin (c=false) of 2*pi*k/n
+constexpr double cx_trig2pi(long long k, long long n, bool c) {
+    long long m = ((k % n) + n) % n;
+    long long o = (8 * m) / n;                 // octant
+    long long rem = 8 * m - o * n;             // angle within octant = (pi/4) * rem / n
+    double th = (cx_pi / 4.0) * (double)rem / (double)n;
+    double cth = (cx_pi / 4.0) * (double)(n - rem) / (double)n;  // pi/4 - th
+    double cs = 0, sn = 0;
+    switch (o) {
+        case 0: cs = cx_cos_series(th); sn = cx_sin_series(th); break;
+        case 1: cs = cx_sin_series(cth); sn = cx_cos_series(cth); break;
+        case 2: cs = -cx_sin_series(th); sn = cx_cos_series(th); break;
+        case 3: cs = -cx_cos_series(cth); sn = cx_sin_series(cth); break;
+        case 4: cs = -cx_cos_series(th); sn = -cx_sin_series(th); break;
+        case 5: cs = -cx_sin_series(cth); sn = -cx_cos_series(cth); break;
+        case 6: cs = cx_sin_series(th); sn = -cx_cos_series(th); break;
+        default: cs = cx_cos_series(cth); sn = -cx_sin_series(cth); break;
+    }
+    return c ? cs : sn;
+}
+
+// ---------------------------------------------------------------------------------------------
+// complex helpers (float2 = (re, im))
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// multiply by exp(DIR * 2*pi*i * K / R), K and R compile-time
+template <int K, int R, int DIR>
+__device__ __forceinline__ float2 twiddle_const(float2 v) {
+    constexpr int k = ((K % R) + R) % R;
+    if constexpr (k == 0) {
+        return v;
+    } else if constexpr (4 * k == R) {          // exp(DIR*i*pi/2) = DIR*i
+        return DIR > 0 ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+    } else if constexpr (2 * k == R) {          // -1
+        return make_float2(-v.x, -v.y);
+    } else if constexpr (4 * k == 3 * R) {      // exp(DIR*i*3pi/2) = -DIR*i
+        return DIR > 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+    } else if constexpr (8 * k == R || 8 * k == 3 * R || 8 * k == 5 * R || 8 * k == 7 * R) {
+        constexpr float h = 0.70710678118654752440f;
+        constexpr float c = (8 * k == R || 8 * k == 7 * R) ? h : -h;
+        constexpr float s = (float)(DIR * ((8 * k == R || 8 * k == 3 * R) ? 1 : -1)) * h;
+        return make_float2((v.x * c - v.y * s), (v.x * s + v.y * c));
+    } else {
+        constexpr float c = (float)cx_trig2pi(k, R, true);
+        constexpr float s = (float)(DIR * cx_trig2pi(k, R, false));
+        return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+    }
+}
+
+// In-register DFT of length R (natural order in and out), dir = -1 forward, +1 inverse,
+// unnormalised. Radix-4 / radix-2 decimation in time, fully unrolled; trivial twiddles folded.
+template <int R, int DIR>
+__device__ __forceinline__ void dft(float2* v) {
+    if constexpr (R == 1) {
+    } else if constexpr (R == 2) {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        float2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
+        float2 jt3 = twiddle_const<1, 4, DIR>(t3);
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, jt3);
+        v[3] = csub(t1, jt3);
+    } else if constexpr (R % 4 == 0) {
+        // radix-4 DIT: four interleaved sub-DFTs of length R/4
+        constexpr int Q = R / 4;
+        float2 a[Q], b[Q], c[Q], d[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            a[i] = v[4 * i];
+            b[i] = v[4 * i + 1];
+            c[i] = v[4 * i + 2];
+            d[i] = v[4 * i + 3];
+        }
+        dft<Q, DIR>(a);
+        dft<Q, DIR>(b);
+        dft<Q, DIR>(c);
+        dft<Q, DIR>(d);
+        static_for<0, Q>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            float2 bb = twiddle_const<k, R, DIR>(b[k]);
+            float2 cc = twiddle_const<2 * k, R, DIR>(c[k]);
+            float2 dd = twiddle_const<3 * k, R, DIR>(d[k]);
+            float2 s0 = cadd(a[k], cc), s1 = csub(a[k], cc);
+            float2 s2 = cadd(bb, dd), s3 = twiddle_const<1, 4, DIR>(csub(bb, dd));
+            v[k] = cadd(s0, s2);
+            v[k + 2 * Q] = csub(s0, s2);
+            v[k + Q] = cadd(s1, s3);
+            v[k + 3 * Q] = csub(s1, s3);
+        });
+    } else {
+        constexpr int H = R / 2;
+        float2 e[H], o[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            e[i] = v[2 * i];
+            o[i] = v[2 * i + 1];
+        }
+        dft<H, DIR>(e);
+        dft<H, DIR>(o);
+        static_for<0, H>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            float2 t = twiddle_const<k, R, DIR>(o[k]);
+            v[k] = cadd(e[k], t);
+            v[k + H] = csub(e[k], t);
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Line plans: N points, E points per thread, radices of the forward transform in stage order.
+// The inverse uses the same radices reversed (see the header comment).
+
+template <int N>
+struct LinePlan;
+
+template <> struct LinePlan<64>   { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 4, 1}; };
+template <> struct LinePlan<128>  { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 8, 1}; };
+template <> struct LinePlan<256>  { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 16, 1}; };
+template <> struct LinePlan<512>  { static constexpr int E = 32; static constexpr int NS = 2; static constexpr int R[3] = {32, 16, 1}; };
+template <> struct LinePlan<1024> { static constexpr int E = 32; static constexpr int NS = 2; static constexpr int R[3] = {32, 32, 1}; };
+template <> struct LinePlan<2048> { static constexpr int E = 32; static constexpr int NS = 3; static constexpr int R[3] = {32, 8, 8}; };
+
+// Radix of stage s of a transform whose stage order is `rev` ? reversed : plan order.
+template <int N, bool REV, int S>
+struct StageRadix {
+    static constexpr int NSTAGE = LinePlan<N>::NS;
+    static constexpr int value = LinePlan<N>::R[REV ? (NSTAGE - 1 - S) : S];
+};
+
+// Product of the radices before stage s.
+template <int N, bool REV, int S>
+struct StageNs {
+    static constexpr int value = (S == 0) ? 1 : StageNs<N, REV, (S > 0 ? S - 1 : 0)>::value * StageRadix<N, REV, (S > 0 ? S - 1 : 0)>::value;
+};
+template <int N, bool REV>
+struct StageNs<N, REV, 0> {
+    static constexpr int value = 1;
+};
+
+// Padded shared-memory index for an exchange written by a stage of radix RW.
+template <int RW>
+__device__ __forceinline__ int pad_idx(int p) {
+    return p + p / RW;
+}
+
+// Shared-memory floats needed per line (max over the paddings used).
+template <int N>
+struct LineSmem {
+    static constexpr int value = N + N / 4 + 1;  // smallest radix 4 -> largest padding
+};
+
+// Per-stage twiddle table in shared memory: tw[(m*R + r)*TPL + t] = exp(-2*pi*i*r*k/(Ns*R)),
+// k = (t + TPL*m) % Ns. The inverse direction uses the conjugate.
+template <int N, bool REV, int S>
+struct TwTable {
+    static constexpr int E = LinePlan<N>::E;
+    static constexpr int TPL = N / E;
+    static constexpr int R = StageRadix<N, REV, S>::value;
+    static constexpr int NSV = StageNs<N, REV, S>::value;
+    static constexpr int SIZE = (NSV > 1) ? E * TPL : 0;  // = N entries
+};
+
+template <int N, bool REV, int S>
+__device__ void fill_twiddles(float2* tw, int tid, int nthreads) {
+    using TT = TwTable<N, REV, S>;
+    if constexpr (TT::SIZE > 0) {
+        for (int i = tid; i < TT::SIZE; i += nthreads) {
+            int t = i % TT::TPL;
+            int mr = i / TT::TPL;
+            int r = mr % TT::R;
+            int m = mr / TT::R;
+            int k = (t + TT::TPL * m) % TT::NSV;
+            double s, c;
+            sincospi(-2.0 * (double)(r * k) / (double)(TT::NSV * TT::R), &s, &c);
+            tw[i] = make_float2((float)c, (float)s);
+        }
+    }
+}
+
+// Compute stage S (twiddle + DFT) in registers. x[m*R + r] holds input j + r*N/R, j = t + TPL*m.
+template <int N, bool REV, int S, int DIR>
+__device__ __forceinline__ void stage_compute(float2* x, int t, const float2* tw) {
+    constexpr int E = LinePlan<N>::E;
+    constexpr int TPL = N / E;
+    constexpr int R = StageRadix<N, REV, S>::value;
+    constexpr int NSV = StageNs<N, REV, S>::value;
+    static_for<0, E / R>([&](auto mc) {
+        constexpr int m = decltype(mc)::value;
+        if constexpr (NSV > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                float2 w = tw[(m * R + r) * TPL + t];
+                x[m * R + r] = (DIR < 0) ? cmul(x[m * R + r], w) : cmulc(x[m * R + r], w);
+            }
+        }
+        dft<R, DIR>(&x[m * R]);
+    });
+}
+
+// Exchange after stage S through the line buffer `buf` (floats as float2), then load the inputs
+// of stage S+1. Caller provides the barrier functor (warp- or block-level).
+template <int N, bool REV, int S, class Sync>
+__device__ __forceinline__ void stage_exchange(float2* x, float2* buf, int t, Sync sync) {
+    constexpr int E = LinePlan<N>::E;
+    constexpr int TPL = N / E;
+    constexpr int R = StageRadix<N, REV, S>::value;
+    constexpr int NSV = StageNs<N, REV, S>::value;
+    constexpr int R2 = StageRadix<N, REV, S + 1>::value;
+    sync();
+#pragma unroll
+    for (int m = 0; m < E / R; ++m) {
+        int j = t + TPL * m;
+        int base = (j / NSV) * NSV * R + (j % NSV);
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[pad_idx<R>(base + r * NSV)] = x[m * R + r];
+    }
+    sync();
+#pragma unroll
+    for (int m = 0; m < E / R2; ++m) {
+        int j = t + TPL * m;
+#pragma unroll
+        for (int r = 0; r < R2; ++r) x[m * R2 + r] = buf[pad_idx<R>(j + r * (N / R2))];
+    }
+}
+
+// Full transform: x holds the first stage's inputs (positions j + r*N/R_first); on return it
+// holds outputs at positions j + r*N/R_last. tw[s] are the stage twiddle tables.
+template <int N, bool REV, int DIR, class Sync>
+__device__ __forceinline__ void line_fft(float2* x, float2* buf, const float2* const* tw, int t, Sync sync) {
+    constexpr int NSTAGE = LinePlan<N>::NS;
+    static_for<0, NSTAGE>([&](auto sc) {
+        constexpr int s = decltype(sc)::value;
+        stage_compute<N, REV, s, DIR>(x, t, tw[s]);
+        if constexpr (s + 1 < NSTAGE) stage_exchange<N, REV, s>(x, buf, t, sync);
+    });
+}
+
+// Position held by register i after a transform whose last stage has radix RL:
+// i = m*RL + r  ->  j + r*N/RL with j = t + TPL*m.
+template <int N, int RL>
+__device__ __forceinline__ int reg_pos(int i, int t) {
+    constexpr int TPL = N / LinePlan<N>::E;
+    return (t + TPL * (i / RL)) + (i % RL) * (N / RL);
+}
+
+}  // namespace mtb

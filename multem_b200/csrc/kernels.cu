@@ -1,0 +1,302 @@
+// Device kernels of the multislice engine (sm_100a).
+//
+// Data layout in HBM follows the reference (column-major, element (iy, ix) at ix*ny + iy, real
+// space fft-shifted the way Grid_2d::ind_col_pbc_shift stores the potential, src/types.cuh:2229).
+// A probe wave between passes is kept "hybrid": Fourier transformed along y (contiguous lines)
+// and real along x. One multislice step psi <- IFFT2[P * FFT2[T * psi]] is then two passes, each
+// reading and writing the wave once:
+//   rows  (contiguous y-lines): S <- F_y( T * F_y^-1 S )
+//   cols  (strided x-lines)   : S <- F_x^-1( P * F_x S )
+// because F = F_x F_y and the two 1-D transforms commute. The annular-detector sums of the
+// reference's get_psi + sum_square_over_Det (src/wave_function.cuh:96-155) are taken inside the
+// column pass right after the P multiply, where the registers hold FFT2(psi)/N.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+
+#include "common.hpp"
+#include "fft_core.cuh"
+#include "kernels.cuh"
+
+namespace mtb {
+
+static std::atomic<long long> g_launches{0};
+long long launches_issued() { return g_launches.load(); }
+void note_launch() { g_launches++; }
+
+// =============================================================================================
+// Projected potential splat fused with the transmission function.
+//
+// Projected_Potential::operator() (src/projected_potential.cuh:127-156) evaluates, for every atom
+// of a slice and every pixel of its footprint box (get_bn, src/cpu_fcns.hpp:1670-1684),
+//   R2 = (ix*dRx + Rx_0 - x)^2 + (iy*dRy + Ry_0 - y)^2;  if R2 < R2_max:
+//   V[ind_col_pbc_shift(ix, iy)] += occ * cubic(R2)   (eval_cubic_poly, src/cgpu_fcns.cuh:1498-1567)
+// with an FP32 atomicAdd per contribution. Here one CTA owns a 16 x 32 tile of the stored
+// (shifted) grid of one slice, culls the slice's atoms against its tile, and sums the
+// contributions of the surviving atoms in atom order in registers (deterministic, no atomics).
+// The epilogue writes T = exp(i*w*V) (functor::transmission_function, src/cgpu_fcns.cuh:3072-3086)
+// directly; V never goes to HBM unless asked for. Float products and sums use the _rn intrinsics
+// so they are not fused into FMAs and round like the reference's host float path.
+// =============================================================================================
+constexpr int SPLAT_TX = 16;   // tile extent along x (slow index)
+constexpr int SPLAT_TY = 32;   // tile extent along y (contiguous index)
+constexpr int SPLAT_THREADS = 256;
+constexpr int SPLAT_MAXT_SMEM = 8;
+
+__device__ __forceinline__ int pmod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+struct AtomFoot {
+    float x, y, occ;
+    int type;
+    int ix0, nxa, iy0, nya;
+    int sx, sy;  // first footprint pixel in stored (shifted) coordinates
+};
+
+__global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int islice_0) {
+    extern __shared__ float sm_tab[];
+    __shared__ AtomFoot s_list[SPLAT_THREADS];
+    __shared__ int s_warp_cnt[SPLAT_THREADS / 32];
+    __shared__ int s_n;
+
+    const int nR = a.nR;
+    const int ntab = (a.n_types <= SPLAT_MAXT_SMEM) ? a.n_types : 0;
+    for (int i = threadIdx.x; i < ntab * 5 * nR; i += blockDim.x) sm_tab[i] = a.tab[i];
+    const float* tab = (ntab > 0) ? sm_tab : a.tab;
+
+    const GridDev g = a.g;
+    const int islice = islice_0 + blockIdx.z;
+    const int tx0 = blockIdx.y * SPLAT_TX;
+    const int ty0 = blockIdx.x * SPLAT_TY;
+    const int ly = threadIdx.x % SPLAT_TY;
+    const int lx = threadIdx.x / SPLAT_TY;  // 0..7
+    const int jy = ty0 + ly;
+    const int jx0 = tx0 + lx, jx1 = tx0 + lx + 8;
+    float V0 = 0.0f, V1 = 0.0f;
+
+    const int2 rng = a.slice_range[islice];
+    __syncthreads();
+    for (int c0 = rng.x; c0 <= rng.y; c0 += SPLAT_THREADS) {
+        const int ia = c0 + threadIdx.x;
+        AtomFoot f;
+        bool hit = false;
+        if (ia <= rng.y) {
+            float4 at = a.atoms[ia];
+            f.x = at.x;
+            f.y = at.y;
+            f.occ = at.z;
+            f.type = __float_as_int(at.w);
+            const float Rm = a.R_max[f.type];
+            // get_bn (src/cpu_fcns.hpp:1670-1684), periodic
+            int i0 = (int)floorf(__fdiv_rn(__fsub_rn(f.x, Rm), g.dRx));
+            int ie = (int)ceilf(__fdiv_rn(__fadd_rn(f.x, Rm), g.dRx));
+            f.ix0 = i0;
+            f.nxa = (i0 == ie) ? 0 : ie - i0 + 1;
+            i0 = (int)floorf(__fdiv_rn(__fsub_rn(f.y, Rm), g.dRy));
+            ie = (int)ceilf(__fdiv_rn(__fadd_rn(f.y, Rm), g.dRy));
+            f.iy0 = i0;
+            f.nya = (i0 == ie) ? 0 : ie - i0 + 1;
+            f.sx = (pmod(f.ix0, g.nx) + g.nxh) % g.nx;
+            f.sy = (pmod(f.iy0, g.ny) + g.nyh) % g.ny;
+            // circular overlap of [sx, sx+nxa) with [tx0, tx0+TX) (and y)
+            bool ox = (f.nxa >= g.nx) || (pmod(tx0 - f.sx, g.nx) < f.nxa) || (pmod(f.sx - tx0, g.nx) < SPLAT_TX);
+            bool oy = (f.nya >= g.ny) || (pmod(ty0 - f.sy, g.ny) < f.nya) || (pmod(f.sy - ty0, g.ny) < SPLAT_TY);
+            hit = ox && oy && f.nxa > 0 && f.nya > 0;
+        }
+        // deterministic compaction in atom order
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) s_warp_cnt[warp] = __popc(m);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int w = 0; w < SPLAT_THREADS / 32; w++) {
+                int cnt = s_warp_cnt[w];
+                s_warp_cnt[w] = acc;
+                acc += cnt;
+            }
+            s_n = acc;
+        }
+        __syncthreads();
+        if (hit) s_list[s_warp_cnt[warp] + __popc(m & ((1u << lane) - 1u))] = f;
+        __syncthreads();
+        const int n = s_n;
+        for (int k = 0; k < n; k++) {
+            const AtomFoot af = s_list[k];
+            const float* T = tab + (size_t)af.type * 5 * nR;
+            const float Rm = a.R_max[af.type];
+            const float R2_max = __fmul_rn(Rm, Rm);
+            // y offsets are shared by both pixels of this thread
+            int offy = pmod(jy - af.sy, g.ny);
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                const int jx = p == 0 ? jx0 : jx1;
+                int offx = pmod(jx - af.sx, g.nx);
+                for (int ox = offx; ox < af.nxa; ox += g.nx) {
+                    const int ix = af.ix0 + ox;
+                    const float Rx = __fsub_rn(__fadd_rn(__fmul_rn((float)ix, g.dRx), g.Rx_0), af.x);
+                    for (int oy = offy; oy < af.nya; oy += g.ny) {
+                        const int iy = af.iy0 + oy;
+                        const float Ry = __fsub_rn(__fadd_rn(__fmul_rn((float)iy, g.dRy), g.Ry_0), af.y);
+                        const float R2 = __fadd_rn(__fmul_rn(Rx, Rx), __fmul_rn(Ry, Ry));
+                        if (R2 < R2_max) {
+                            // unrolledBinarySearch_c_nR (src/cgpu_fcns.cuh:1498-1518) over 128 knots
+                            int i0 = 0, ie = nR - 1;
+#pragma unroll
+                            for (int it = 0; it < 7; it++) {
+                                int im = (i0 + ie) >> 1;
+                                if (R2 < T[im]) ie = im; else i0 = im;
+                            }
+                            const float dx = __fsub_rn(R2, T[i0]);
+                            const float c3 = T[4 * nR + i0], c2 = T[3 * nR + i0], c1 = T[2 * nR + i0], c0v = T[nR + i0];
+                            float v = __fadd_rn(__fmul_rn(c3, dx), c2);
+                            v = __fadd_rn(__fmul_rn(v, dx), c1);
+                            v = __fadd_rn(__fmul_rn(v, dx), c0v);
+                            v = __fmul_rn(af.occ, v);
+                            if (p == 0) V0 += v; else V1 += v;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const size_t base = (size_t)islice * g.nx * g.ny;
+    const float Vs[2] = {V0, V1};
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const int jx = p == 0 ? jx0 : jx1;
+        const size_t idx = base + (size_t)jx * g.ny + jy;
+        if (a.V) a.V[idx] = Vs[p];
+        if (a.trans) {
+            const float th = __fmul_rn(a.w, Vs[p]);
+            float sn, cs;
+            if (a.wpo) {
+                cs = 1.0f;
+                sn = th;
+            } else {
+                sincosf(th, &sn, &cs);
+            }
+            a.trans[idx] = make_float2(cs, sn);
+        }
+    }
+}
+
+void launch_splat(const SplatArgs& a, int islice_0, int n_slice, cudaStream_t s) {
+    if (a.g.nx % SPLAT_TX || a.g.ny % SPLAT_TY) fail(MT_ERR_UNSUPPORTED, "grid must be a multiple of 16 x 32");
+    dim3 grid(a.g.ny / SPLAT_TY, a.g.nx / SPLAT_TX, n_slice);
+    size_t sm = (a.n_types <= SPLAT_MAXT_SMEM) ? (size_t)a.n_types * 5 * a.nR * sizeof(float) : 0;
+    splat_kernel<<<grid, SPLAT_THREADS, sm, s>>>(a, islice_0);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
+// =============================================================================================
+// Line passes
+// =============================================================================================
+template <int NY>
+void rows_dispatch_mode(RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s);
+template <int NX>
+void cols_dispatch_flags(int flags, const ColArgs& a, int grid_ctas, cudaStream_t s);
+
+int col_tiles(int nx, int ny) {
+    int tpl = 0;
+    switch (nx) {
+        case 64: tpl = 64 / LinePlan<64>::E; break;
+        case 128: tpl = 128 / LinePlan<128>::E; break;
+        case 256: tpl = 256 / LinePlan<256>::E; break;
+        case 512: tpl = 512 / LinePlan<512>::E; break;
+        case 1024: tpl = 1024 / LinePlan<1024>::E; break;
+        case 2048: tpl = 2048 / LinePlan<2048>::E; break;
+        default: fail(MT_ERR_UNSUPPORTED, "unsupported nx");
+    }
+    return ny / (256 / tpl);
+}
+
+void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s) {
+    if (a.nx % 256 != 0 && a.nx % 16 != 0) fail(MT_ERR_UNSUPPORTED, "nx must be a multiple of 16");
+    switch (ny) {
+        case 64: rows_dispatch_mode<64>(mode, a, grid_ctas, s); break;
+        case 128: rows_dispatch_mode<128>(mode, a, grid_ctas, s); break;
+        case 256: rows_dispatch_mode<256>(mode, a, grid_ctas, s); break;
+        case 512: rows_dispatch_mode<512>(mode, a, grid_ctas, s); break;
+        case 1024: rows_dispatch_mode<1024>(mode, a, grid_ctas, s); break;
+        case 2048: rows_dispatch_mode<2048>(mode, a, grid_ctas, s); break;
+        default: fail(MT_ERR_UNSUPPORTED, "ny must be one of 64, 128, 256, 512, 1024, 2048");
+    }
+}
+
+void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_t s) {
+    switch (nx) {
+        case 64: cols_dispatch_flags<64>(flags, a, grid_ctas, s); break;
+        case 128: cols_dispatch_flags<128>(flags, a, grid_ctas, s); break;
+        case 256: cols_dispatch_flags<256>(flags, a, grid_ctas, s); break;
+        case 512: cols_dispatch_flags<512>(flags, a, grid_ctas, s); break;
+        case 1024: cols_dispatch_flags<1024>(flags, a, grid_ctas, s); break;
+        case 2048: cols_dispatch_flags<2048>(flags, a, grid_ctas, s); break;
+        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 512, 1024, 2048");
+    }
+}
+
+// =============================================================================================
+// Detector reduction: one thread per (probe, detector); tiles summed in order (deterministic).
+__global__ void det_reduce_kernel(const double* __restrict__ partial, int nprobe, int n_tiles, int n_det,
+                                  const int* __restrict__ scan_index, double w, double* __restrict__ image,
+                                  int n_scan) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nprobe * n_det) return;
+    const int b = i / n_det, d = i % n_det;
+    double s = 0.0;
+    for (int k = 0; k < n_tiles; k++) s += partial[((size_t)b * n_tiles + k) * n_det + d];
+    image[(size_t)d * n_scan + scan_index[b]] += w * s;
+}
+
+void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det, const int* scan_index, double w,
+                       double* image, int n_scan, cudaStream_t s) {
+    const int n = nprobe * n_det;
+    det_reduce_kernel<<<(n + 127) / 128, 128, 0, s>>>(partial, nprobe, n_tiles, n_det, scan_index, w, image, n_scan);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
+// =============================================================================================
+// EW output accumulation with fft-shift and crop (add_scale_crop_shift_2d /
+// add_scale_square_crop_shift_2d / assign_crop_shift_2d, src/cgpu_fcns.cuh:1681-1780).
+__global__ void ew_accumulate_kernel(const float2* __restrict__ psi, int nx, int ny, int ix0, int ix1, int iy0,
+                                     int iy1, double w, int assign, double* __restrict__ psi_out,
+                                     double* __restrict__ m2_out) {
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y;
+    if (iy >= ny || ix >= nx) return;
+    if (ix < ix0 || ix >= ix1 || iy < iy0 || iy >= iy1) return;
+    // output pixel (ix, iy) takes the stored pixel shifted by half the grid
+    const int sx = (ix + nx / 2) % nx, sy = (iy + ny / 2) % ny;
+    const float2 v = psi[(size_t)sx * ny + sy];
+    const size_t o = (size_t)(ix - ix0) * (iy1 - iy0) + (iy - iy0);
+    if (psi_out) {
+        if (assign) {
+            psi_out[2 * o] = v.x;
+            psi_out[2 * o + 1] = v.y;
+        } else {
+            psi_out[2 * o] += w * v.x;
+            psi_out[2 * o + 1] += w * v.y;
+        }
+    }
+    if (m2_out) {
+        const float n2 = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+        m2_out[o] += w * (double)n2;
+    }
+}
+
+void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, int iy0, int iy1, double w,
+                          int assign, double* psi_out, double* m2_out, cudaStream_t s) {
+    dim3 grid((ny + 127) / 128, nx);
+    ew_accumulate_kernel<<<grid, 128, 0, s>>>(psi, nx, ny, ix0, ix1, iy0, iy1, w, assign, psi_out, m2_out);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
+}  // namespace mtb

@@ -1,0 +1,105 @@
+// Device kernels of the multislice engine and their launch wrappers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace mtb {
+
+constexpr int kMaxDet = 8;
+constexpr int kMaxTypes = 16;
+
+// Grid_2d<float> fields the kernels use (src/types.cuh:2107-2655).
+struct GridDev {
+    int nx, ny, nxh, nyh;
+    float lx, ly, dRx, dRy, Rx_0, Ry_0, dgx, dgy;
+};
+
+// ---- projected potential + transmission (splat) ----
+struct SplatArgs {
+    GridDev g;
+    const float4* atoms;       // (x, y, occ, type index as int bits), z-sorted
+    const int2* slice_range;   // per slice (iatom_0, iatom_e), empty when iatom_0 > iatom_e
+    const float* tab;          // per type 5*nR floats: R2, c0, c1, c2, c3
+    const float* R_max;        // per type (float)
+    int n_types;
+    int nR;
+    float w;                   // Vr_factor: T = exp(i*w*V)
+    int wpo;                   // weak phase object: T = 1 + i*w*V
+    float2* trans;             // [n_slice][nx*ny] or null
+    float* V;                  // [n_slice][nx*ny] or null
+};
+void launch_splat(const SplatArgs& a, int islice_0, int n_slice, cudaStream_t s);
+
+// ---- line passes ----
+// Contiguous-line (y) pass modes.
+enum RowMode : int {
+    ROW_STEP = 0,       // load hybrid, inverse FFT_y, * T, forward FFT_y, store
+    ROW_FIRST_ONE = 1,  // psi = 1 (plane wave), * T, forward FFT_y, store
+    ROW_FIRST_REAL = 2, // load real-space psi, * T, forward FFT_y, store
+    ROW_INVERSE = 3     // load hybrid, inverse FFT_y, * scale, store (real-space output)
+};
+struct RowArgs {
+    const float2* in;
+    float2* out;
+    const float2* trans;   // [nx*ny] of the slice
+    int nx;                // lines per probe
+    int nprobe;
+    float scale;
+};
+void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s);
+
+// Strided-line (x) pass modes (bit flags).
+enum ColFlags : int {
+    COL_LOAD = 1,      // load hybrid and forward FFT_x (else generate the probe)
+    COL_PROP = 2,      // multiply by Px[ix]*Py[iy]
+    COL_DETECT = 4,    // ring sums of |psi_hat|^2 into partials
+    COL_INVERSE = 8,   // inverse FFT_x before the store
+    COL_STORE = 16     // store the result
+};
+struct ProbeDev {
+    float c_c_10, c_c_30, c_c_50;
+    float g2_min, g2_max;
+    float gxu, gyu;
+    float norm;
+    int phi_required;
+    // phi-dependent aberrations (c_c_xx, phi_xx) and vortex momentum
+    float c_c_12, phi_12, c_c_21, phi_21, c_c_23, phi_23, c_c_32, phi_32, c_c_34, phi_34;
+    float c_c_41, phi_41, c_c_43, phi_43, c_c_45, phi_45, c_c_52, phi_52, c_c_54, phi_54, c_c_56, phi_56;
+    int m;
+    int nz_c10, nz_c30, nz_c50;
+};
+struct ColArgs {
+    const float2* in;
+    float2* out;
+    int ny;                    // line stride (elements) and number of columns
+    int nprobe;
+    GridDev g;
+    const float2* Px;          // [nx] propagator factor along x (includes 1/N)
+    const float2* Py;          // [ny]
+    // probe generation
+    const float2* beam;        // per probe (x, y) = exp_factor_R(beam position)
+    ProbeDev probe;
+    // detectors
+    int n_det;
+    float det_g2_min[kMaxDet], det_g2_max[kMaxDet];
+    float gx_0, gy_0;
+    double* det_partial;       // [nprobe][n_tiles][n_det]
+};
+void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_t s);
+int col_tiles(int nx, int ny);  // column tiles per probe (partials per probe per detector)
+
+// Sum detector partials over tiles and add w * sum into image[(idet*n_scan) + scan_index].
+void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det, const int* scan_index,
+                       double w, double* image, int n_scan, cudaStream_t s);
+
+// EW output: out[(ix-ix0)*oy + (iy-iy0)] accumulates psi (complex) and |psi|^2 over the output
+// area after an fft-shift by (nx/2, ny/2) (add_scale_crop_shift_2d, src/cgpu_fcns.cuh:1701-1739).
+void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, int iy0, int iy1, double w,
+                          int assign, double* psi_out, double* m2_out, cudaStream_t s);
+
+// Device-side counters of this library's launches (for reporting).
+long long launches_issued();
+
+}  // namespace mtb

@@ -1,0 +1,7 @@
+// Line-pass kernels for lines of 64 points (see line_kernels.cuh).
+#include "line_kernels.cuh"
+
+namespace mtb {
+template void rows_dispatch_mode<64>(RowMode, const RowArgs&, int, cudaStream_t);
+template void cols_dispatch_flags<64>(int, const ColArgs&, int, cudaStream_t);
+}  // namespace mtb

@@ -1,0 +1,237 @@
+// FP64 build of the Lobato radial projected-potential spline tables on the GPU.
+//
+// Follows Atomic_Data::get_atom_coef (src/atomic_data.hpp:1547-1668) for neutral atoms with the
+// Lobato (0-12) parameterisation (set_Lobato_neutral_coef, src/atomic_data.hpp:1441-1486):
+//   VR.cl = 2*Potf*pi^2*cl/cnl^1.5, VR.cnl = 2*pi/sqrt(cnl)        (projected potential)
+//   Vr.cl =   Potf*pi^2*cl/cnl^1.5, Vr.cnl = 2*pi/sqrt(cnl)        (3-D potential)
+//   R_min = max(dR_min, rn_c), rn_c = 1.2e-5*A^(1/3)
+//   R_max = root of Vr(r) = Vrl by bisection on [rn_c, 25] (Atom_Cal::AtomicRadius_Cutoff,
+//           src/atomic_fcns_mt.hpp:269-295; Root_Finder, src/cgpu_fcns.cuh:262-286),
+//           R_max = max(R_max, 2*R_min), or 1.75*ra when it is zero
+//   R_tap = R_min + 0.85*(R_max - R_min), tap_cf = (pi/2)/(R_max^2 - R_tap^2)
+//   nR log-spaced knots R_i = R_min*exp(i*ln(R_max/R_min)/(nR-1)), spline variable R^2
+//   VR(R) = sum_5 cl*(2*K0(cnl*R)/cnl + R*K1(cnl*R)), dVR/dR = -sum_5 cl*(cnl*R*K0 + 2*K1)
+//           (VR_dVR_Lobato_neutral_0_12, src/cgpu_fcns.cuh:1256-1268)
+//   c0 = VR, c1 = dVR/d(R^2) = 0.5*dVR/R, both cosine-tapered beyond R_tap^2 (apply_tapering,
+//   src/cgpu_fcns.cuh:1530-1540); c2, c3 from the Hermite conditions between knots
+//   (src/atomic_data.hpp:1652-1663).
+// The modified Bessel functions K0, K1 use the polynomial approximations of Abramowitz & Stegun,
+// Handbook of Mathematical Functions, 9.8.1-9.8.8 (I0, I1 for x <= 3.75; K0, K1 for x <= 2 and
+// x > 2), the same published approximations the reference uses (src/math.cuh:465-630).
+// R_min/R_max/R_tap come from element_head() on the host (a sequential root find in FP64); one
+// CUDA block then builds the knots and coefficients of one element, one thread per knot, in FP64.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.hpp"
+#include "tables.hpp"
+
+namespace mtb {
+
+namespace {
+
+#include "atomic_params.inc"
+
+constexpr double kPotf = 47.877645145863056;
+constexpr double kPi = 3.141592653589793238463;
+constexpr double kPi2 = 9.869604401089358618834;
+constexpr double k2Pi = 6.283185307179586476925;
+constexpr double kHalfPi = 1.570796326794896619231;
+
+struct ElemCoef {
+    double VRcl[5], VRcnl[5], Vrcl[5], Vrcnl[5];
+    double rn_c, ra;
+};
+
+__device__ double as_i0(double x) {  // A&S 9.8.1 / 9.8.2
+    double ax = fabs(x), y;
+    if (ax < 3.75) {
+        y = x / 3.75;
+        y = y * y;
+        return 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 + y * (0.2659732 + y * (0.360768e-1 + y * 0.45813e-2)))));
+    }
+    y = 3.75 / ax;
+    return (exp(ax) / sqrt(ax)) *
+           (0.39894228 + y * (0.1328592e-1 + y * (0.225319e-2 + y * (-0.157565e-2 + y * (0.916281e-2 + y * (-0.2057706e-1 + y * (0.2635537e-1 + y * (-0.1647633e-1 + y * 0.392377e-2))))))));
+}
+
+__device__ double as_i1(double x) {  // A&S 9.8.3 / 9.8.4
+    double ax = fabs(x), y, ans;
+    if (ax < 3.75) {
+        y = x / 3.75;
+        y = y * y;
+        ans = ax * (0.5 + y * (0.87890594 + y * (0.51498869 + y * (0.15084934 + y * (0.2658733e-1 + y * (0.301532e-2 + y * 0.32411e-3))))));
+    } else {
+        y = 3.75 / ax;
+        ans = 0.2282967e-1 + y * (-0.2895312e-1 + y * (0.1787654e-1 - y * 0.420059e-2));
+        ans = 0.39894228 + y * (-0.3988024e-1 + y * (-0.362018e-2 + y * (0.163801e-2 + y * (-0.1031555e-1 + y * ans))));
+        ans *= (exp(ax) / sqrt(ax));
+    }
+    return (x < 0.0) ? -ans : ans;
+}
+
+__device__ double as_k0(double x) {  // A&S 9.8.5 / 9.8.6
+    double y;
+    if (x <= 2.0) {
+        y = x * x / 4.0;
+        return (-log(x / 2.0) * as_i0(x)) +
+               (-0.57721566 + y * (0.42278420 + y * (0.23069756 + y * (0.3488590e-1 + y * (0.262698e-2 + y * (0.10750e-3 + y * 0.74e-5))))));
+    }
+    y = 2.0 / x;
+    return (exp(-x) / sqrt(x)) *
+           (1.25331414 + y * (-0.7832358e-1 + y * (0.2189568e-1 + y * (-0.1062446e-1 + y * (0.587872e-2 + y * (-0.251540e-2 + y * 0.53208e-3))))));
+}
+
+__device__ double as_k1(double x) {  // A&S 9.8.7 / 9.8.8
+    double y;
+    if (x <= 2.0) {
+        y = x * x / 4.0;
+        return (log(x / 2.0) * as_i1(x)) +
+               (1.0 / x) * (1.0 + y * (0.15443144 + y * (-0.67278579 + y * (-0.18156897 + y * (-0.1919402e-1 + y * (-0.110404e-2 + y * (-0.4686e-4)))))));
+    }
+    y = 2.0 / x;
+    return (exp(-x) / sqrt(x)) *
+           (1.25331414 + y * (0.23498619 + y * (-0.3655620e-1 + y * (0.1504268e-1 + y * (-0.780353e-2 + y * (0.325614e-2 + y * (-0.68245e-3)))))));
+}
+
+__global__ void build_tables_kernel(const ElemCoef* __restrict__ coef, const TableHead* __restrict__ head,
+                                    int n_elem, int nR, float* __restrict__ tab) {
+    const int ie = blockIdx.x;
+    if (ie >= n_elem) return;
+    const ElemCoef c = coef[ie];
+    const TableHead h = head[ie];
+    extern __shared__ double sdyn[];
+    double* c0 = sdyn;
+    double* c1 = sdyn + nR;
+    double* R2 = sdyn + 2 * nR;
+    const double R_min = h.R_min, R_max = h.R_max, R_tap = h.R_tap, tap_cf = h.tap_cf;
+    const double dlnr = log(R_max / R_min) / (double)(nR - 1);
+    const double x_tap = pow(R_tap, 2);
+    for (int iR = threadIdx.x; iR < nR; iR += blockDim.x) {
+        double R = R_min * exp(iR * dlnr);
+        double r2 = pow(R, 2);
+        double y = 0, dy = 0;
+        for (int i = 0; i < 5; i++) {
+            double k0 = as_k0(c.VRcnl[i] * R);
+            double k1 = as_k1(c.VRcnl[i] * R);
+            y += c.VRcl[i] * (2 * k0 / c.VRcnl[i] + R * k1);
+            dy += -c.VRcl[i] * (c.VRcnl[i] * R * k0 + 2 * k1);
+        }
+        dy = 0.5 * dy / R;
+        if (x_tap < r2) {
+            double s, co;
+            sincos(tap_cf * (r2 - x_tap), &s, &co);
+            dy = dy * co - tap_cf * y * s;
+            y *= co;
+        }
+        c0[iR] = y;
+        c1[iR] = dy;
+        R2[iR] = r2;
+    }
+    __syncthreads();
+    float* t = tab + (size_t)ie * 5 * nR;
+    for (int iR = threadIdx.x; iR < nR; iR += blockDim.x) {
+        double c2 = 0, c3 = 0;
+        if (iR < nR - 1) {
+            double idR = 1.0 / (R2[iR + 1] - R2[iR]);
+            double V = c0[iR], Vn = c0[iR + 1], dV = c1[iR], dVn = c1[iR + 1];
+            double mm = (Vn - V) * idR, n = dV + dVn;
+            c2 = (3.0 * mm - n - dV) * idR;
+            c3 = (n - 2.0 * mm) * idR * idR;
+        }
+        t[iR] = (float)R2[iR];
+        t[nR + iR] = (float)c0[iR];
+        t[2 * nR + iR] = (float)c1[iR];
+        t[3 * nR + iR] = (float)c2;
+        t[4 * nR + iR] = (float)c3;
+    }
+}
+
+// set_Lobato_neutral_coef (src/atomic_data.hpp:1441-1486) and the rn_c of To_atom_type_CPU
+// (src/atomic_data.hpp:148-176)
+ElemCoef element_coef(int Z) {
+    ElemCoef e{};
+    int iZ = Z - 1;
+    for (int j = 0; j < 5; j++) {
+        double cl = kLobatoCl[iZ][j];
+        double cnl = (std::fabs(cl) <= 1e-13) ? 0.0 : kLobatoCnl[iZ][j];
+        bool nz = !((std::fabs(cl) <= 1e-13) || (std::fabs(cnl) <= 1e-13));
+        if (nz) {
+            e.Vrcl[j] = kPotf * kPi2 * cl / std::pow(cnl, 1.5);
+            e.Vrcnl[j] = k2Pi / std::sqrt(cnl);
+            e.VRcl[j] = 2.0 * kPotf * kPi2 * cl / std::pow(cnl, 1.5);
+            e.VRcnl[j] = k2Pi / std::sqrt(cnl);
+        } else {
+            e.Vrcl[j] = 0.0;
+            e.Vrcnl[j] = 1.0;
+            e.VRcl[j] = 0.0;
+            e.VRcnl[j] = 1.0;
+        }
+    }
+    e.rn_c = 1.2e-05 * std::pow((double)kMassNumber[iZ], 1.0 / 3.0);
+    e.ra = kAtomicRadius[iZ];
+    return e;
+}
+
+}  // namespace
+
+// 3-D potential of the Lobato parameterisation (Vr_Lobato_neutral_0_12,
+// src/cgpu_fcns.cuh:1111-1120)
+static double lobato_vr_host(double x, const ElemCoef& c) {
+    double ix = 1.0 / x, y = 0;
+    for (int i = 0; i < 5; i++) y += c.Vrcl[i] * std::exp(-c.Vrcnl[i] * x) * ix * (2.0 / c.Vrcnl[i] + x);
+    return y;
+}
+
+TableHead element_head(int Z, float dR_min, float Vrl_f) {
+    const ElemCoef c = element_coef(Z);
+    const double Vrl = (double)Vrl_f;
+    const double R_min = std::fmax(c.rn_c, (double)dR_min);
+    double R_max = 0;
+    const bool nonzero = !(std::fabs(Vrl) <= 1e-13) && !(std::fabs(c.Vrcl[0]) <= 1e-13);
+    if (nonzero) {
+        // Root_Finder (src/cgpu_fcns.cuh:262-286): bisection on [rn_c, 25], |f| <= 1e-8 or 200 steps
+        double x0 = c.rn_c, xe = 25.0, x = 0, fx;
+        double fxe = lobato_vr_host(xe, c) - Vrl;
+        int it = 0;
+        do {
+            x = 0.5 * (x0 + xe);
+            fx = lobato_vr_host(x, c) - Vrl;
+            if (fx * fxe < 0) {
+                x0 = x;
+            } else {
+                xe = x;
+                fxe = fx;
+            }
+            it++;
+        } while ((std::fabs(fx) > 1e-8) && (it < 200));
+        R_max = x;
+    }
+    R_max = std::fmax(R_max, 2.0 * R_min);
+    if (std::fabs(R_max) <= 1e-13) R_max = 1.75 * c.ra;
+    const double R_tap = R_min + 0.85 * (R_max - R_min);
+    const double tap_cf = kHalfPi / (std::pow(R_max, 2) - std::pow(R_tap, 2));
+    return TableHead{R_min, R_max, R_tap, tap_cf};
+}
+
+void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
+                  cudaStream_t stream) {
+    const int n = (int)Zs.size();
+    std::vector<ElemCoef> h(n);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i]);
+    ElemCoef* d_coef = nullptr;
+    TableHead* d_head = nullptr;
+    MTB_CUDA(cudaMallocAsync(&d_coef, sizeof(ElemCoef) * n, stream));
+    MTB_CUDA(cudaMallocAsync(&d_head, sizeof(TableHead) * n, stream));
+    MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
+    MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));
+    build_tables_kernel<<<n, 128, 3 * nR * sizeof(double), stream>>>(d_coef, d_head, n, nR, d_tab);
+    MTB_CUDA(cudaGetLastError());
+    MTB_CUDA(cudaStreamSynchronize(stream));
+    MTB_CUDA(cudaFreeAsync(d_coef, stream));
+    MTB_CUDA(cudaFreeAsync(d_head, stream));
+}
+
+}  // namespace mtb

@@ -1,0 +1,24 @@
+// FP64 spline-table build for the Lobato projected potential (see tables.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace mtb {
+
+struct TableHead {
+    double R_min, R_max, R_tap, tap_cf;
+};
+
+// FP64 header of element Z on the host: R_min = max(dR_min, rn_c), R_max from the Vr = Vrl root,
+// R_tap and the taper factor (Atomic_Data::get_atom_coef, src/atomic_data.hpp:1590-1620).
+TableHead element_head(int Z, float dR_min, float Vrl);
+
+// Build the spline tables of the elements in Zs (with their heads) on the device in FP64. d_tab
+// receives, per element, 5*nR floats: R2[nR], c0[nR], c1[nR], c2[nR], c3[nR] (the float tables
+// the splat evaluates). Synchronises `stream`.
+void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
+                  cudaStream_t stream);
+
+}  // namespace mtb

@@ -1,0 +1,25 @@
+"""Lobato (0-12) coefficients, mass numbers and atomic radii for Z = 1..103, read from the data file
+the engine compiles in (multem_b200/csrc/atomic_params.inc, extracted from the reference's
+src/atomic_data.hpp by multem_b200/csrc/gen_atomic_params.py). Test infrastructure only."""
+import re
+from pathlib import Path
+
+_INC = Path(__file__).resolve().parents[1] / "multem_b200" / "csrc" / "atomic_params.inc"
+
+
+def _parse():
+    s = _INC.read_text()
+
+    def table(name):
+        body = re.search(name + r"\[103\]\[5\] = \{(.*?)\n\};", s, re.S).group(1)
+        rows = re.findall(r"\{([^}]*)\}", body)
+        return [[float(v) for v in r.split(",")] for r in rows]
+
+    def vec(name, cast):
+        body = re.search(name + r"\[103\] = \{([^}]*)\}", s).group(1)
+        return [cast(v) for v in body.split(",")]
+
+    return table("kLobatoCl"), table("kLobatoCnl"), vec("kMassNumber", int), vec("kAtomicRadius", float)
+
+
+LOBATO_CL, LOBATO_CNL, MASS_NUMBER, ATOMIC_RADIUS = _parse()

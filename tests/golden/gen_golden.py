@@ -1,0 +1,102 @@
+"""Generate golden fixtures from the reference's own CPU path (oracle/_ref/libmultem_ref.so).
+
+The reference has no test vectors of its own, so these fixtures are outputs of the reference code
+itself (its Multislice<T, e_host>, compiled from its sources by oracle/Makefile) on small seeded
+inputs. They let the oracle and the engine be checked where oracle/_ref is not built.
+
+    make -C oracle && python tests/golden/gen_golden.py
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from multem_b200 import specimens  # noqa: E402
+from oracle import reference as R  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def stem_small():
+    return specimens.stem_srtio3(nx=128, ny=128, na=4, nb=4, nc=4, ns=4, nconf=2, seed=7)
+
+
+def stem_thick():
+    p = specimens.stem_srtio3(nx=128, ny=128, na=4, nb=4, nc=4, ns=3, nconf=2, seed=11)
+    p.thick_type = 2
+    p.thick = [4.0, 8.0, 12.0]
+    p.cond_lens_c_10 = 15.0
+    p.cond_lens_c_30 = 0.001
+    return p
+
+
+def ew_small():
+    return specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+
+
+def ew_config1():
+    return specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=8)
+
+
+def main():
+    if not R.available():
+        raise SystemExit("oracle/_ref not built: make -C oracle")
+    rec = {}
+    # specimen host logic: displaced atoms and slicing of two configurations
+    for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
+                     ("ew_config1", ew_config1)):
+        p = fn()
+        for iconf in (1, 2):
+            if iconf > p.pn_nconf:
+                continue
+            sp = R.specimen(p, iconf)
+            for k in ("Z", "xyz", "z_0", "z_e", "iatom_0", "iatom_e", "ithk"):
+                rec[f"{name}_c{iconf}_{k}"] = sp[k]
+        rec[f"{name}_params"] = np.array([R.params(p)[k] for k in ("lambda", "Vr_factor", "cond_zero_defocus_plane",
+                                                                  "n_slice", "n_atoms", "dz", "n_thick")])
+    # spline tables at the small grids' sampling
+    p = stem_small()
+    for Z in (8, 22, 38):
+        for prec in (1, 2):
+            t = R.atom_type(p, Z, prec)
+            rec[f"tab_Z{Z}_p{prec}_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
+            rec[f"tab_Z{Z}_p{prec}_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
+    q = ew_small()
+    for prec in (1, 2):
+        t = R.atom_type(q, 14, prec)
+        rec[f"tab_Z14_p{prec}_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
+        rec[f"tab_Z14_p{prec}_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
+    # projected potential and transmission of one slice
+    for prec in (1, 2):
+        rec[f"stem_small_V_c1_s3_p{prec}"] = R.projected_potential(p, 1, 3, prec).astype(np.float64)
+        rec[f"stem_small_T_c1_s3_p{prec}"] = R.transmission_function(p, 1, 3, prec).astype(np.complex128)
+    # incident wave at an off-centre position
+    pw = stem_small()
+    pw.iw_x, pw.iw_y = [3.3], [7.1]
+    pw.cond_lens_c_10 = 25.0
+    pw.cond_lens_c_30 = 0.002
+    for prec in (1, 2):
+        rec[f"probe_real_p{prec}"] = R.incident_wave(pw, 1, prec)
+        rec[f"probe_fourier_p{prec}"] = R.incident_wave(pw, 2, prec)
+    # full runs
+    for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
+                     ("ew_config1", ew_config1)):
+        p = fn()
+        for prec in (1, 2):
+            out = R.run(p, precision=prec, nthreads=8)
+            for k in ("image_tot", "psi_coh", "m2psi_tot", "thick", "x", "y"):
+                if k in out:
+                    v = out[k]
+                    rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64) \
+                        if name == "ew_config1" else v
+    np.savez_compressed(OUT / "reference_fixtures.npz", **rec)
+    print("wrote", OUT / "reference_fixtures.npz", len(rec), "arrays")
+
+
+if __name__ == "__main__":
+    main()
