@@ -226,6 +226,13 @@ mt_status mt_engine_prepare_confs(mt_engine* eng, int iconf_0, int iconf_e);
 mt_status mt_engine_run_prepared(mt_engine* eng, int iconf_0, int iconf_e);
 /* Number of kernel launches the last run issued (own kernels only). */
 mt_status mt_engine_launch_count(mt_engine* eng, long long* n);
+/* Device timing (no counterpart in the reference): with timing on, each run records CUDA events on
+ * the engine's stream around the whole run and around every line-pass launch. mt_engine_timing
+ * returns the last run's device time and the summed durations and counts of the contiguous-line
+ * (rows) and strided-line (cols) passes. */
+mt_status mt_engine_set_timing(mt_engine* eng, int on);
+mt_status mt_engine_timing(mt_engine* eng, double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms,
+                           long long* n_cols);
 mt_status mt_engine_destroy(mt_engine* eng);
 
 /* ---- operator-level entries (ilc_projected_potential, ilc_transmission_function,

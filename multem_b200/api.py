@@ -141,6 +141,16 @@ class Engine:
     def cancel(self):
         capi.check(self.lib.mt_engine_cancel(self.h))
 
+    def set_timing(self, on: bool):
+        capi.check(self.lib.mt_engine_set_timing(self.h, 1 if on else 0))
+
+    def timing(self) -> dict:
+        """Device time of the last run_prepared (CUDA events on the engine's stream)."""
+        t, r, c = C.c_double(), C.c_double(), C.c_double()
+        nr, nc = C.c_longlong(), C.c_longlong()
+        capi.check(self.lib.mt_engine_timing(self.h, C.byref(t), C.byref(r), C.byref(nr), C.byref(c), C.byref(nc)))
+        return {"total_ms": t.value, "rows_ms": r.value, "n_rows": nr.value, "cols_ms": c.value, "n_cols": nc.value}
+
     def progress(self):
         i, n = C.c_int(), C.c_int()
         capi.check(self.lib.mt_engine_progress(self.h, C.byref(i), C.byref(n)))

@@ -110,6 +110,9 @@ SIGNATURES = {
     "mt_engine_run_prepared": (c_int, [_VP, c_int, c_int]),
     "mt_engine_launch_count": (c_int, [_VP, C.POINTER(C.c_longlong)]),
     "mt_engine_destroy": (c_int, [_VP]),
+    "mt_engine_set_timing": (c_int, [_VP, c_int]),
+    "mt_engine_timing": (c_int, [_VP, P_double, P_double, C.POINTER(C.c_longlong), P_double,
+                                 C.POINTER(C.c_longlong)]),
     "mt_projected_potential": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), c_int, c_int,
                                        P_double]),
     "mt_transmission_function": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), c_int, c_int,

@@ -142,6 +142,21 @@ mt_status mt_engine_launch_count(mt_engine* eng, long long* n) {
     });
 }
 
+mt_status mt_engine_set_timing(mt_engine* eng, int on) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        eng->eng->set_timing(on != 0);
+    });
+}
+
+mt_status mt_engine_timing(mt_engine* eng, double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms,
+                           long long* n_cols) {
+    return guarded([&] {
+        if (!eng || !total_ms || !rows_ms || !n_rows || !cols_ms || !n_cols) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        eng->eng->timing(total_ms, rows_ms, n_rows, cols_ms, n_cols);
+    });
+}
+
 mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislice* in, mt_output_multislice* out) {
     return guarded([&] {
         mt_system_conf c = conf ? *conf : default_conf();

@@ -120,6 +120,12 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
 Engine::~Engine() {
     if (stream_) {
         cudaStreamSynchronize(stream_);
+        for (auto& t : tl_) {
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        if (run_a_) cudaEventDestroy(run_a_);
+        if (run_b_) cudaEventDestroy(run_b_);
         cudaStreamDestroy(stream_);
     }
 }
@@ -161,10 +167,14 @@ void Engine::build_types() {
 // Fresnel propagator factors for distance dz, separable in x and y:
 // P(ix, iy) = exp(i*w*(gx^2 + gy^2))/N, w = -pi*lambda*dz (propagate, src/cgpu_fcns.cuh:1837-1845;
 // get_propagator_factor, src/input_multislice.cuh:909-912). Phases in double, stored as float.
-void Engine::prop_tables(float dz, float2* px, float2* py) const {
+void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const double w = (double)m_.propagator_factor(dz);
-    const double m = (double)(1.0f / (float)(nx * ny));
+    // Between passes the wave is kept as F_y(psi)/ny (the unnormalised row transforms of one step
+    // multiply by ny, the column transforms by nx). Inside the loop P carries the reference's 1/N;
+    // the output tables (back-propagation to the zero-defocus plane) carry 1/nx so that the
+    // materialised wave is psi (or FFT2(psi)*P) itself.
+    const double m = output ? 1.0 / (double)nx : (double)(1.0f / (float)(nx * ny));
     const double gx0 = m_.gx_0(), gy0 = m_.gy_0();
     for (int ix = 0; ix < nx; ix++) {
         double gx = (double)((float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx) - gx0;
@@ -237,9 +247,9 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     for (size_t t = 0; t < TH.size(); t++) cd.thick_z_back_prop[t] = TH[t].z_back_prop;
     const size_t pl = (size_t)nx + ny;
     std::vector<float2> prop((S.size() + TH.size()) * pl);
-    for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), &prop[k * pl], &prop[k * pl + nx]);
+    for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), &prop[k * pl], &prop[k * pl + nx], false);
     for (size_t t = 0; t < TH.size(); t++)
-        prop_tables(TH[t].z_back_prop, &prop[(S.size() + t) * pl], &prop[(S.size() + t) * pl + nx]);
+        prop_tables(TH[t].z_back_prop, &prop[(S.size() + t) * pl], &prop[(S.size() + t) * pl + nx], true);
     // incident-wave defocus relative to the first slice (Incident_Wave::operator(),
     // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0))
     const float z_init = (float)(0.5 * (S[0].z_0 + S[0].z_e));
@@ -278,12 +288,73 @@ void Engine::check_cancel() {
 void Engine::run_prepared(int c0, int c1) {
     if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
     long long l0 = launches_issued();
+    tl_used_ = 0;
+    if (!run_a_) {
+        MTB_CUDA(cudaEventCreate(&run_a_));
+        MTB_CUDA(cudaEventCreate(&run_b_));
+    }
+    MTB_CUDA(cudaEventRecord(run_a_, stream_));
     for (int c = c0; c <= c1; c++) {
         ConfData* cd = find_conf(c);
         if (!cd) fail(MT_ERR_INVALID_ARG, "configuration not prepared");
         run_conf(*cd);
     }
+    MTB_CUDA(cudaEventRecord(run_b_, stream_));
     launches_ = launches_issued() - l0;
+    synchronize();
+}
+
+// ---- device timing ----
+void Engine::tl_begin(int kind) {
+    if (!timing_) return;
+    if (tl_used_ == tl_.size()) {
+        TimedLaunch t{};
+        MTB_CUDA(cudaEventCreate(&t.a));
+        MTB_CUDA(cudaEventCreate(&t.b));
+        tl_.push_back(t);
+    }
+    tl_[tl_used_].kind = kind;
+    MTB_CUDA(cudaEventRecord(tl_[tl_used_].a, stream_));
+}
+
+void Engine::tl_end() {
+    if (!timing_) return;
+    MTB_CUDA(cudaEventRecord(tl_[tl_used_].b, stream_));
+    tl_used_++;
+}
+
+void Engine::rows(RowMode mode, const RowArgs& a) {
+    tl_begin(0);
+    launch_rows(m_.grid.ny, mode, a, 0, stream_);
+    tl_end();
+}
+
+void Engine::cols(int flags, const ColArgs& a) {
+    tl_begin(1);
+    launch_cols(m_.grid.nx, flags, a, 0, stream_);
+    tl_end();
+}
+
+void Engine::timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols) {
+    synchronize();
+    float ms = 0;
+    *total_ms = 0;
+    if (run_a_) {
+        MTB_CUDA(cudaEventElapsedTime(&ms, run_a_, run_b_));
+        *total_ms = ms;
+    }
+    *rows_ms = *cols_ms = 0;
+    *n_rows = *n_cols = 0;
+    for (size_t i = 0; i < tl_used_; i++) {
+        MTB_CUDA(cudaEventElapsedTime(&ms, tl_[i].a, tl_[i].b));
+        if (tl_[i].kind == 0) {
+            *rows_ms += ms;
+            (*n_rows)++;
+        } else {
+            *cols_ms += ms;
+            (*n_cols)++;
+        }
+    }
 }
 
 void Engine::run_confs(int c0, int c1) {
@@ -352,12 +423,12 @@ void Engine::run_stem(ConfData& cd) {
         ca.beam = d_beam_.p + p0;
         ca.Px = nullptr;
         ca.Py = nullptr;
-        launch_cols(nx, COL_INVERSE | COL_STORE, ca, 0, stream_);
+        cols(COL_INVERSE | COL_STORE, ca);
         for (int k = 0; k <= cd.last_slice; k++) {
             ra.in = d_psi_.p;
             ra.out = d_psi_.p;
             ra.trans = d_trans_.p + (size_t)k * nxy;
-            launch_rows(ny, ROW_STEP, ra, 0, stream_);
+            rows(ROW_STEP, ra);
             const int ithk = cd.slice_ithk[k];
             int flags = COL_LOAD | COL_PROP;
             if (ithk >= 0) flags |= COL_DETECT;
@@ -367,7 +438,7 @@ void Engine::run_stem(ConfData& cd) {
             ca.Px = cd.prop.p + (size_t)k * pl;
             ca.Py = ca.Px + nx;
             ca.det_partial = d_partial_.p + (size_t)(ithk >= 0 ? ithk : 0) * batch_ * tiles * n_det;
-            launch_cols(nx, flags, ca, 0, stream_);
+            cols(flags, ca);
         }
         for (int t = 0; t < n_thk; t++)
             launch_det_reduce(d_partial_.p + (size_t)t * batch_ * tiles * n_det, nb, tiles, n_det, d_scan_idx_.p + p0, w,
@@ -399,12 +470,12 @@ void Engine::run_ew(ConfData& cd) {
         ra.in = d_psi_.p;
         ra.out = d_psi_.p;
         ra.trans = d_trans_.p + (size_t)k * nxy;
-        launch_rows(ny, k == 0 ? ROW_FIRST_ONE : ROW_STEP, ra, 0, stream_);
+        rows(k == 0 ? ROW_FIRST_ONE : ROW_STEP, ra);
         ca.in = d_psi_.p;
         ca.out = d_psi_.p;
         ca.Px = cd.prop.p + (size_t)k * pl;
         ca.Py = ca.Px + nx;
-        launch_cols(nx, COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca, 0, stream_);
+        cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca);
         const int ithk = cd.slice_ithk[k];
         if (ithk < 0) continue;
         // wave at this thickness (Wave_Function::get_psi, src/wave_function.cuh:96-105)
@@ -417,17 +488,17 @@ void Engine::run_ew(ConfData& cd) {
         if (m_.is_EWRS()) {
             RowArgs rb = ra;
             if (zbp != 0.0f) {
-                launch_cols(nx, COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cb, 0, stream_);
+                cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cb);
                 rb.in = d_tmp_.p;
                 rb.scale = 1.0f;
             } else {
                 rb.in = d_psi_.p;
-                rb.scale = 1.0f / (float)ny;
+                rb.scale = 1.0f;
             }
             rb.out = d_tmp_.p;
-            launch_rows(ny, ROW_INVERSE, rb, 0, stream_);
+            rows(ROW_INVERSE, rb);
         } else {
-            launch_cols(nx, COL_LOAD | COL_PROP | COL_STORE, cb, 0, stream_);
+            cols(COL_LOAD | COL_PROP | COL_STORE, cb);
         }
         launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
                              d_ew_psi_.p + (size_t)ithk * onxy * 2, sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy,
@@ -575,16 +646,16 @@ void Engine::incident_wave(int space, double* psi) {
     ca.probe = probe_params(Lp.c_c_10, !is_zero_f(f_s));
     ca.out = dpsi.p;
     if (space == 2) {
-        launch_cols(nx, COL_STORE, ca, 0, stream_);
+        cols(COL_STORE, ca);
     } else {
-        launch_cols(nx, COL_INVERSE | COL_STORE, ca, 0, stream_);
+        cols(COL_INVERSE | COL_STORE, ca);
         RowArgs ra{};
         ra.in = dpsi.p;
         ra.out = dpsi.p;
         ra.nx = nx;
         ra.nprobe = nb;
         ra.scale = 1.0f;
-        launch_rows(ny, ROW_INVERSE, ra, 0, stream_);
+        rows(ROW_INVERSE, ra);
     }
     std::vector<float2> h(nxy * nb);
     MTB_CUDA(cudaMemcpyAsync(h.data(), dpsi.p, sizeof(float2) * h.size(), cudaMemcpyDeviceToHost, stream_));

@@ -82,7 +82,23 @@ class Engine {
     cudaStream_t stream() const { return stream_; }
     int batch_size() const { return batch_; }
 
+    // device timing
+    void set_timing(bool on) { timing_ = on; }
+    void timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols);
+
   private:
+    bool timing_ = false;
+    struct TimedLaunch {
+        cudaEvent_t a, b;
+        int kind;  // 0 rows, 1 cols
+    };
+    std::vector<TimedLaunch> tl_;
+    size_t tl_used_ = 0;
+    cudaEvent_t run_a_ = nullptr, run_b_ = nullptr;
+    void tl_begin(int kind);
+    void tl_end();
+    void rows(RowMode mode, const RowArgs& a);
+    void cols(int flags, const ColArgs& a);
     Model m_;
     std::unique_ptr<Specimen> spec_;
     int device_ = 0;
@@ -120,7 +136,7 @@ class Engine {
     void run_conf(ConfData& cd);
     void run_stem(ConfData& cd);
     void run_ew(ConfData& cd);
-    void prop_tables(float dz, float2* px, float2* py) const;
+    void prop_tables(float dz, float2* px, float2* py, bool output) const;
     ProbeDev probe_params(float c_c_10, int nz_c10) const;
     void check_cancel();
     ConfData* find_conf(int iconf);
