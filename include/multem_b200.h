@@ -259,6 +259,14 @@ mt_status mt_propagate(const mt_system_conf* conf, const mt_input_multislice* in
 mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space,
                            double* psi_out);
 
+/* Radial projected-potential spline tables of the elements Z[0..n) built on the GPU in FP64
+ * (Atomic_Data::get_atom_coef, src/atomic_data.hpp:1547-1668, Lobato 0-12, neutral atoms) for a
+ * grid of minimum sampling dR_min and cut-off potential Vrl. heads[4*i..] = R_min, R_max, R_tap,
+ * tap_cf; tab[5*nR*i..] = R2[nR], c0[nR], c1[nR], c2[nR], c3[nR] as float (the tables the
+ * projected-potential splat evaluates). Host buffers. */
+mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
+                           double* heads, float* tab);
+
 /* ---- specimen host logic, exposed for parity checks ---- */
 
 /* Number of atoms kept after validation and the slice count for configuration `iconf`. */

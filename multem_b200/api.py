@@ -184,6 +184,18 @@ def ilc_incident_wave(system_conf, params: Parameters, space: int = 1) -> np.nda
     return (t[0::2] + 1j * t[1::2]).reshape(params.nx, params.ny).T
 
 
+def spline_tables(Z, dR_min: float, Vrl: float = 0.015, nR: int = 128, system_conf=None):
+    """FP64 GPU build of the Lobato spline tables: returns (heads[n, 4], tab[n, 5, nR] float32)."""
+    lib = capi.load()
+    z = np.ascontiguousarray(np.asarray(Z, dtype=np.int32))
+    heads = np.zeros((z.size, 4))
+    tab = np.zeros((z.size, 5, nR), dtype=np.float32)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_spline_tables(C.byref(conf), z.ctypes.data_as(capi.P_int), z.size, float(dR_min), float(Vrl),
+                                    nR, _dp(heads), tab.ctypes.data_as(C.POINTER(C.c_float))))
+    return heads, tab
+
+
 def specimen_atoms(params: Parameters, iconf: int):
     """Displaced z-sorted atoms of configuration iconf (host logic, no GPU)."""
     lib = capi.load()

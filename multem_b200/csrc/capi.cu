@@ -1,5 +1,6 @@
 // extern "C" entry points declared in include/multem_b200.h.
 #include <cstring>
+#include <vector>
 #include <exception>
 #include <memory>
 #include <string>
@@ -201,6 +202,35 @@ mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice
         mt_system_conf c = conf ? *conf : default_conf();
         mtb::Engine e(&c, in);
         e.incident_wave(space, psi_out);
+    });
+}
+
+mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
+                           double* heads, float* tab) {
+    return guarded([&] {
+        if (!Z || n <= 0 || !tab || nR < 2) mtb::fail(MT_ERR_INVALID_ARG, "bad arguments");
+        for (int i = 0; i < n; i++)
+            if (Z[i] < 1 || Z[i] > 103) mtb::fail(MT_ERR_INVALID_ARG, "Z out of range 1..103");
+        const int dev = conf ? conf->gpu_device : 0;
+        MTB_CUDA(cudaSetDevice(dev));
+        cudaStream_t s;
+        MTB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        std::vector<int> zs(Z, Z + n);
+        std::vector<mtb::TableHead> hd;
+        for (int z : zs) hd.push_back(mtb::element_head(z, (float)dR_min, (float)Vrl));
+        mtb::DevBuf<float> d_tab;
+        d_tab.alloc((size_t)n * 5 * nR);
+        mtb::build_tables(zs, hd, nR, d_tab.p, s);
+        MTB_CUDA(cudaMemcpyAsync(tab, d_tab.p, sizeof(float) * (size_t)n * 5 * nR, cudaMemcpyDeviceToHost, s));
+        MTB_CUDA(cudaStreamSynchronize(s));
+        MTB_CUDA(cudaStreamDestroy(s));
+        if (heads)
+            for (int i = 0; i < n; i++) {
+                heads[4 * i] = hd[i].R_min;
+                heads[4 * i + 1] = hd[i].R_max;
+                heads[4 * i + 2] = hd[i].R_tap;
+                heads[4 * i + 3] = hd[i].tap_cf;
+            }
     });
 }
 

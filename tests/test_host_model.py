@@ -1,0 +1,74 @@
+"""Host-side model (validation, phonon displacements, slicing) against the reference's own dumps.
+
+These run without a GPU: the specimen entry points of the C ABI use host code only.
+"""
+import numpy as np
+import pytest
+
+from multem_b200 import api, specimens
+
+
+def cases():
+    p = specimens.stem_srtio3(nx=128, ny=128, na=4, nb=4, nc=4, ns=3, nconf=2, seed=11)
+    p.thick_type = 2
+    p.thick = [4.0, 8.0, 12.0]
+    p.cond_lens_c_10 = 15.0
+    p.cond_lens_c_30 = 0.001
+    return {
+        "stem_small": specimens.stem_srtio3(nx=128, ny=128, na=4, nb=4, nc=4, ns=4, nconf=2, seed=7),
+        "stem_thick": p,
+        "ew_small": specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2),
+        "ew_config1": specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=8),
+    }
+
+
+@pytest.mark.parametrize("name", ["stem_small", "stem_thick", "ew_small", "ew_config1"])
+@pytest.mark.parametrize("iconf", [1, 2])
+def test_displaced_atoms_and_slices_bit_exact(golden, name, iconf):
+    p = cases()[name]
+    if iconf > p.pn_nconf:
+        pytest.skip("single configuration")
+    Z, xyz = api.specimen_atoms(p, iconf)
+    np.testing.assert_array_equal(Z, golden[f"{name}_c{iconf}_Z"])
+    np.testing.assert_array_equal(xyz.astype(np.float32), golden[f"{name}_c{iconf}_xyz"].astype(np.float32))
+    s = api.specimen_slices(p, iconf)
+    for k in ("iatom_0", "iatom_e", "ithk"):
+        np.testing.assert_array_equal(s[k], golden[f"{name}_c{iconf}_{k}"])
+    for k in ("z_0", "z_e"):
+        np.testing.assert_array_equal(s[k].astype(np.float32), golden[f"{name}_c{iconf}_{k}"].astype(np.float32))
+
+
+def test_output_dims_host_only(golden):
+    p = cases()["stem_thick"]
+    d = api.output_dims(p)
+    assert (d.n_thick, d.n_detector, d.nx, d.ny) == (3, 2, 3, 3)
+    assert d.n_x == 9 and d.has_image_tot == 1
+
+
+def test_seed_zero_is_clamped_to_one():
+    """validate_parameters clamps pn_seed to >= 1 (src/input_multislice.cuh:624)."""
+    p0 = specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    p1 = p0.copy()
+    p0.pn_seed, p1.pn_seed = 0, 1
+    np.testing.assert_array_equal(api.specimen_atoms(p0, 1)[1], api.specimen_atoms(p1, 1)[1])
+
+
+def test_configurations_differ_and_repeat():
+    p = cases()["stem_small"]
+    a1, a2 = api.specimen_atoms(p, 1)[1], api.specimen_atoms(p, 2)[1]
+    assert not np.array_equal(a1, a2)
+    np.testing.assert_array_equal(a1, api.specimen_atoms(p, 1)[1])
+    # pn_dim = 110: z untouched
+    np.testing.assert_array_equal(a1[:, 2], a2[:, 2])
+
+
+@pytest.mark.parametrize("field,value,status", [
+    ("simulation_type", 21, 6), ("potential_type", 5, 6), ("potential_slicing", 3, 6), ("nx", 0, 1),
+])
+def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
+    from multem_b200 import capi
+    p = cases()["stem_small"]
+    setattr(p, field, value)
+    with pytest.raises(capi.MtError) as e:
+        api.output_dims(p)
+    assert e.value.status == status
