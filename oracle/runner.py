@@ -28,8 +28,9 @@ def _slices(p, iconf, grid, tabs, w, dtype):
     return Z, xyz, s, Ts, dzs
 
 
-def stem(p, dtype=np.float64):
-    """image_tot[ithk][idet] as (ny, nx) arrays (MATLAB orientation)."""
+def stem(p, dtype=np.float64, confs=None):
+    """image_tot[ithk][idet] as (ny, nx) arrays (MATLAB orientation), summed over the phonon
+    configurations `confs` (default: all), each weighted 1/pn_nconf like the reference."""
     grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)
     Zs = sorted({int(z) % 1000 for z in np.asarray(p.spec_atoms)[:, 0]})
     tabs = {Z: O.atom_table(Z, grid.dRx) for Z in Zs}
@@ -46,7 +47,7 @@ def stem(p, dtype=np.float64):
         (np.float32(p.scanning_xe) - np.float32(p.scanning_x0)) / np.float32(p.scanning_ns if p.scanning_periodic else p.scanning_ns - 1))
     ys = np.float32(p.scanning_y0) + np.arange(out.ny, dtype=np.float32) * np.float32(
         (np.float32(p.scanning_ye) - np.float32(p.scanning_y0)) / np.float32(p.scanning_ns if p.scanning_periodic else p.scanning_ns - 1))
-    for iconf in range(1, nconf + 1):
+    for iconf in (confs if confs is not None else range(1, nconf + 1)):
         Z, xyz, s, Ts, dzs = _slices(p, iconf, grid, tabs, w, dtype)
         thk_slices = {int(k): int(s["ithk"][k]) for k in range(len(s["ithk"])) if s["ithk"][k] >= 0}
         z_init = float(np.float32(0.5 * (np.float64(s["z_0"][0]) + np.float64(s["z_e"][0]))))
