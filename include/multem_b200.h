@@ -267,6 +267,22 @@ mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice
 mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
                            double* heads, float* tab);
 
+/* Allocation-free form of mt_spline_tables; it has no counterpart in the reference. It is for
+ * callers that cannot call cudaMalloc: code running inside a CUDA stream capture, code whose GPU
+ * memory is owned by a framework's pool allocator (a stray cudaMalloc would bypass the pool's budget
+ * or fail), or real-time loops where an allocation is not allowed. The caller passes the output:
+ * d_tab is a device buffer of n*5*nR floats on the current device, laid out as mt_spline_tables'
+ * tab; heads (optional) is a host buffer of 4*n doubles. The only scratch is a fixed 26 KB device
+ * array inside the library (held on every GPU that loads the library until the process exits):
+ * n is limited to 128 elements and nR to 1024, larger requests return MT_ERR_INVALID_ARG. The work
+ * is enqueued on `stream` (a cudaStream_t, NULL for the legacy default stream) and is complete when
+ * that stream is; nothing is allocated and nothing is synchronised. The first call on a device looks
+ * up the scratch array's device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture. Calls share the scratch array: two calls that overlap on
+ * the GPU (different streams or threads on one device) race on it. */
+mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
+                                   float* d_tab, void* stream);
+
 /* ---- specimen host logic, exposed for parity checks ---- */
 
 /* Number of atoms kept after validation and the slice count for configuration `iconf`. */

@@ -121,6 +121,8 @@ SIGNATURES = {
     "mt_incident_wave": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), c_int, P_double]),
     "mt_spline_tables": (c_int, [C.POINTER(MtSystemConf), P_int, c_int, c_double, c_double, c_int, P_double,
                                  C.POINTER(C.c_float)]),
+    "mt_spline_tables_noalloc": (c_int, [P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
+                                         C.c_void_p]),
     "mt_specimen_info": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_int, P_int]),
     "mt_specimen_atoms": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_double, c_int]),
     "mt_specimen_slices": (c_int, [C.POINTER(MtInputMultislice), c_int, P_double, P_double, P_int, P_int, P_int,

@@ -234,6 +234,27 @@ mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, doub
     });
 }
 
+mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
+                                   float* d_tab, void* stream) {
+    return guarded([&] {
+        if (!Z || !d_tab) mtb::fail(MT_ERR_INVALID_ARG, "Z and d_tab must not be NULL");
+        if (n < 1) mtb::fail(MT_ERR_INVALID_ARG, "n must be positive");
+        for (int i = 0; i < n; i++)
+            if (Z[i] < 1 || Z[i] > 103) mtb::fail(MT_ERR_INVALID_ARG, "Z out of range 1..103");
+        std::vector<int> zs(Z, Z + n);
+        std::vector<mtb::TableHead> hd;
+        for (int z : zs) hd.push_back(mtb::element_head(z, (float)dR_min, (float)Vrl));
+        mtb::build_tables_noalloc(zs, hd, nR, d_tab, static_cast<cudaStream_t>(stream));
+        if (heads)
+            for (int i = 0; i < n; i++) {
+                heads[4 * i] = hd[i].R_min;
+                heads[4 * i + 1] = hd[i].R_max;
+                heads[4 * i + 2] = hd[i].R_tap;
+                heads[4 * i + 3] = hd[i].tap_cf;
+            }
+    });
+}
+
 // Host-only parity helpers: no GPU needed.
 namespace {
 struct HostSpec {

@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.hpp"
@@ -232,6 +234,59 @@ void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& head
     MTB_CUDA(cudaStreamSynchronize(stream));
     MTB_CUDA(cudaFreeAsync(d_coef, stream));
     MTB_CUDA(cudaFreeAsync(d_head, stream));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free variant of build_tables.
+//
+// The per-call scratch of build_tables (the element coefficients and table heads the kernel reads)
+// lives here in one file-scope device array instead of memory obtained from cudaMallocAsync. The
+// array is kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead)) bytes (about 26 KB) and is
+// held by every GPU that loads this library until the process exits. All calls share it: each
+// call overwrites the entries it uses before its kernel reads them (nothing has to start at zero),
+// and two calls whose copies and kernels overlap on the GPU (different streams, or different host
+// threads on one device) race on it.
+constexpr int kNoAllocMaxElements = 128;
+static __device__ __align__(256) unsigned char
+    g_noalloc_table_scratch[kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead))];
+
+// Device address of the scratch array on `dev`. Host code may not use the symbol itself (it names
+// a host-side stand-in, not device memory); the address is looked up once per device with that
+// device current and cached.
+static unsigned char* noalloc_scratch_address(int dev) {
+    constexpr int kMaxDevices = 64;
+    static unsigned char* addr[kMaxDevices] = {};
+    static std::mutex mu;
+    if (dev < 0 || dev >= kMaxDevices) fail(MT_ERR_INVALID_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_table_scratch);
+        if (e != cudaSuccess) throw Error(MT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        addr[dev] = static_cast<unsigned char*>(p);
+    }
+    return addr[dev];
+}
+
+void build_tables_noalloc(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
+                          cudaStream_t stream) {
+    const int n = (int)Zs.size();
+    if (n < 1 || n > kNoAllocMaxElements)
+        fail(MT_ERR_INVALID_ARG, "allocation-free table build takes 1.." + std::to_string(kNoAllocMaxElements) +
+                                     " elements, got " + std::to_string(n));
+    if (nR < 2 || nR > 1024) fail(MT_ERR_INVALID_ARG, "nR must be in 2..1024");
+    int dev = 0;
+    MTB_CUDA(cudaGetDevice(&dev));
+    unsigned char* base = noalloc_scratch_address(dev);
+    ElemCoef* d_coef = reinterpret_cast<ElemCoef*>(base);
+    TableHead* d_head = reinterpret_cast<TableHead*>(base + kNoAllocMaxElements * sizeof(ElemCoef));
+    std::vector<ElemCoef> h(n);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i]);
+    // pageable sources: each copy returns once its source has been staged, so the vectors may go
+    MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
+    MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));
+    build_tables_kernel<<<n, 128, 3 * nR * sizeof(double), stream>>>(d_coef, d_head, n, nR, d_tab);
+    MTB_CUDA(cudaGetLastError());
 }
 
 }  // namespace mtb

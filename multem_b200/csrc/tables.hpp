@@ -21,4 +21,10 @@ TableHead element_head(int Z, float dR_min, float Vrl);
 void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
                   cudaStream_t stream);
 
+// Same build without allocating: the kernel's scratch is a fixed file-scope device array (at most
+// 128 elements per call), d_tab is the caller's device buffer, and the work is only enqueued on
+// `stream` (no synchronisation). Calls that overlap on the GPU race on the shared scratch.
+void build_tables_noalloc(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
+                          cudaStream_t stream);
+
 }  // namespace mtb
