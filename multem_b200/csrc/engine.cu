@@ -114,6 +114,9 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     }
     d_psi_.alloc((size_t)batch_ * nxy);
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
+    d_err_.alloc(1);
+    MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
+    pipe_ = env_int("MTB_PIPE", 3);  // bit 0: row pass, bit 1: column pass
     reset();
 }
 
@@ -130,7 +133,17 @@ Engine::~Engine() {
     }
 }
 
-void Engine::synchronize() { MTB_CUDA(cudaStreamSynchronize(stream_)); }
+void Engine::synchronize() {
+    MTB_CUDA(cudaStreamSynchronize(stream_));
+    if (d_err_.p) {
+        int e = 0;
+        MTB_CUDA(cudaMemcpy(&e, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            MTB_CUDA(cudaMemset(d_err_.p, 0, sizeof(int)));
+            fail(MT_ERR_TIMEOUT, "a line pass timed out waiting for its bulk copies; results are invalid");
+        }
+    }
+}
 
 void Engine::reset() {
     if (d_image_.p) MTB_CUDA(cudaMemsetAsync(d_image_.p, 0, sizeof(double) * d_image_.n, stream_));
@@ -323,15 +336,20 @@ void Engine::tl_end() {
     tl_used_++;
 }
 
+// Passes get the engine's error flag, which selects the bulk-copy-fed kernels where they fit.
 void Engine::rows(RowMode mode, const RowArgs& a) {
+    RowArgs b = a;
+    b.err = (pipe_ & 1) ? d_err_.p : nullptr;
     tl_begin(0);
-    launch_rows(m_.grid.ny, mode, a, 0, stream_);
+    launch_rows(m_.grid.ny, mode, b, 0, stream_);
     tl_end();
 }
 
 void Engine::cols(int flags, const ColArgs& a) {
+    ColArgs b = a;
+    b.err = (pipe_ & 2) ? d_err_.p : nullptr;
     tl_begin(1);
-    launch_cols(m_.grid.nx, flags, a, 0, stream_);
+    launch_cols(m_.grid.nx, flags, b, 0, stream_);
     tl_end();
 }
 
@@ -409,6 +427,7 @@ void Engine::run_stem(ConfData& cd) {
     }
     ca.gx_0 = 0;
     ca.gy_0 = 0;
+    ca.det_w = col_det_width(nx);
     RowArgs ra{};
     ra.nx = nx;
     ra.scale = 1.0f;

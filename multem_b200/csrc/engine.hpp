@@ -117,6 +117,8 @@ class Engine {
 
     // wave state
     int batch_ = 1;
+    DevBuf<int> d_err_;              // set by a line pass whose bounded wait gave up
+    int pipe_ = 3;                   // bulk-copy-fed line passes where they fit (bit 0 rows, bit 1 cols)
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;
     DevBuf<float2> d_tmp_;

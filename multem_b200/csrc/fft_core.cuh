@@ -181,18 +181,20 @@ __device__ __forceinline__ void dft(float2* v) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Line plans: N points, E points per thread, radices of the forward transform in stage order.
-// The inverse uses the same radices reversed (see the header comment).
+// Line plans: N points, E points per thread, T threads per CTA (per group, in the pipelined
+// passes) of the line passes, B resident CTAs per SM the per-thread-load kernels are compiled for
+// (caps registers at 65536 / (B*T)), radices of the forward transform in stage order. The inverse
+// uses the same radices reversed (see the header comment).
 
 template <int N>
 struct LinePlan;
 
-template <> struct LinePlan<64>   { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 4, 1}; };
-template <> struct LinePlan<128>  { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 8, 1}; };
-template <> struct LinePlan<256>  { static constexpr int E = 16; static constexpr int NS = 2; static constexpr int R[3] = {16, 16, 1}; };
-template <> struct LinePlan<512>  { static constexpr int E = 32; static constexpr int NS = 2; static constexpr int R[3] = {32, 16, 1}; };
-template <> struct LinePlan<1024> { static constexpr int E = 32; static constexpr int NS = 2; static constexpr int R[3] = {32, 32, 1}; };
-template <> struct LinePlan<2048> { static constexpr int E = 32; static constexpr int NS = 3; static constexpr int R[3] = {32, 8, 8}; };
+template <> struct LinePlan<64>   { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 4, 1}; };
+template <> struct LinePlan<128>  { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 8, 1}; };
+template <> struct LinePlan<256>  { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 16, 1}; };
+template <> struct LinePlan<512>  { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 16, 1}; };
+template <> struct LinePlan<1024> { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 32, 1}; };
+template <> struct LinePlan<2048> { static constexpr int E = 32, T = 256, B = 2, NS = 3; static constexpr int R[3] = {32, 8, 8}; };
 
 // Radix of stage s of a transform whose stage order is `rev` ? reversed : plan order.
 template <int N, bool REV, int S>
@@ -295,6 +297,89 @@ __device__ __forceinline__ void stage_exchange(float2* x, float2* buf, int t, Sy
 #pragma unroll
         for (int r = 0; r < R2; ++r) x[m * R2 + r] = buf[pad_idx<R>(j + r * (N / R2))];
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Half-line exchange: the same permutation through a buffer of N/2 positions, in two rounds.
+//
+// For a two-stage plan the first stage (Ns = 1, radix R) writes position p = (t + TPL*m)*R + r
+// and the second (radix R2) reads p = t + TPL*m' + r'*N/R2. A position bit B >= log2(TPL) that
+// the writer fixes through (m, r) alone is fixed for the reader through (m', r') alone too, so
+// round h moves exactly the positions whose bit B is h, with compile-time register selection
+// on both sides. B exists when R > TPL (B = log2 TPL, a bit of r) or E/R >= 2 (B = log2(R*TPL),
+// a bit of m); it does not for plans with R = TPL and E = R (256 and 1024 here).
+
+constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v / 2); }
+
+template <int N, bool REV>
+struct HalfExchange {
+    static constexpr int E = LinePlan<N>::E;
+    static constexpr int TPL = N / E;
+    static constexpr int R = StageRadix<N, REV, 0>::value;
+    static constexpr int R2 = StageRadix<N, REV, 1>::value;
+    static constexpr int LT = ilog2c(TPL), LR = ilog2c(R);
+    static constexpr int B = (LinePlan<N>::NS != 2) ? -1 : (LR > LT) ? LT : ((E / R >= 2) ? LR + LT : -1);
+    // thread stride of the writer's positions after removing bit B; padding by it keeps the
+    // writes of consecutive threads on distinct banks
+    static constexpr int PADW = (B >= 0 && B < LR) ? R / 2 : R;
+    // round 1 writes must not read registers that round 0's reads already replaced
+    static constexpr bool disjoint() {
+        if (B < 0) return false;
+        const int sb = B < 0 ? 0 : B;
+        for (int i = 0; i < E; i++) {
+            const int mw = i / R, rw = i % R;  // writer register i
+            const int mr = i / R2, rr = i % R2;  // reader register i
+            const bool w1 = ((TPL * mw * R + rw) >> sb) & 1;
+            const bool r0 = !(((TPL * mr + rr * (N / R2)) >> sb) & 1);
+            if (w1 && r0) return false;
+        }
+        return true;
+    }
+    static constexpr bool OK = (B >= 0) && disjoint();
+};
+
+template <int B>
+__device__ __forceinline__ int drop_bit(int p) {
+    return (p & ((1 << B) - 1)) | ((p >> (B + 1)) << B);
+}
+
+// Line buffer length (float2) for the half-line exchange: N/2 positions padded by the smallest
+// PADW of the plan (>= RMIN/2), odd.
+template <int N>
+struct HalfLineSmem {
+    static constexpr int RMIN = (LinePlan<N>::R[0] < LinePlan<N>::R[1]) ? LinePlan<N>::R[0] : LinePlan<N>::R[1];
+    static constexpr int value = N / 2 + N / RMIN + 1;
+};
+
+template <int N, bool REV, class Sync>
+__device__ __forceinline__ void stage_exchange_half(float2* x, float2* buf, int t, Sync sync) {
+    using H = HalfExchange<N, REV>;
+    constexpr int E = H::E, TPL = H::TPL, R = H::R, R2 = H::R2, B = H::B, PW = H::PADW;
+    static_assert(H::OK, "plan has no half-line exchange");
+    static_for<0, 2>([&](auto hc) {
+        constexpr int h = decltype(hc)::value;
+        sync();
+        static_for<0, E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int cpos = TPL * (i / R) * R + (i % R);  // writer position less t*R
+            if constexpr (((cpos >> B) & 1) == h) buf[pad_idx<PW>(drop_bit<B>(t * R + cpos))] = x[i];
+        });
+        sync();
+        static_for<0, E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            constexpr int cpos = TPL * (i / R2) + (i % R2) * (N / R2);  // reader position less t
+            if constexpr (((cpos >> B) & 1) == h) x[i] = buf[pad_idx<PW>(drop_bit<B>(t + cpos))];
+        });
+    });
+}
+
+// Two-stage transform with the half-line exchange (see line_fft below).
+template <int N, bool REV, int DIR, class Sync>
+__device__ __forceinline__ void line_fft_half(float2* x, float2* buf, const float2* const* tw, int t, Sync sync) {
+    static_assert(LinePlan<N>::NS == 2, "half-line exchange needs a two-stage plan");
+    stage_compute<N, REV, 0, DIR>(x, t, tw[0]);
+    stage_exchange_half<N, REV>(x, buf, t, sync);
+    stage_compute<N, REV, 1, DIR>(x, t, tw[1]);
 }
 
 // Full transform: x holds the first stage's inputs (positions j + r*N/R_first); on return it

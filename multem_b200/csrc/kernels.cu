@@ -10,6 +10,8 @@
 // because F = F_x F_y and the two 1-D transforms commute. The annular-detector sums of the
 // reference's get_psi + sum_square_over_Det (src/wave_function.cuh:96-155) are taken inside the
 // column pass right after the P multiply, where the registers hold FFT2(psi)/N.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -24,6 +26,26 @@ namespace mtb {
 static std::atomic<long long> g_launches{0};
 long long launches_issued() { return g_launches.load(); }
 void note_launch() { g_launches++; }
+
+void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        MTB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    // float32 [nprobe][nx][2*ldy]; box: 2w floats (w complex columns) x boxr rows x 1 probe
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * ldy, (cuuint64_t)nx, (cuuint64_t)nprobe};
+    const cuuint64_t strides[2] = {(cuuint64_t)2 * ldy * sizeof(float), (cuuint64_t)2 * ldy * nx * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * w), (cuuint32_t)boxr, 1};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides, box,
+                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the column-pass tile map");
+}
 
 // =============================================================================================
 // Projected potential splat fused with the transmission function.
@@ -202,22 +224,48 @@ void rows_dispatch_mode(RowMode mode, const RowArgs& a, int grid_ctas, cudaStrea
 template <int NX>
 void cols_dispatch_flags(int flags, const ColArgs& a, int grid_ctas, cudaStream_t s);
 
-int col_tiles(int nx, int ny) {
-    int tpl = 0;
-    switch (nx) {
-        case 64: tpl = 64 / LinePlan<64>::E; break;
-        case 128: tpl = 128 / LinePlan<128>::E; break;
-        case 256: tpl = 256 / LinePlan<256>::E; break;
-        case 512: tpl = 512 / LinePlan<512>::E; break;
-        case 1024: tpl = 1024 / LinePlan<1024>::E; break;
-        case 2048: tpl = 2048 / LinePlan<2048>::E; break;
-        default: fail(MT_ERR_UNSUPPORTED, "unsupported nx");
+template <int N>
+constexpr int lines_per_cta() {
+    return LinePlan<N>::T / (N / LinePlan<N>::E);
+}
+
+static int lines_per_cta(int n) {
+    switch (n) {
+        case 64: return lines_per_cta<64>();
+        case 128: return lines_per_cta<128>();
+        case 256: return lines_per_cta<256>();
+        case 512: return lines_per_cta<512>();
+        case 1024: return lines_per_cta<1024>();
+        case 2048: return lines_per_cta<2048>();
+        default: fail(MT_ERR_UNSUPPORTED, "grid sizes must be one of 64, 128, 256, 512, 1024, 2048");
     }
-    return ny / (256 / tpl);
+    return 0;
+}
+
+template <int NX>
+int cols_det_width();
+
+int col_det_width(int nx) {
+    switch (nx) {
+        case 64: return cols_det_width<64>();
+        case 128: return cols_det_width<128>();
+        case 256: return cols_det_width<256>();
+        case 512: return cols_det_width<512>();
+        case 1024: return cols_det_width<1024>();
+        case 2048: return cols_det_width<2048>();
+        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 512, 1024, 2048");
+    }
+    return 0;
+}
+
+int col_tiles(int nx, int ny) {
+    const int w = col_det_width(nx);
+    if (ny % w != 0) fail(MT_ERR_UNSUPPORTED, "ny must be a multiple of the column-pass tile width");
+    return ny / w;
 }
 
 void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s) {
-    if (a.nx % 256 != 0 && a.nx % 16 != 0) fail(MT_ERR_UNSUPPORTED, "nx must be a multiple of 16");
+    if (a.nx % lines_per_cta(ny) != 0) fail(MT_ERR_UNSUPPORTED, "nx must be a multiple of the row-pass line group");
     switch (ny) {
         case 64: rows_dispatch_mode<64>(mode, a, grid_ctas, s); break;
         case 128: rows_dispatch_mode<128>(mode, a, grid_ctas, s); break;
@@ -230,6 +278,7 @@ void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStre
 }
 
 void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_t s) {
+    if (a.ny % lines_per_cta(nx) != 0) fail(MT_ERR_UNSUPPORTED, "ny must be a multiple of the column-pass tile width");
     switch (nx) {
         case 64: cols_dispatch_flags<64>(flags, a, grid_ctas, s); break;
         case 128: cols_dispatch_flags<128>(flags, a, grid_ctas, s); break;

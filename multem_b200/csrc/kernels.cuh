@@ -47,6 +47,7 @@ struct RowArgs {
     int nx;                // lines per probe
     int nprobe;
     float scale;
+    int* err;              // device flag, set when a bounded wait inside the pass gives up
 };
 void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s);
 
@@ -85,10 +86,13 @@ struct ColArgs {
     int n_det;
     float det_g2_min[kMaxDet], det_g2_max[kMaxDet];
     float gx_0, gy_0;
-    double* det_partial;       // [nprobe][n_tiles][n_det]
+    double* det_partial;       // [nprobe][ny / det_w][n_det]
+    int det_w;                 // columns per detector partial (col_det_width)
+    int* err;                  // device flag, set when a bounded wait inside the pass gives up
 };
 void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_t s);
-int col_tiles(int nx, int ny);  // column tiles per probe (partials per probe per detector)
+int col_det_width(int nx);      // columns per detector partial
+int col_tiles(int nx, int ny);  // detector partials per probe per detector (ny / col_det_width)
 
 // Sum detector partials over tiles and add w * sum into image[(idet*n_scan) + scan_index].
 void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det, const int* scan_index,

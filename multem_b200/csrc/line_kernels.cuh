@@ -3,6 +3,7 @@
 // parallelises; kernels.cu dispatches on the runtime size.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -26,6 +27,8 @@ template <int N>
 struct LineGeom {
     static constexpr int E = LinePlan<N>::E;
     static constexpr int TPL = N / E;
+    static constexpr int THREADS = LinePlan<N>::T;  // threads per CTA (per group when pipelined)
+    static constexpr int LPC = THREADS / TPL;       // lines per CTA (per group)
     static constexpr int NSG = LinePlan<N>::NS;
     static constexpr int R1 = LinePlan<N>::R[0];
     static constexpr int RL = LinePlan<N>::R[NSG - 1];
@@ -54,6 +57,7 @@ __device__ __forceinline__ void setup_twiddles(float2* base, const float2** twI,
 }
 
 struct WarpSync {
+    int grp = 0;  // unused; lets the pipelined kernels construct either barrier from the group index
     __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
 struct BlockSync {
@@ -61,11 +65,12 @@ struct BlockSync {
 };
 
 // ---------------------------------------------------------------------------------------------
-// Contiguous-line pass. 256 threads; each line of NY points is owned by TPL = NY/E threads.
+// Contiguous-line pass. LinePlan<NY>::T threads; each line of NY points is owned by TPL = NY/E
+// threads.
 template <int NY, int MODE>
-__global__ void __launch_bounds__(256) rows_kernel(RowArgs a) {
+__global__ void __launch_bounds__(LineGeom<NY>::THREADS, LinePlan<NY>::B) rows_kernel(RowArgs a) {
     using G = LineGeom<NY>;
-    constexpr int E = G::E, TPL = G::TPL, LPC = 256 / TPL;
+    constexpr int E = G::E, TPL = G::TPL, LPC = G::LPC;
     extern __shared__ float2 smem2[];
     const float2* twI[3] = {nullptr, nullptr, nullptr};
     const float2* twF[3] = {nullptr, nullptr, nullptr};
@@ -112,12 +117,12 @@ __global__ void __launch_bounds__(256) rows_kernel(RowArgs a) {
 template <int NY>
 static size_t rows_smem() {
     using G = LineGeom<NY>;
-    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + (256 / G::TPL) * G::LS);
+    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + G::LPC * G::LS);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Strided-line pass. 256 threads; W = 256/TPL adjacent columns per CTA (coalesced rows of W
-// complex values); column c is owned by threads c, c+W, c+2W, ...
+// Strided-line pass. LinePlan<NX>::T threads; W = T/TPL adjacent columns per CTA (coalesced rows
+// of W complex values); column c is owned by threads c, c+W, c+2W, ...
 __device__ __forceinline__ int ig_shift(int i, int nh, int n) { return (i < nh) ? i : (i - n); }
 
 // exp_i_chi (src/cgpu_fcns.cuh:1951-1980) for one Fourier-space pixel, times the normalisation.
@@ -155,11 +160,26 @@ __device__ __forceinline__ float2 probe_value(const ProbeDev& pr, const GridDev&
     return make_float2(__fmul_rn(cs, pr.norm), __fmul_rn(sn, pr.norm));
 }
 
+// Detector partials are kept per det_w columns (ColArgs::det_w, the narrowest tile width of the
+// column kernels for this size): a tile of W >= det_w columns starting at column iy0 writes its
+// sum to the first of its W/det_w partials and zero to the others.
+template <class Sum>
+__device__ __forceinline__ void write_det_partials(const ColArgs& a, int b, int iy0, int W, int tid, int nthreads,
+                                                   Sum sum) {
+    const int nsub = W / a.det_w;
+    const int det_tiles = a.ny / a.det_w;
+    const size_t base = ((size_t)b * det_tiles + iy0 / a.det_w) * a.n_det;
+    for (int i = tid; i < nsub * a.n_det; i += nthreads) {
+        const int sub = i / a.n_det, d = i % a.n_det;
+        a.det_partial[base + (size_t)sub * a.n_det + d] = (sub == 0) ? sum(d) : 0.0;
+    }
+}
+
 // LDY is the line stride (= ny) when known at compile time (square grids), 0 for a runtime stride.
 template <int NX, int FLAGS, int LDY>
-__global__ void __launch_bounds__(256) cols_kernel(ColArgs a) {
+__global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_kernel(ColArgs a) {
     using G = LineGeom<NX>;
-    constexpr int E = G::E, TPL = G::TPL, W = 256 / TPL;
+    constexpr int E = G::E, W = G::LPC, NWARP = G::THREADS / 32;
     constexpr bool LOAD = FLAGS & COL_LOAD, PROP = FLAGS & COL_PROP, DET = FLAGS & COL_DETECT;
     constexpr bool INV = FLAGS & COL_INVERSE, STORE = FLAGS & COL_STORE;
     extern __shared__ float2 smem2[];
@@ -183,7 +203,7 @@ __global__ void __launch_bounds__(256) cols_kernel(ColArgs a) {
     }
     float2* s_px = smem2 + G::TW_I + G::TW_F;
     float2* lines = s_px + (PROP ? NX : 0);
-    __shared__ double s_red[8][kMaxDet];
+    __shared__ double s_red[NWARP][kMaxDet];
     if constexpr (PROP) {
         for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
     }
@@ -242,11 +262,11 @@ __global__ void __launch_bounds__(256) cols_kernel(ColArgs a) {
                 if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5][d] = v;
             }
             __syncthreads();
-            if (threadIdx.x < a.n_det) {
+            write_det_partials(a, b, ct * W, W, threadIdx.x, G::THREADS, [&](int d) {
                 double s = 0.0;
-                for (int w = 0; w < 8; w++) s += s_red[w][threadIdx.x];
-                a.det_partial[((size_t)b * tiles + ct) * a.n_det + threadIdx.x] = s;
-            }
+                for (int w = 0; w < NWARP; w++) s += s_red[w][d];
+                return s;
+            });
             __syncthreads();
         }
         if constexpr (INV) {
@@ -264,13 +284,394 @@ template <int NX, int FLAGS>
 static size_t cols_smem() {
     using G = LineGeom<NX>;
     constexpr bool PROP = FLAGS & COL_PROP;
-    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + (PROP ? NX : 0) + (256 / G::TPL) * G::LS);
+    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + (PROP ? NX : 0) + G::LPC * G::LS);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Bulk-copy-fed line passes.
+//
+// One CTA per SM with two groups of T threads; group g transforms the CTA's items k = g, g+2,
+// g+4, ... (line groups of the row pass, column tiles of the column pass). Each group owns a
+// landing buffer in shared memory that the copy engine fills with the input lines of its next
+// item (cp.async.bulk for the contiguous lines of the row pass, a 3-D tensor copy for the
+// strided tile of the column pass; completion on mbarrier full[g], the group's j-th item being
+// that barrier's phase j). A group waits for its landing buffer, reads it into registers,
+// synchronises its own threads on a named barrier and issues the copy of its item k+2 into the
+// same buffer before it transforms item k, so each SM keeps two items' reads in flight while
+// both groups compute, and no thread waits on a global load of the wave. The exchanges between
+// the two radix stages go through a per-group half-line buffer in two rounds
+// (stage_exchange_half), which is what makes two landing buffers fit. Results are stored
+// straight from registers.
+
+constexpr unsigned long long kWaitLimitNs = 4000000000ull;  // bounded waits: 4 s, then error flag
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the phase with the given parity; after kWaitLimitNs record an error and go on (the
+// pass's results are then invalid and the host reports the error).
+__device__ __forceinline__ void mbar_wait(unsigned long long* bar, unsigned parity, int* err) {
+    if (mbar_try_wait(bar, parity)) return;
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 1; it < (1u << 30); it++) {
+        if (mbar_try_wait(bar, parity)) return;
+        if ((it & 63u) == 0 && global_ns() - t0 > kWaitLimitNs) break;
+    }
+    atomicOr(err, 1);
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// 3-D tile copy (no multicast) of the box at (x, y, z) described by the tensor map.
+__device__ __forceinline__ void tensor_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                               unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Barrier over the T threads of group `grp` (named barrier 1 + grp; barrier 15 is the row pass's
+// CTA-wide barrier).
+template <int T>
+struct GroupSync {
+    int grp;
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(T) : "memory"); }
+};
+
+constexpr size_t kPipeSmemMax = 232448 - 2048;  // opt-in shared memory per CTA less static use
+
+
+// Row pass, bulk-copy fed, with the transmission rows resident in shared memory.
+//
+// The transmission function is the same for every probe, so a CTA takes a contiguous range of
+// (line group, probe) items in line-group-major order, in units of NG items that never straddle
+// a line group (nprobe % NG == 0): the CTA's NG groups of GT threads always work on the same
+// line group g, and its LPC = GT/TPL transmission rows stay in shared memory (one bulk copy per
+// change of g, after every group has finished with the previous rows). Group x transforms the
+// items k = x, x+NG, ... from its own landing slot (mbarrier full[x], the group's j-th item being
+// its phase j). With EARLY, the group issues the copy of its next item as soon as it has read
+// the slot, and exchanges through its own half-line buffer (stage_exchange_half); otherwise the
+// slot, sized for the full exchange buffer, serves as the exchange buffer and the next copy is
+// issued once the forward transform's exchange has been read back.
+template <int NY, int GT, int NG, bool EARLY>
+struct RowPipe {
+    using G = LineGeom<NY>;
+    static constexpr int TPL = G::TPL;
+    static constexpr int LPC = GT / TPL;
+    static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
+    static constexpr size_t LAND = (size_t)LPC * NY;
+    static constexpr size_t SLOT = EARLY ? LAND : ((size_t)LPC * G::LS > LAND ? (size_t)LPC * G::LS : LAND);
+    static constexpr size_t HBUF = EARLY ? (size_t)LPC * HalfLineSmem<NY>::value : 0;
+    static constexpr size_t SMEM = sizeof(float2) * (TW + LAND + NG * SLOT + NG * HBUF);
+    static constexpr bool OK = (GT % TPL == 0) && (GT % 32 == 0) && (SLOT % 2 == 0) && (HBUF % 2 == 0) &&
+                               SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14) &&
+                               (!EARLY || (HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK));
+};
+
+template <int NY, int MODE, int GT, int NG, bool EARLY>
+__global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
+    using G = LineGeom<NY>;
+    using P = RowPipe<NY, GT, NG, EARLY>;
+    constexpr int E = G::E, TPL = G::TPL, LPC = P::LPC;
+    static_assert(MODE == ROW_STEP || MODE == ROW_INVERSE || MODE == ROW_FIRST_REAL, "mode without a load");
+    constexpr bool TRANS = MODE != ROW_INVERSE;
+    constexpr unsigned LINE_BYTES = NY * sizeof(float2);
+    extern __shared__ __align__(1024) unsigned char pipe_smem[];
+    __shared__ unsigned long long full[NG], tbar;
+    float2* sm = reinterpret_cast<float2*>(pipe_smem);
+    const float2* twI[3] = {nullptr, nullptr, nullptr};
+    const float2* twF[3] = {nullptr, nullptr, nullptr};
+    setup_twiddles<NY>(sm, twI, twF);
+    float2* s_trans = sm + P::TW;  // [LPC][NY]
+    float2* slots = s_trans + P::LAND;
+    const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
+    const int li = gtid / TPL, t = gtid % TPL;
+    float2* slot = slots + grp * P::SLOT;
+    float2* buf = EARLY ? slots + NG * P::SLOT + grp * P::HBUF + (size_t)li * HalfLineSmem<NY>::value
+                        : slot + (size_t)li * G::LS;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
+        mbar_init(&tbar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // this CTA's items: [i0, i0 + K), item = g * nprobe + b, in units of NG
+    const long long units = (long long)a.nx / LPC * a.nprobe / NG;
+    const long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+    const long long i0 = NG * u0;
+    const int K = (int)(NG * (u1 - u0));
+    // issued by a whole warp: item k's LPC lines into slot k % NG
+    auto issue = [&](int k, int lane) {
+        const long long item = i0 + k;
+        const int g = (int)(item / a.nprobe), b = (int)(item % a.nprobe);
+        const float2* src = a.in + ((size_t)b * a.nx + (size_t)g * LPC) * NY;
+        unsigned long long* bar = &full[k % NG];
+        float2* dst = slots + (k % NG) * P::SLOT;
+        if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(bar, LPC * LINE_BYTES);
+        }
+        __syncwarp();
+        for (int l = lane; l < LPC; l += 32) bulk_load(dst + (size_t)l * NY, src + (size_t)l * NY, LINE_BYTES, bar);
+    };
+    // issued by warp 0: the transmission rows of line group g
+    auto issue_trans = [&](int g, int lane) {
+        const float2* src = a.trans + (size_t)g * LPC * NY;
+        if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(&tbar, LPC * LINE_BYTES);
+        }
+        __syncwarp();
+        for (int l = lane; l < LPC; l += 32) bulk_load(s_trans + (size_t)l * NY, src + (size_t)l * NY, LINE_BYTES, &tbar);
+    };
+    if (gtid < 32 && grp < K) issue(grp, gtid);
+    int g_cur = K > 0 ? (int)(i0 / a.nprobe) : 0;
+    unsigned tphase = 0;
+    if constexpr (TRANS) {
+        if (threadIdx.x < 32 && K > 0) issue_trans(g_cur, threadIdx.x);
+    }
+
+    using Sync = typename std::conditional<(TPL <= 32), WarpSync, GroupSync<GT>>::type;
+    using GSync = typename std::conditional<(GT == 32), WarpSync, GroupSync<GT>>::type;
+    const GSync gsync{grp};
+    for (int k = grp; k < K; k += NG) {
+        const long long item = i0 + k;
+        const int g = (int)(item / a.nprobe), b = (int)(item % a.nprobe);
+        if constexpr (TRANS) {
+            if (g != g_cur) {
+                // every group reaches this point at the first unit of the new line group, after
+                // finishing its last item of the old one
+                asm volatile("bar.sync 15, %0;" ::"r"(NG * GT) : "memory");
+                if (threadIdx.x < 32) issue_trans(g, threadIdx.x);
+                g_cur = g;
+                tphase ^= 1u;
+            }
+        }
+        const int ix = g * LPC + li;
+        const size_t off = ((size_t)b * a.nx + ix) * NY;
+        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err);
+        const float2* lsrc = slot + (size_t)li * NY;
+        float2 x[E];
+        if constexpr (MODE == ROW_FIRST_REAL) {
+#pragma unroll
+            for (int i = 0; i < E; i++) x[i] = lsrc[reg_pos<NY, G::RL>(i, t)];
+        } else {
+#pragma unroll
+            for (int i = 0; i < E; i++) x[i] = lsrc[reg_pos<NY, G::R1>(i, t)];
+        }
+        gsync();  // the slot's lines are in registers
+        if constexpr (EARLY) {
+            if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
+        }
+        if constexpr (MODE == ROW_STEP || MODE == ROW_INVERSE) {
+            if constexpr (EARLY) line_fft_half<NY, false, +1>(x, buf, twI, t, Sync{grp});
+            else line_fft<NY, false, +1>(x, buf, twI, t, Sync{grp});
+        }
+        if constexpr (MODE == ROW_INVERSE) {
+            if constexpr (!EARLY) {
+                gsync();
+                if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
+            }
+#pragma unroll
+            for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::RL>(i, t)] = cscale(x[i], a.scale);
+        } else {
+            mbar_wait(&tbar, tphase, a.err);
+            const float2* Tr = s_trans + (size_t)li * NY;
+#pragma unroll
+            for (int i = 0; i < E; i++) x[i] = cmul(x[i], Tr[reg_pos<NY, G::RL>(i, t)]);
+            if constexpr (EARLY) {
+                line_fft_half<NY, true, -1>(x, buf, twF, t, Sync{grp});
+            } else {
+                line_fft<NY, true, -1>(x, buf, twF, t, Sync{grp});
+                gsync();  // every exchange read of the slot is done
+                if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
+            }
+#pragma unroll
+            for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::R1>(i, t)] = x[i];
+        }
+    }
+}
+
+// Row-pass pipeline shape per line length: threads per group, groups, early issue (where the
+// plan has a half-line exchange).
+template <int NY>
+struct RowPipeShape {
+    static constexpr int GT = 64, NG = 8;
+    static constexpr bool EARLY = HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK;
+};
+
+// Column pass, bulk-copy fed: NG groups of GT threads, W = GT/TPL columns per tile. The tensor
+// map describes the probe batch as float32 [nprobe][NX][2*ldy] (re, im interleaved) with a box
+// of 2W x BOXR x 1: one box is BOXR rows of a W-column tile, landing as [row][W]. Group x
+// transforms the items k = x, x+NG, ... of the CTA (item = blockIdx.x + k*gridDim.x) from its
+// own landing buffer, issues the copy of its next item as soon as it has read the buffer, and
+// exchanges through its own half-line buffers.
+template <int NX, int GT, int NG>
+struct ColPipe {
+    using G = LineGeom<NX>;
+    static constexpr int W = GT / G::TPL;
+    static constexpr int LSH = HalfLineSmem<NX>::value;
+    static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
+    static constexpr size_t LAND = (size_t)W * NX;
+    static constexpr size_t HBUF = (size_t)W * LSH;
+    static constexpr size_t SMEM = sizeof(float2) * (TW + NX + NG * LAND + NG * HBUF);
+    static constexpr int BOXR = NX < 256 ? NX : 256;
+    static constexpr bool OK = HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK && (GT % G::TPL == 0) &&
+                               (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) && (HBUF % 2 == 0) &&
+                               SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
+};
+
+template <int NX>
+struct ColPipeShape {
+    static constexpr int GT = 256, NG = 2;
+};
+
+template <int NX, int FLAGS, int LDY, int GT, int NG>
+__global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const __grid_constant__ CUtensorMap map) {
+    using G = LineGeom<NX>;
+    using P = ColPipe<NX, GT, NG>;
+    constexpr int E = G::E, W = P::W, NWARP = GT / 32;
+    constexpr bool PROP = FLAGS & COL_PROP, DET = FLAGS & COL_DETECT;
+    constexpr bool INV = FLAGS & COL_INVERSE, STORE = FLAGS & COL_STORE;
+    static_assert(FLAGS & COL_LOAD, "column pass without a load");
+    constexpr unsigned TILE_BYTES = NX * W * sizeof(float2);
+    extern __shared__ __align__(1024) unsigned char pipe_smem[];
+    __shared__ unsigned long long full[NG];
+    __shared__ double s_red[NG][NWARP][kMaxDet];
+    float2* sm = reinterpret_cast<float2*>(pipe_smem);
+    const float2* twP[3] = {nullptr, nullptr, nullptr};  // plan order: the forward transform here
+    const float2* twR[3] = {nullptr, nullptr, nullptr};  // reversed order: the inverse transform
+    setup_twiddles<NX>(sm, twP, twR);
+    float2* s_px = sm + P::TW;
+    float2* land0 = s_px + NX;  // NG landing buffers, [row][W] each
+    const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
+    const int c = gtid % W, t = gtid / W;
+    const float2* land = land0 + grp * P::LAND;
+    float2* buf = land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH;
+    if constexpr (PROP) {
+        for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    const int ldy = LDY ? LDY : a.ny;
+    const int tiles = ldy / W;
+    const int items = tiles * a.nprobe;
+    const size_t pstride = (size_t)NX * ldy;
+    const int K = (int)blockIdx.x < items ? (items - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    // issued by one thread: item k's tile into landing buffer k % NG
+    auto issue = [&](int k) {
+        const int item = blockIdx.x + k * gridDim.x;
+        unsigned long long* bar = &full[k % NG];
+        float2* dst = land0 + (k % NG) * P::LAND;
+        fence_proxy_async();
+        mbar_expect_tx(bar, TILE_BYTES);
+#pragma unroll
+        for (int r0 = 0; r0 < NX; r0 += P::BOXR)
+            tensor_load_3d(dst + (size_t)r0 * W, &map, (item % tiles) * 2 * W, r0, item / tiles, bar);
+    };
+    if (gtid == 0 && grp < K) issue(grp);
+
+    using GSync = typename std::conditional<(GT == 32), WarpSync, GroupSync<GT>>::type;
+    const GSync gsync{grp};
+    for (int k = grp; k < K; k += NG) {
+        const int item = blockIdx.x + k * gridDim.x;
+        const int b = item / tiles, ct = item % tiles;
+        const int iy = ct * W + c;
+        const size_t off = (size_t)b * pstride + iy + (size_t)t * ldy;
+        float2* dst = a.out + off;
+        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err);
+        float2 x[E];
+#pragma unroll
+        for (int i = 0; i < E; i++) x[i] = land[(size_t)reg_pos<NX, G::R1>(i, t) * W + c];
+        gsync();  // the whole group has read its landing buffer
+        if (gtid == 0 && k + NG < K) issue(k + NG);
+        line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
+        if constexpr (PROP) {
+            const float2 py = a.Py[iy];
+#pragma unroll
+            for (int i = 0; i < E; i++) x[i] = cmul(x[i], cmul(s_px[reg_pos<NX, G::RL>(i, t)], py));
+        }
+        if constexpr (DET) {
+            double acc[kMaxDet];
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
+            const float gy = __fsub_rn(__fmul_rn((float)ig_shift(iy, a.g.nyh, a.g.ny), a.g.dgy), 0.0f);
+            const float gy2 = __fmul_rn(gy, gy);
+#pragma unroll
+            for (int i = 0; i < E; i++) {
+                const int ix = reg_pos<NX, G::RL>(i, t);
+                const float gx = __fmul_rn((float)ig_shift(ix, a.g.nxh, a.g.nx), a.g.dgx);
+                const float g2 = __fadd_rn(__fmul_rn(gx, gx), gy2);
+                const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
+#pragma unroll
+                for (int d = 0; d < kMaxDet; d++)
+                    if (d < a.n_det && a.det_g2_min[d] <= g2 && g2 < a.det_g2_max[d]) acc[d] += (double)v2;
+            }
+            // deterministic group reduction: warp shuffles, then the group's warps in order
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++) {
+                double v = acc[d];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if ((gtid & 31) == 0) s_red[grp][gtid >> 5][d] = v;
+            }
+            gsync();
+            write_det_partials(a, b, ct * W, W, gtid, GT, [&](int d) {
+                double s = 0.0;
+                for (int w = 0; w < NWARP; w++) s += s_red[grp][w][d];
+                return s;
+            });
+            gsync();
+        }
+        if constexpr (INV) {
+            line_fft_half<NX, true, +1>(x, buf, twR, t, gsync);
+#pragma unroll
+            for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::R1>(i, t) - t) * ldy] = x[i];
+        } else if constexpr (STORE) {
+#pragma unroll
+            for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::RL>(i, t) - t) * ldy] = x[i];
+        }
+    }
+}
+
+// Tensor map for cols_pipe_kernel over a probe batch at `base` (cuTensorMapEncodeTiled through
+// the runtime's driver entry point, so the library needs no link to the driver library).
+void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr);
 
 // ---------------------------------------------------------------------------------------------
 // launch helpers
 template <class K>
-static int max_ctas(K kernel, size_t smem) {
+static int max_ctas(K kernel, int threads, size_t smem) {
     static int nsm = 0;
     if (nsm == 0) {
         int dev = 0;
@@ -279,21 +680,41 @@ static int max_ctas(K kernel, size_t smem) {
     }
     MTB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
-    MTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 256, smem));
+    MTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem));
     if (occ < 1) fail(MT_ERR_UNSUPPORTED, "line-pass kernel does not fit on an SM");
     return nsm * occ;
 }
 
+// The bulk-copy-fed kernels run where their shared memory fits and the pass loads its input;
+// they need the error flag of their bounded waits (a.err), and without it the per-thread-load
+// kernels run.
 template <int NY, int MODE>
 static void rows_launch(const RowArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NY>;
+    using S = RowPipeShape<NY>;
+    using RP = RowPipe<NY, S::GT, S::NG, S::EARLY>;
+    if constexpr (RP::OK && MODE != ROW_FIRST_ONE) {
+        if (a.err && a.nprobe % S::NG == 0) {
+            constexpr size_t sm = RP::SMEM;
+            auto kern = rows_pipe_kernel<NY, MODE, S::GT, S::NG, S::EARLY>;
+            static int cap = 0;
+            if (cap == 0) cap = max_ctas(kern, S::GT * S::NG, sm);
+            const int units = (a.nx / RP::LPC) * a.nprobe / S::NG;
+            int grid = grid_ctas > 0 ? grid_ctas : cap;
+            if (grid > units) grid = units;
+            kern<<<grid, S::GT * S::NG, sm, s>>>(a);
+            note_launch();
+            MTB_CUDA(cudaGetLastError());
+            return;
+        }
+    }
     const size_t sm = rows_smem<NY>();
     static int cap = 0;
-    if (cap == 0) cap = max_ctas(rows_kernel<NY, MODE>, sm);
-    const int items = (a.nx / (256 / G::TPL)) * a.nprobe;
+    if (cap == 0) cap = max_ctas(rows_kernel<NY, MODE>, G::THREADS, sm);
+    const int items = (a.nx / G::LPC) * a.nprobe;
     int grid = grid_ctas > 0 ? grid_ctas : cap;
     if (grid > items) grid = items;
-    rows_kernel<NY, MODE><<<grid, 256, sm, s>>>(a);
+    rows_kernel<NY, MODE><<<grid, G::THREADS, sm, s>>>(a);
     note_launch();
     MTB_CUDA(cudaGetLastError());
 }
@@ -311,13 +732,32 @@ void rows_dispatch_mode(RowMode mode, const RowArgs& a, int grid_ctas, cudaStrea
 template <int NX, int FLAGS, int LDY>
 static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NX>;
+    using S = ColPipeShape<NX>;
+    using CP = ColPipe<NX, S::GT, S::NG>;
+    if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
+        if (a.err) {
+            constexpr size_t sm = CP::SMEM;
+            auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG>;
+            static int cap = 0;
+            if (cap == 0) cap = max_ctas(kern, S::GT * S::NG, sm);
+            const int items = (a.ny / CP::W) * a.nprobe;
+            int grid = grid_ctas > 0 ? grid_ctas : cap;
+            if (grid > items) grid = items;
+            CUtensorMap map;
+            encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP::W, CP::BOXR);
+            kern<<<grid, S::GT * S::NG, sm, s>>>(a, map);
+            note_launch();
+            MTB_CUDA(cudaGetLastError());
+            return;
+        }
+    }
     const size_t sm = cols_smem<NX, FLAGS>();
     static int cap = 0;
-    if (cap == 0) cap = max_ctas(cols_kernel<NX, FLAGS, LDY>, sm);
-    const int items = (a.ny / (256 / G::TPL)) * a.nprobe;
+    if (cap == 0) cap = max_ctas(cols_kernel<NX, FLAGS, LDY>, G::THREADS, sm);
+    const int items = (a.ny / G::LPC) * a.nprobe;
     int grid = grid_ctas > 0 ? grid_ctas : cap;
     if (grid > items) grid = items;
-    cols_kernel<NX, FLAGS, LDY><<<grid, 256, sm, s>>>(a);
+    cols_kernel<NX, FLAGS, LDY><<<grid, G::THREADS, sm, s>>>(a);
     note_launch();
     MTB_CUDA(cudaGetLastError());
 }
@@ -334,6 +774,15 @@ constexpr int COL_F_STEP_DET = COL_LOAD | COL_PROP | COL_DETECT | COL_INVERSE | 
 constexpr int COL_F_LAST_DET = COL_LOAD | COL_PROP | COL_DETECT;
 constexpr int COL_F_FOURIER = COL_LOAD | COL_PROP | COL_STORE;
 constexpr int COL_F_PROBE_FS = COL_STORE;
+
+// Columns per detector partial: the narrowest tile of the column kernels for this length.
+template <int NX>
+int cols_det_width() {
+    constexpr int wc = LineGeom<NX>::LPC;
+    using S = ColPipeShape<NX>;
+    constexpr int wp = ColPipe<NX, S::GT, S::NG>::OK ? ColPipe<NX, S::GT, S::NG>::W : wc;
+    return wp < wc ? wp : wc;
+}
 
 template <int NX>
 void cols_dispatch_flags(int flags, const ColArgs& a, int grid_ctas, cudaStream_t s) {

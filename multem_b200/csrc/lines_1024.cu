@@ -4,4 +4,5 @@
 namespace mtb {
 template void rows_dispatch_mode<1024>(RowMode, const RowArgs&, int, cudaStream_t);
 template void cols_dispatch_flags<1024>(int, const ColArgs&, int, cudaStream_t);
+template int cols_det_width<1024>();
 }  // namespace mtb

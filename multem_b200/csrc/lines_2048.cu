@@ -4,4 +4,5 @@
 namespace mtb {
 template void rows_dispatch_mode<2048>(RowMode, const RowArgs&, int, cudaStream_t);
 template void cols_dispatch_flags<2048>(int, const ColArgs&, int, cudaStream_t);
+template int cols_det_width<2048>();
 }  // namespace mtb

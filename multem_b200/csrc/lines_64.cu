@@ -4,4 +4,5 @@
 namespace mtb {
 template void rows_dispatch_mode<64>(RowMode, const RowArgs&, int, cudaStream_t);
 template void cols_dispatch_flags<64>(int, const ColArgs&, int, cudaStream_t);
+template int cols_det_width<64>();
 }  // namespace mtb
