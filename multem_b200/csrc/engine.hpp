@@ -7,6 +7,7 @@
 #include <memory>
 #include <vector>
 
+#include "devmem.hpp"
 #include "host_model.hpp"
 #include "kernels.cuh"
 #include "multem_b200.h"
@@ -14,22 +15,29 @@
 
 namespace mtb {
 
+// Device array from the library's memory pool (devmem.hpp).
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    int dev = 0;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
-    DevBuf& operator=(DevBuf&& o) noexcept { std::swap(p, o.p); std::swap(n, o.n); return *this; }
-    ~DevBuf() { if (p) cudaFree(p); }
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), dev(o.dev) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        std::swap(dev, o.dev);
+        return *this;
+    }
+    ~DevBuf() { if (p) dev_free(p, dev); }
     void alloc(size_t count) {
         if (count <= n && p) return;
-        if (p) cudaFree(p);
+        if (p) dev_free(p, dev);
         p = nullptr;
         n = 0;
-        cuda_check(cudaMalloc(&p, sizeof(T) * (count ? count : 1)), "cudaMalloc");
+        p = static_cast<T*>(dev_alloc(sizeof(T) * (count ? count : 1), &dev));
         n = count;
     }
     void upload(const T* h, size_t count, cudaStream_t s) {

@@ -273,29 +273,72 @@ __device__ __forceinline__ void stage_compute(float2* x, int t, const float2* tw
     });
 }
 
+// Padded buffer index of the exchange after stage S, for thread t and register i, on the writing
+// side (stage S's output position) and the reading side (stage S+1's input position). When both
+// are t * stride + f(i) for every t and i (checked at compile time), each access is a per-thread
+// base plus a compile-time offset.
+template <int N, bool REV, int S>
+struct ExchangeMap {
+    static constexpr int E = LinePlan<N>::E;
+    static constexpr int TPL = N / E;
+    static constexpr int R = StageRadix<N, REV, S>::value;
+    static constexpr int NSV = StageNs<N, REV, S>::value;
+    static constexpr int R2 = StageRadix<N, REV, S + 1>::value;
+    static constexpr int wpos(int t, int i) {
+        const int j = t + TPL * (i / R);
+        const int p = (j / NSV) * NSV * R + (j % NSV) + (i % R) * NSV;
+        return p + p / R;
+    }
+    static constexpr int rpos(int t, int i) {
+        const int p = t + TPL * (i / R2) + (i % R2) * (N / R2);
+        return p + p / R;
+    }
+    static constexpr int SW = wpos(1, 0) - wpos(0, 0);
+    static constexpr int SR = rpos(1, 0) - rpos(0, 0);
+    static constexpr bool linear() {
+        for (int t = 0; t < TPL; t++)
+            for (int i = 0; i < E; i++)
+                if (wpos(t, i) != t * SW + wpos(0, i) || rpos(t, i) != t * SR + rpos(0, i)) return false;
+        return true;
+    }
+    static constexpr bool LINEAR = linear();
+};
+
 // Exchange after stage S through the line buffer `buf` (floats as float2), then load the inputs
 // of stage S+1. Caller provides the barrier functor (warp- or block-level).
 template <int N, bool REV, int S, class Sync>
 __device__ __forceinline__ void stage_exchange(float2* x, float2* buf, int t, Sync sync) {
-    constexpr int E = LinePlan<N>::E;
-    constexpr int TPL = N / E;
-    constexpr int R = StageRadix<N, REV, S>::value;
-    constexpr int NSV = StageNs<N, REV, S>::value;
-    constexpr int R2 = StageRadix<N, REV, S + 1>::value;
-    sync();
+    using M = ExchangeMap<N, REV, S>;
+    constexpr int E = M::E, TPL = M::TPL, R = M::R, NSV = M::NSV, R2 = M::R2;
+    if constexpr (M::LINEAR) {
+        sync();
+        float2* bw = buf + t * M::SW;
+        static_for<0, E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            bw[M::wpos(0, i)] = x[i];
+        });
+        sync();
+        const float2* br = buf + t * M::SR;
+        static_for<0, E>([&](auto ic) {
+            constexpr int i = decltype(ic)::value;
+            x[i] = br[M::rpos(0, i)];
+        });
+    } else {
+        sync();
 #pragma unroll
-    for (int m = 0; m < E / R; ++m) {
-        int j = t + TPL * m;
-        int base = (j / NSV) * NSV * R + (j % NSV);
+        for (int m = 0; m < E / R; ++m) {
+            int j = t + TPL * m;
+            int base = (j / NSV) * NSV * R + (j % NSV);
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[pad_idx<R>(base + r * NSV)] = x[m * R + r];
-    }
-    sync();
+            for (int r = 0; r < R; ++r) buf[pad_idx<R>(base + r * NSV)] = x[m * R + r];
+        }
+        sync();
 #pragma unroll
-    for (int m = 0; m < E / R2; ++m) {
-        int j = t + TPL * m;
+        for (int m = 0; m < E / R2; ++m) {
+            int j = t + TPL * m;
 #pragma unroll
-        for (int r = 0; r < R2; ++r) x[m * R2 + r] = buf[pad_idx<R>(j + r * (N / R2))];
+            for (int r = 0; r < R2; ++r) x[m * R2 + r] = buf[pad_idx<R>(j + r * (N / R2))];
+        }
     }
 }
 
@@ -342,6 +385,7 @@ template <int B>
 __device__ __forceinline__ int drop_bit(int p) {
     return (p & ((1 << B) - 1)) | ((p >> (B + 1)) << B);
 }
+constexpr int drop_bit_c(int p, int b) { return (p & ((1 << b) - 1)) | ((p >> (b + 1)) << b); }
 
 // Line buffer length (float2) for the half-line exchange: N/2 positions padded by the smallest
 // PADW of the plan (>= RMIN/2), odd.
@@ -351,24 +395,54 @@ struct HalfLineSmem {
     static constexpr int value = N / 2 + N / RMIN + 1;
 };
 
+// Buffer index of the half-line exchange (as ExchangeMap, with bit B of the position dropped).
+template <int N, bool REV>
+struct HalfExchangeMap {
+    using H = HalfExchange<N, REV>;
+    static constexpr int E = H::E, TPL = H::TPL, R = H::R, R2 = H::R2, B = H::B < 0 ? 0 : H::B, PW = H::PADW;
+    static constexpr int wcpos(int i) { return TPL * (i / R) * R + (i % R); }        // writer position less t*R
+    static constexpr int rcpos(int i) { return TPL * (i / R2) + (i % R2) * (N / R2); }  // reader position less t
+    static constexpr int idx(int p) { return drop_bit_c(p, B) + drop_bit_c(p, B) / PW; }
+    static constexpr int wpos(int t, int i) { return idx(t * R + wcpos(i)); }
+    static constexpr int rpos(int t, int i) { return idx(t + rcpos(i)); }
+    static constexpr int SW = wpos(1, 0) - wpos(0, 0);
+    static constexpr int SR = rpos(1, 0) - rpos(0, 0);
+    static constexpr bool linear() {
+        for (int t = 0; t < TPL; t++)
+            for (int i = 0; i < E; i++)
+                if (wpos(t, i) != t * SW + wpos(0, i) || rpos(t, i) != t * SR + rpos(0, i)) return false;
+        return true;
+    }
+    static constexpr bool LINEAR = H::OK && linear();
+};
+
 template <int N, bool REV, class Sync>
 __device__ __forceinline__ void stage_exchange_half(float2* x, float2* buf, int t, Sync sync) {
     using H = HalfExchange<N, REV>;
-    constexpr int E = H::E, TPL = H::TPL, R = H::R, R2 = H::R2, B = H::B, PW = H::PADW;
+    using M = HalfExchangeMap<N, REV>;
+    constexpr int E = H::E, R = H::R, B = H::B, PW = H::PADW;
     static_assert(H::OK, "plan has no half-line exchange");
+    float2* bw = buf + (M::LINEAR ? t * M::SW : 0);
+    const float2* br = buf + (M::LINEAR ? t * M::SR : 0);
     static_for<0, 2>([&](auto hc) {
         constexpr int h = decltype(hc)::value;
         sync();
         static_for<0, E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            constexpr int cpos = TPL * (i / R) * R + (i % R);  // writer position less t*R
-            if constexpr (((cpos >> B) & 1) == h) buf[pad_idx<PW>(drop_bit<B>(t * R + cpos))] = x[i];
+            constexpr int cpos = M::wcpos(i);
+            if constexpr (((cpos >> B) & 1) == h) {
+                if constexpr (M::LINEAR) bw[M::wpos(0, i)] = x[i];
+                else buf[pad_idx<PW>(drop_bit<B>(t * R + cpos))] = x[i];
+            }
         });
         sync();
         static_for<0, E>([&](auto ic) {
             constexpr int i = decltype(ic)::value;
-            constexpr int cpos = TPL * (i / R2) + (i % R2) * (N / R2);  // reader position less t
-            if constexpr (((cpos >> B) & 1) == h) x[i] = buf[pad_idx<PW>(drop_bit<B>(t + cpos))];
+            constexpr int cpos = M::rcpos(i);
+            if constexpr (((cpos >> B) & 1) == h) {
+                if constexpr (M::LINEAR) x[i] = br[M::rpos(0, i)];
+                else x[i] = buf[pad_idx<PW>(drop_bit<B>(t + cpos))];
+            }
         });
     });
 }

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "devmem.hpp"
 #include "tables.hpp"
 
 namespace mtb {
@@ -223,24 +224,23 @@ void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& head
     const int n = (int)Zs.size();
     std::vector<ElemCoef> h(n);
     for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i]);
-    ElemCoef* d_coef = nullptr;
-    TableHead* d_head = nullptr;
-    MTB_CUDA(cudaMallocAsync(&d_coef, sizeof(ElemCoef) * n, stream));
-    MTB_CUDA(cudaMallocAsync(&d_head, sizeof(TableHead) * n, stream));
+    int dev = 0;
+    auto* d_coef = static_cast<ElemCoef*>(dev_alloc(sizeof(ElemCoef) * n, &dev));
+    auto* d_head = static_cast<TableHead*>(dev_alloc(sizeof(TableHead) * n, &dev));
     MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
     MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));
     build_tables_kernel<<<n, 128, 3 * nR * sizeof(double), stream>>>(d_coef, d_head, n, nR, d_tab);
     MTB_CUDA(cudaGetLastError());
     MTB_CUDA(cudaStreamSynchronize(stream));
-    MTB_CUDA(cudaFreeAsync(d_coef, stream));
-    MTB_CUDA(cudaFreeAsync(d_head, stream));
+    dev_free(d_coef, dev);
+    dev_free(d_head, dev);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Allocation-free variant of build_tables.
 //
 // The per-call scratch of build_tables (the element coefficients and table heads the kernel reads)
-// lives here in one file-scope device array instead of memory obtained from cudaMallocAsync. The
+// lives here in one file-scope device array instead of memory allocated from the device pool. The
 // array is kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead)) bytes (about 26 KB) and is
 // held by every GPU that loads this library until the process exits. All calls share it: each
 // call overwrites the entries it uses before its kernel reads them (nothing has to start at zero),
