@@ -250,8 +250,10 @@ mt_status mt_projected_potential(const mt_system_conf* conf, const mt_input_mult
  * src/transmission_function.cuh:54-85). trans: interleaved complex. */
 mt_status mt_transmission_function(const mt_system_conf* conf, const mt_input_multislice* in,
                                    int iconf, int islice, double* trans);
-/* Propagate the user wave in->iw_psi by distance z (ilc_propagate.cu:125; Propagator::operator(),
- * src/propagator.cuh:34-86). space 1 = real, 2 = reciprocal. psi_out: interleaved complex. */
+/* Propagate the user wave in->iw_psi (iw_type 3) by distance z (ilc_propagate.cu:125-147, which
+ * passes obj_lens_c_10 as z; Propagator::operator(), src/propagator.cuh:51-103). Reads only nx, ny,
+ * spec_lx/ly, iw_psi, E_0, theta, phi. space 1 = real, 2 = reciprocal. psi_out: interleaved
+ * complex, column-major like iw_psi. */
 mt_status mt_propagate(const mt_system_conf* conf, const mt_input_multislice* in, int space,
                        double z, double* psi_out);
 /* Incident wave at in->iw_x/iw_y (ilc_incident_wave.cu:154; Incident_Wave::operator(),

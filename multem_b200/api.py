@@ -184,6 +184,24 @@ def ilc_incident_wave(system_conf, params: Parameters, space: int = 1) -> np.nda
     return (t[0::2] + 1j * t[1::2]).reshape(params.nx, params.ny).T
 
 
+def propagate(system_conf, params: Parameters, z: float, space: int = 1) -> np.ndarray:
+    """The user wave params.iw_psi ([ny, nx], iw_type 3) propagated by z (Angstrom); space 1 real,
+    2 reciprocal (Propagator::operator(), src/propagator.cuh:51-103). Returns [ny, nx] complex."""
+    lib = capi.load()
+    s, keep = params.to_c()
+    t = np.zeros(2 * params.nx * params.ny)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_propagate(C.byref(conf), C.byref(s), int(space), float(z), _dp(t)))
+    return (t[0::2] + 1j * t[1::2]).reshape(params.nx, params.ny).T
+
+
+def ilc_propagate(system_conf, params: Parameters) -> dict:
+    """ilc_propagate (mex_files_multem/ilc_propagate.cu:125-175): propagates iw_psi by obj_lens_c_10
+    in real space; returns {dx, dy, psi}."""
+    psi = propagate(system_conf, params, params.obj_lens_c_10, 1)
+    return {"dx": params.spec_lx / params.nx, "dy": params.spec_ly / params.ny, "psi": psi}
+
+
 def spline_tables(Z, dR_min: float, Vrl: float = 0.015, nR: int = 128, system_conf=None):
     """FP64 GPU build of the Lobato spline tables: returns (heads[n, 4], tab[n, 5, nR] float32)."""
     lib = capi.load()

@@ -191,8 +191,7 @@ mt_status mt_propagate(const mt_system_conf* conf, const mt_input_multislice* in
                        double* psi_out) {
     return guarded([&] {
         mt_system_conf c = conf ? *conf : default_conf();
-        mtb::Engine e(&c, in);
-        e.propagate(space, z, psi_out);
+        mtb::propagate_wave(&c, in, space, z, psi_out);
     });
 }
 

@@ -34,6 +34,23 @@ int env_int(const char* name, int dflt) {
 
 }  // namespace
 
+GridDev grid_dev(const GridF& g) {
+    GridDev d{};
+    d.nx = g.nx;
+    d.ny = g.ny;
+    d.nxh = g.nxh;
+    d.nyh = g.nyh;
+    d.lx = g.lx;
+    d.ly = g.ly;
+    d.dRx = g.dRx;
+    d.dRy = g.dRy;
+    d.Rx_0 = g.Rx_0;
+    d.Ry_0 = g.Ry_0;
+    d.dgx = g.dgx;
+    d.dgy = g.dgy;
+    return d;
+}
+
 Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     if (conf) {
         if (conf->precision != 1)
@@ -53,18 +70,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     if (!pow2(nx) || !pow2(ny)) fail(MT_ERR_UNSUPPORTED, "nx and ny must be powers of two in [64, 2048]");
     if (m_.is_EW() && !m_.is_plane_wave()) fail(MT_ERR_UNSUPPORTED, "EW simulations need a plane incident wave");
 
-    gdev_.nx = nx;
-    gdev_.ny = ny;
-    gdev_.nxh = m_.grid.nxh;
-    gdev_.nyh = m_.grid.nyh;
-    gdev_.lx = m_.grid.lx;
-    gdev_.ly = m_.grid.ly;
-    gdev_.dRx = m_.grid.dRx;
-    gdev_.dRy = m_.grid.dRy;
-    gdev_.Rx_0 = m_.grid.Rx_0;
-    gdev_.Ry_0 = m_.grid.Ry_0;
-    gdev_.dgx = m_.grid.dgx;
-    gdev_.dgy = m_.grid.dgy;
+    gdev_ = grid_dev(m_.grid);
 
     build_types();
     std::vector<float> rmax_of_Z(103, 0.0f);
@@ -180,7 +186,7 @@ void Engine::build_types() {
 // Fresnel propagator factors for distance dz, separable in x and y:
 // P(ix, iy) = exp(i*w*(gx^2 + gy^2))/N, w = -pi*lambda*dz (propagate, src/cgpu_fcns.cuh:1837-1845;
 // get_propagator_factor, src/input_multislice.cuh:909-912). Phases in double, stored as float.
-void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const {
+void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const double w = (double)m_.propagator_factor(dz);
     // Between passes the wave is kept as F_y(psi)/ny (the unnormalised row transforms of one step
@@ -200,6 +206,8 @@ void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const {
         py[iy] = make_float2((float)std::cos(th), (float)std::sin(th));
     }
 }
+
+void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const { mtb::prop_tables(m_, dz, px, py, output); }
 
 ProbeDev Engine::probe_params(float c_c_10, int nz_c10) const {
     const LensF& L = m_.cond_lens;
@@ -690,8 +698,100 @@ void Engine::incident_wave(int space, double* psi) {
     }
 }
 
-void Engine::propagate(int, double, double*) {
-    fail(MT_ERR_UNSUPPORTED, "mt_propagate is not implemented yet");
+// ilc_propagate (mex_files_multem/ilc_propagate.cu:125-147; Propagator::operator(),
+// src/propagator.cuh:51-103): the user wave iw_psi is fft-shifted in, Fourier transformed, multiplied
+// by the Fresnel propagator of distance z (tilt offset g0 from theta/phi, 1/N folded in) and, for
+// real-space output, transformed back; then shifted back. With |z| <= 1e-5 (isZero) the real-space
+// result is the wave itself and the reciprocal one FFT2(psi)/N. One wave runs through the same line
+// passes as a multislice step with a transmission function of ones: row pass F_y, column pass
+// F_x * P (* F_x^-1), row pass F_y^-1.
+void propagate_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space, double z, double* psi_out) {
+    if (space != 1 && space != 2) fail(MT_ERR_INVALID_ARG, "space must be 1 (real) or 2 (reciprocal)");
+    if (!psi_out) fail(MT_ERR_INVALID_ARG, "psi_out is NULL");
+    int device = 0;
+    if (conf) {
+        if (conf->precision != 1) fail(MT_ERR_UNSUPPORTED, "this engine computes in FP32 (system_conf.precision must be 1)");
+        if (conf->device != 2) fail(MT_ERR_UNSUPPORTED, "this engine runs on the GPU (system_conf.device must be 2)");
+        device = conf->gpu_device;
+    }
+    const Model m = build_prop_model(in);
+    const int nx = m.grid.nx, ny = m.grid.ny;
+    const size_t nxy = (size_t)nx * ny;
+    std::vector<float2> h(nxy);
+    for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny; iy++) {
+            const size_t src = (size_t)ix * ny + iy;
+            const size_t dst = (size_t)((ix + m.grid.nxh) % nx) * ny + (iy + m.grid.nyh) % ny;
+            h[dst] = make_float2(m.iw_psi[2 * src], m.iw_psi[2 * src + 1]);
+        }
+    auto write_out = [&](const std::vector<float2>& v) {
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++) {
+                const size_t src = (size_t)((ix + m.grid.nxh) % nx) * ny + (iy + m.grid.nyh) % ny;
+                const size_t dst = (size_t)ix * ny + iy;
+                psi_out[2 * dst] = v[src].x;
+                psi_out[2 * dst + 1] = v[src].y;
+            }
+    };
+    const bool zero = is_zero_f((float)z);
+    if (zero && space == 1) {
+        write_out(h);
+        return;
+    }
+    int ndev = 0;
+    MTB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) fail(MT_ERR_INVALID_ARG, "gpu_device out of range");
+    MTB_CUDA(cudaSetDevice(device));
+    cudaStream_t st;
+    MTB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{st};
+    std::vector<float2> ones(nxy, make_float2(1.0f, 0.0f));
+    std::vector<float2> prop((size_t)nx + ny);
+    prop_tables(m, zero ? 0.0f : (float)z, prop.data(), prop.data() + nx, false);
+    DevBuf<float2> d_psi, d_out, d_one, d_prop;
+    d_psi.upload(h.data(), nxy, st);
+    d_one.upload(ones.data(), nxy, st);
+    d_prop.upload(prop.data(), prop.size(), st);
+    d_out.alloc(nxy);
+    RowArgs ra{};
+    ra.in = d_psi.p;
+    ra.out = d_psi.p;
+    ra.trans = d_one.p;
+    ra.nx = nx;
+    ra.nprobe = 1;
+    ra.scale = 1.0f;
+    launch_rows(ny, ROW_FIRST_REAL, ra, 0, st);
+    ColArgs ca{};
+    ca.in = d_psi.p;
+    ca.out = d_psi.p;
+    ca.ny = ny;
+    ca.nprobe = 1;
+    ca.g = grid_dev(m.grid);
+    ca.Px = d_prop.p;
+    ca.Py = d_prop.p + nx;
+    ca.det_w = 1;
+    launch_cols(nx, space == 1 ? (COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE) : (COL_LOAD | COL_PROP | COL_STORE), ca, 0,
+                st);
+    const float2* res = d_psi.p;
+    if (space == 1) {
+        RowArgs rb{};
+        rb.in = d_psi.p;
+        rb.out = d_out.p;
+        rb.nx = nx;
+        rb.nprobe = 1;
+        rb.scale = 1.0f;
+        launch_rows(ny, ROW_INVERSE, rb, 0, st);
+        res = d_out.p;
+    }
+    MTB_CUDA(cudaMemcpyAsync(h.data(), res, sizeof(float2) * nxy, cudaMemcpyDeviceToHost, st));
+    MTB_CUDA(cudaStreamSynchronize(st));
+    write_out(h);
 }
 
 }  // namespace mtb

@@ -46,6 +46,12 @@ struct DevBuf {
     }
 };
 
+GridDev grid_dev(const GridF& g);
+// Fresnel propagator factors Px[nx], Py[ny] of distance dz (see engine.cu).
+void prop_tables(const Model& m, float dz, float2* px, float2* py, bool output);
+// mt_propagate: the user wave in->iw_psi propagated by z (space 1 real, 2 reciprocal).
+void propagate_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space, double z, double* psi_out);
+
 // Per phonon configuration: displaced atoms, slice ranges, propagator tables, probe defocus.
 struct ConfData {
     int iconf = 0;
@@ -85,7 +91,6 @@ class Engine {
     // operator-level entries
     void projected_potential(int iconf, int islice, double* V, double* trans);
     void incident_wave(int space, double* psi);
-    void propagate(int space, double z, double* psi);
 
     cudaStream_t stream() const { return stream_; }
     int batch_size() const { return batch_; }

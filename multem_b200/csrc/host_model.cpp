@@ -444,6 +444,40 @@ float Model::phonon_weight() const {
 // read_input_multislice + validate_parameters (mex_files_multem/ilc_multem.cu:38-379,
 // src/input_multislice.cuh:622-796) for the simulation types, slicing and incident waves this
 // engine implements; anything else is rejected with MT_ERR_UNSUPPORTED.
+// read_input_multislice of ilc_propagate (mex_files_multem/ilc_propagate.cu:34-95): the grid from
+// spec_lx/ly and nx/ny (lz = 0, dz = 0.25, no band-width limit, periodic), the user wave, E_0 and
+// the beam tilt; nothing of the specimen is read.
+Model build_prop_model(const mt_input_multislice* in) {
+    if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
+    auto pow2 = [](int n) { return n >= 64 && n <= 2048 && (n & (n - 1)) == 0; };
+    if (!pow2(in->nx) || !pow2(in->ny)) fail(MT_ERR_UNSUPPORTED, "nx and ny must be powers of two in [64, 2048]");
+    if (!(in->spec_lx > 0) || !(in->spec_ly > 0)) fail(MT_ERR_INVALID_ARG, "spec_lx and spec_ly must be positive");
+    if (in->iw_type != 3 || !in->iw_psi)
+        fail(MT_ERR_INVALID_ARG, "propagation needs a user-defined wave (iw_type 3 with iw_psi)");
+    Model m;
+    m.simulation_type = in->simulation_type;
+    m.grid.set(in->nx, in->ny, (float)in->spec_lx, (float)in->spec_ly, 0.25f, false, true);
+    m.iw_type = 3;
+    const size_t n = (size_t)in->nx * in->ny;
+    m.iw_psi.resize(2 * n);
+    for (size_t i = 0; i < 2 * n; i++) m.iw_psi[i] = (float)in->iw_psi[i];
+    m.E_0 = (float)in->E_0;
+    m.theta = (float)((float)in->theta * kDeg);
+    m.phi = (float)((float)in->phi * kDeg);
+    m.lambda = lambda_f(m.E_0);
+    m.mul_sign = 1;
+    // set_incident_angle (src/input_multislice.cuh:891-895): the tilt is snapped so that
+    // sin(theta)/lambda is a whole number of Fourier pixels
+    if (is_zero_f(m.theta)) {
+        m.theta = 0;
+    } else {
+        const float dg = m.grid.dg_min();
+        const float n = std::round(std::sin(m.theta) / (m.lambda * dg));
+        m.theta = std::asin(n * m.lambda * dg);
+    }
+    return m;
+}
+
 Model build_model(const mt_input_multislice* in) {
     if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
     Model m;

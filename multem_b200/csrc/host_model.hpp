@@ -157,6 +157,8 @@ struct Model {
 
 // Validate `in` like read_input_multislice + validate_parameters; throws mtb::Error.
 Model build_model(const mt_input_multislice* in);
+// The fields ilc_propagate reads (grid, user wave, E_0, tilt); throws mtb::Error.
+Model build_prop_model(const mt_input_multislice* in);
 
 // Per-element spline-table header needed on the host (R_max drives statistics and footprints).
 struct AtomTypeHead {

@@ -253,6 +253,34 @@ def propagator(grid: Grid, lam, dz, dtype=np.float64):
     return np.exp(1j * w * g2) / (grid.nx * grid.ny)
 
 
+def incident_angle(theta, lam, dg_min):
+    """set_incident_angle (src/input_multislice.cuh:891-895): the tilt snapped to a whole number of
+    Fourier pixels, sin(theta)/lambda = n*dg_min (FP64)."""
+    if abs(theta) <= 1e-13:
+        return 0.0
+    n = np.round(np.sin(theta) / (lam * dg_min))
+    return float(np.arcsin(n * lam * dg_min))
+
+
+def propagate_wave(grid: Grid, lam, psi, z, space=1, gx0=0.0, gy0=0.0):
+    """Propagator::operator()(space, gxu, gyu, z, output) on a user wave (src/propagator.cuh:51-103,
+    propagate src/cgpu_fcns.cuh:1837-1845): fft2-shift in, FFT, P = exp(-i*pi*lam*z*|g - g0|^2)/N,
+    inverse FFT (unnormalised) for real-space output, shift back. |z| <= 1e-5 is isZero
+    (src/types.cuh:564-600): the wave itself (real) or FFT2(psi)/N (reciprocal). psi and the
+    result are [iy, ix] (MATLAB orientation)."""
+    a = np.fft.fftshift(np.asarray(psi, np.complex128).T)
+    n = grid.nx * grid.ny
+    if abs(float(z)) <= 1e-5:
+        out = a if space == 1 else np.fft.fft2(a) / n
+    else:
+        w = -C_PI * float(lam) * float(z)
+        gx, gy = grid.g_shift()
+        g2 = (gx.astype(np.float64)[:, None] - gx0) ** 2 + (gy.astype(np.float64)[None, :] - gy0) ** 2
+        f = np.fft.fft2(a) * np.exp(1j * w * g2) / n
+        out = f if space == 2 else np.fft.ifft2(f) * n
+    return np.fft.fftshift(out).T
+
+
 def probe_fourier(grid: Grid, lam, outer_mrad, inner_mrad, c10, c30_A, beam_x, beam_y, dtype=np.float64):
     """Normalised Fourier-space probe (exp_i_chi + probe, src/cgpu_fcns.cuh:1951-1992 and
     src/gpu_fcns.cuh:1612-1624): aperture * exp(i*(x*gx + y*gy + chi(g)))."""

@@ -16,6 +16,7 @@
 #include "input_multislice.cuh"
 #include "output_multislice.hpp"
 #include "tem_simulation.cuh"
+#include "propagator.cuh"
 
 #include <cstring>
 #include <exception>
@@ -430,6 +431,63 @@ int mtref_incident_wave(const mt_input_multislice* in, int precision, int space,
         if (precision == 2) { WF<double> w(in, 1); return body(w); }
         WF<float> w(in, 1);
         return body(w);
+    });
+}
+
+// Propagation of the user wave in->iw_psi by z, as ilc_propagate does it (read_input_multislice and
+// run_propagate, mex_files_multem/ilc_propagate.cu:34-147): simulation type PropRS, still atoms,
+// grid from spec_lx/ly and nx/ny with lz = 0, dz = 0.25, no band-width limit, then
+// Propagator::operator()(space, gx_0, gy_0, z, output) (src/propagator.cuh:95-103), which fft-shifts
+// the wave in, propagates and shifts it back. The MEX file passes obj_lens_c_10 as z.
+int mtref_propagate(const mt_input_multislice* in, int precision, int space, double z, double* psi) {
+    return guarded([&] {
+        auto body = [&](auto tag) {
+            using TT = decltype(tag);
+            mt::Input_Multislice<TT> im;
+            im.system_conf.precision = std::is_same<TT, float>::value ? mt::eP_float : mt::eP_double;
+            im.system_conf.device = mt::e_host;
+            im.system_conf.cpu_nthread = 1;
+            im.system_conf.validate_parameters();
+            im.simulation_type = mt::eTEMST_PropRS;
+            im.pn_model = mt::ePM_Still_Atom;
+            im.grid_2d.set_input_data(in->nx, in->ny, (TT)in->spec_lx, (TT)in->spec_ly, (TT)0.25, false, true);
+            im.set_incident_wave_type(static_cast<mt::eIncident_Wave_Type>(in->iw_type));
+            const int nxy = in->nx * in->ny;
+            im.iw_psi.resize(nxy);
+            for (int i = 0; i < nxy; i++) im.iw_psi[i] = std::complex<TT>((TT)in->iw_psi[2 * i], (TT)in->iw_psi[2 * i + 1]);
+            for (int i = 0; i < in->n_iw_xy; i++) {
+                im.iw_x.push_back((TT)in->iw_x[i]);
+                im.iw_y.push_back((TT)in->iw_y[i]);
+            }
+            im.E_0 = (TT)in->E_0;
+            im.theta = (TT)(in->theta * mt::c_deg_2_rad);
+            im.phi = (TT)(in->phi * mt::c_deg_2_rad);
+            im.obj_lens.c_10 = (TT)z;
+            im.obj_lens.set_input_data(im.E_0, im.grid_2d);
+            im.output_area.ix_0 = in->output_area_ix_0 - 1;
+            im.output_area.iy_0 = in->output_area_iy_0 - 1;
+            im.output_area.ix_e = in->output_area_ix_e - 1;
+            im.output_area.iy_e = in->output_area_iy_e - 1;
+            im.validate_parameters();
+            mt::Stream<mt::e_host> stream(1);
+            mt::FFT<TT, mt::e_host> fft_2d;
+            fft_2d.create_plan_2d(im.grid_2d.ny, im.grid_2d.nx, 1);
+            mt::Propagator<TT, mt::e_host> prop;
+            prop.set_input_data(&im, &stream, &fft_2d);
+            mt::Output_Multislice<TT> out;
+            out.set_input_data(&im);
+            prop(space == 2 ? mt::eS_Reciprocal : mt::eS_Real, im.gx_0(), im.gy_0(), im.obj_lens.c_10, out);
+            stream.synchronize();
+            const auto& v = out.psi_coh[0];
+            for (size_t i = 0; i < v.size(); i++) {
+                psi[2 * i] = (double)v[i].real();
+                psi[2 * i + 1] = (double)v[i].imag();
+            }
+            fft_2d.cleanup();
+            return 0;
+        };
+        if (precision == 2) return body(double());
+        return body(float());
     });
 }
 

@@ -43,6 +43,7 @@ def lib():
         L.mtref_atom_type.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, capi.P_double, capi.P_double,
                                       C.c_int]
         L.mtref_incident_wave.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, capi.P_double]
+        L.mtref_propagate.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, C.c_double, capi.P_double]
         _lib = L
     return _lib
 
@@ -165,5 +166,14 @@ def incident_wave(p, space=1, precision=1):
     s, keep = p.to_c()
     t = np.zeros(2 * p.nx * p.ny)
     _chk(lib().mtref_incident_wave(C.byref(s), precision, space, _dp(t)))
+    t = t[0::2] + 1j * t[1::2]
+    return t.reshape(p.nx, p.ny).T
+
+
+def propagate(p, z, space=1, precision=1):
+    """The reference's Propagator on the user wave p.iw_psi (ilc_propagate semantics, distance z)."""
+    s, keep = p.to_c()
+    t = np.zeros(2 * p.nx * p.ny)
+    _chk(lib().mtref_propagate(C.byref(s), precision, space, float(z), _dp(t)))
     t = t[0::2] + 1j * t[1::2]
     return t.reshape(p.nx, p.ny).T

@@ -1,0 +1,27 @@
+"""Inputs of the golden cases that are not specimens (shared by gen_golden.py and the tests)."""
+import numpy as np
+
+from multem_b200 import Parameters
+
+
+def prop_case():
+    """A seeded smooth user wave on a 128 x 64 grid (non-square) for ilc_propagate, 200 kV."""
+    p = Parameters()
+    p.nx, p.ny = 128, 64
+    p.spec_lx, p.spec_ly = 20.0, 10.0
+    p.E_0 = 200.0
+    p.iw_type = 3
+    rng = np.random.default_rng(21)
+    y, x = np.meshgrid(np.arange(p.ny) * p.spec_ly / p.ny, np.arange(p.nx) * p.spec_lx / p.nx, indexing="ij")
+    env = np.exp(-((x - 10.0) ** 2 + (y - 5.0) ** 2) / (2 * 3.0 ** 2))
+    phase = rng.standard_normal((p.ny, p.nx))
+    p.iw_psi = env * np.exp(1j * 0.5 * phase)
+    p.iw_x, p.iw_y = [0.0], [0.0]
+    return p
+
+
+def prop_tilt_case():
+    """prop_case with the beam tilted by 0.5 deg at azimuth 30 deg."""
+    p = prop_case()
+    p.theta, p.phi = 0.5, 30.0
+    return p

@@ -5,6 +5,10 @@ itself (its Multislice<T, e_host>, compiled from its sources by oracle/Makefile)
 inputs. They let the oracle and the engine be checked where oracle/_ref is not built.
 
     make -C oracle && python tests/golden/gen_golden.py
+
+The full runs use 8 host threads, and the reference's threaded CPU path does not sum in a fixed
+order: a regeneration reproduces them only to float rounding (about 1e-6 relative in FP32), so
+arrays already in the file are kept and only new keys are added (--overwrite replaces all).
 """
 from __future__ import annotations
 
@@ -17,6 +21,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from multem_b200 import specimens  # noqa: E402
+from cases import prop_case, prop_tilt_case  # noqa: E402
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -83,6 +88,15 @@ def main():
     for prec in (1, 2):
         rec[f"probe_real_p{prec}"] = R.incident_wave(pw, 1, prec)
         rec[f"probe_fourier_p{prec}"] = R.incident_wave(pw, 2, prec)
+    # propagation of a user wave (ilc_propagate), plain and with a beam tilt
+    rec["prop_in"] = np.asarray(prop_case().iw_psi)
+    for name, fn, zs in (("prop", prop_case, (0.0, 35.0)), ("prop_tilt", prop_tilt_case, (35.0,))):
+        q = fn()
+        for z in zs:
+            for space in (1, 2):
+                for prec in ((1, 2) if z != 0 else (1,)):
+                    r = R.propagate(q, z, space, prec)
+                    rec[f"{name}_z{int(z)}_s{space}_p{prec}"] = r.astype(np.complex64) if prec == 1 else r
     # full runs
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
                      ("ew_config1", ew_config1)):
@@ -94,7 +108,11 @@ def main():
                     v = out[k]
                     rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64) \
                         if name == "ew_config1" else v
-    np.savez_compressed(OUT / "reference_fixtures.npz", **rec)
+    path = OUT / "reference_fixtures.npz"
+    if path.exists() and "--overwrite" not in sys.argv:
+        old = np.load(path)
+        rec.update({k: old[k] for k in old.files})
+    np.savez_compressed(path, **rec)
     print("wrote", OUT / "reference_fixtures.npz", len(rec), "arrays")
 
 

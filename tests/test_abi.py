@@ -2,6 +2,9 @@
 import re
 from pathlib import Path
 
+import numpy as np
+import pytest
+
 from multem_b200 import capi
 
 HDR = Path(__file__).resolve().parents[1] / "include" / "multem_b200.h"
@@ -29,3 +32,23 @@ def test_abi_version_and_error_string():
     lib = capi.load()
     assert lib.mt_abi_version() == 1
     assert isinstance(lib.mt_last_error(), bytes)
+
+
+def test_propagate_host_checks_and_zero_distance_without_gpu():
+    """mt_propagate validates its input on the host, and at z = 0 in real space returns the wave
+    itself (isZero in Propagator::operator()) without touching a GPU."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent / "golden"))
+    from cases import prop_case
+    from multem_b200 import api, capi
+    p = prop_case()
+    out = api.propagate(None, p, 0.0, 1)
+    np.testing.assert_array_equal(out, np.asarray(p.iw_psi).astype(np.complex64))
+    p.iw_type = 4
+    with pytest.raises(capi.MtError) as e:
+        api.propagate(None, p, 10.0, 1)
+    assert e.value.status == 1
+    q = prop_case()
+    with pytest.raises(capi.MtError):
+        api.propagate(None, q, 10.0, 3)

@@ -70,3 +70,30 @@ def test_exit_wave_matches_reference(golden, name, args):
     ref32 = golden[f"{name}_run_p1_psi_coh"][0].T
     assert rel_l2(out, ref64) < 1e-5
     assert rel_l2(out, ref32) < 1e-5
+
+
+@pytest.mark.parametrize("name,tilt", [("prop", False), ("prop_tilt", True)])
+@pytest.mark.parametrize("space", [1, 2])
+def test_propagate_matches_reference(golden, name, tilt, space):
+    """The numpy restatement of Propagator::operator() against the reference's own double path
+    (ilc_propagate semantics) at z = 35 A, plain and with a tilted beam."""
+    from cases import prop_case, prop_tilt_case
+    p = prop_tilt_case() if tilt else prop_case()
+    lam = float(O.wavelength(p.E_0, np.float64))
+    grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)
+    th = O.incident_angle(np.deg2rad(p.theta), lam, min(1 / p.spec_lx, 1 / p.spec_ly))
+    ph = np.deg2rad(p.phi)
+    gx0, gy0 = np.sin(th) * np.cos(ph) / lam, np.sin(th) * np.sin(ph) / lam
+    out = O.propagate_wave(grid, lam, golden["prop_in"], 35.0, space, gx0, gy0)
+    assert rel_l2(out, golden[f"{name}_z35_s{space}_p2"]) < 1e-6
+    assert rel_l2(out, golden[f"{name}_z35_s{space}_p1"]) < 1e-5
+
+
+def test_propagate_zero_distance(golden):
+    """isZero(z): real space returns the wave, reciprocal space FFT2(psi)/N."""
+    from cases import prop_case
+    p = prop_case()
+    grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)
+    lam = O.wavelength(p.E_0, np.float32)
+    assert rel_l2(O.propagate_wave(grid, lam, golden["prop_in"], 0.0, 1), golden["prop_z0_s1_p1"]) < 1e-7
+    assert rel_l2(O.propagate_wave(grid, lam, golden["prop_in"], 0.0, 2), golden["prop_z0_s2_p1"]) < 1e-6
