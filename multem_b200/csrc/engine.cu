@@ -66,8 +66,8 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
 
     m_ = build_model(in);
     const int nx = m_.grid.nx, ny = m_.grid.ny;
-    auto pow2 = [](int n) { return n >= 64 && n <= 2048 && (n & (n - 1)) == 0; };
-    if (!pow2(nx) || !pow2(ny)) fail(MT_ERR_UNSUPPORTED, "nx and ny must be powers of two in [64, 2048]");
+    if (!line_size_supported(nx) || !line_size_supported(ny))
+        fail(MT_ERR_UNSUPPORTED, "nx and ny must be one of 64, 128, 256, 384, 512, 1024, 2048");
     if (m_.is_EW() && !m_.is_plane_wave()) fail(MT_ERR_UNSUPPORTED, "EW simulations need a plane incident wave");
 
     gdev_ = grid_dev(m_.grid);
@@ -80,7 +80,10 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     const size_t nxy = (size_t)nx * ny;
     const int n_thk = (int)m_.thick.size();
     if (m_.is_STEM()) {
-        int bmax = env_int("MTB_BATCH", std::max(1, (int)((size_t)1 << 26) / (int)nxy));
+        // 64 Mi complex values (512 MiB) per batch, a multiple of the row pipeline's 8 groups
+        int bdef = std::max(1, (int)((size_t)1 << 26) / (int)nxy);
+        if (bdef >= 8) bdef -= bdef % 8;
+        int bmax = env_int("MTB_BATCH", bdef);
         batch_ = std::max(1, std::min(bmax, m_.n_scan()));
         const int n_det = (int)m_.det_g_inner.size();
         d_image_.alloc((size_t)n_thk * n_det * m_.n_scan());

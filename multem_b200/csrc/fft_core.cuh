@@ -117,11 +117,26 @@ __device__ __forceinline__ float2 twiddle_const(float2 v) {
     }
 }
 
+// 3-point DFT: y0 = a + t1, y1,2 = (a - t1/2) +- DIR*i*(sqrt(3)/2)*t2, t1 = b + c, t2 = b - c.
+template <int DIR>
+__device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
+    constexpr float h = 0.86602540378443864676f;  // sqrt(3)/2
+    const float2 t1 = cadd(b, c), t2 = csub(b, c);
+    const float2 m = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+    const float2 s = DIR > 0 ? make_float2(-h * t2.y, h * t2.x) : make_float2(h * t2.y, -h * t2.x);
+    a = cadd(a, t1);
+    b = cadd(m, s);
+    c = csub(m, s);
+}
+
 // In-register DFT of length R (natural order in and out), dir = -1 forward, +1 inverse,
-// unnormalised. Radix-4 / radix-2 decimation in time, fully unrolled; trivial twiddles folded.
+// unnormalised. Radix-4 / radix-3 / radix-2 decimation in time, fully unrolled; trivial twiddles
+// folded.
 template <int R, int DIR>
 __device__ __forceinline__ void dft(float2* v) {
     if constexpr (R == 1) {
+    } else if constexpr (R == 3) {
+        dft3<DIR>(v[0], v[1], v[2]);
     } else if constexpr (R == 2) {
         float2 a = v[0], b = v[1];
         v[0] = cadd(a, b);
@@ -161,7 +176,29 @@ __device__ __forceinline__ void dft(float2* v) {
             v[k + Q] = cadd(s1, s3);
             v[k + 3 * Q] = csub(s1, s3);
         });
+    } else if constexpr (R % 3 == 0) {
+        // radix-3 DIT: X[k + m*Q] = DFT3 over r of w_R^(k*r) * S_r[k], S_r = DFT_Q of v[3i + r]
+        constexpr int Q = R / 3;
+        float2 a[Q], b[Q], c[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            a[i] = v[3 * i];
+            b[i] = v[3 * i + 1];
+            c[i] = v[3 * i + 2];
+        }
+        dft<Q, DIR>(a);
+        dft<Q, DIR>(b);
+        dft<Q, DIR>(c);
+        static_for<0, Q>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            float2 x0 = a[k], x1 = twiddle_const<k, R, DIR>(b[k]), x2 = twiddle_const<2 * k, R, DIR>(c[k]);
+            dft3<DIR>(x0, x1, x2);
+            v[k] = x0;
+            v[k + Q] = x1;
+            v[k + 2 * Q] = x2;
+        });
     } else {
+        static_assert(R % 2 == 0, "radix must factor into 2, 3 and 4");
         constexpr int H = R / 2;
         float2 e[H], o[H];
 #pragma unroll
@@ -192,6 +229,7 @@ struct LinePlan;
 template <> struct LinePlan<64>   { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 4, 1}; };
 template <> struct LinePlan<128>  { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 8, 1}; };
 template <> struct LinePlan<256>  { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 16, 1}; };
+template <> struct LinePlan<384>  { static constexpr int E = 24, T = 256, B = 2, NS = 3; static constexpr int R[3] = {24, 4, 4}; };
 template <> struct LinePlan<512>  { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 16, 1}; };
 template <> struct LinePlan<1024> { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 32, 1}; };
 template <> struct LinePlan<2048> { static constexpr int E = 32, T = 256, B = 2, NS = 3; static constexpr int R[3] = {32, 8, 8}; };

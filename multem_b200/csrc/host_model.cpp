@@ -444,13 +444,18 @@ float Model::phonon_weight() const {
 // read_input_multislice + validate_parameters (mex_files_multem/ilc_multem.cu:38-379,
 // src/input_multislice.cuh:622-796) for the simulation types, slicing and incident waves this
 // engine implements; anything else is rejected with MT_ERR_UNSUPPORTED.
+// Line lengths with a compiled FFT plan (LinePlan in fft_core.cuh).
+bool line_size_supported(int n) {
+    return n == 64 || n == 128 || n == 256 || n == 384 || n == 512 || n == 1024 || n == 2048;
+}
+
 // read_input_multislice of ilc_propagate (mex_files_multem/ilc_propagate.cu:34-95): the grid from
 // spec_lx/ly and nx/ny (lz = 0, dz = 0.25, no band-width limit, periodic), the user wave, E_0 and
 // the beam tilt; nothing of the specimen is read.
 Model build_prop_model(const mt_input_multislice* in) {
     if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
-    auto pow2 = [](int n) { return n >= 64 && n <= 2048 && (n & (n - 1)) == 0; };
-    if (!pow2(in->nx) || !pow2(in->ny)) fail(MT_ERR_UNSUPPORTED, "nx and ny must be powers of two in [64, 2048]");
+    if (!line_size_supported(in->nx) || !line_size_supported(in->ny))
+        fail(MT_ERR_UNSUPPORTED, "nx and ny must be one of 64, 128, 256, 384, 512, 1024, 2048");
     if (!(in->spec_lx > 0) || !(in->spec_ly > 0)) fail(MT_ERR_INVALID_ARG, "spec_lx and spec_ly must be positive");
     if (in->iw_type != 3 || !in->iw_psi)
         fail(MT_ERR_INVALID_ARG, "propagation needs a user-defined wave (iw_type 3 with iw_psi)");

@@ -157,6 +157,8 @@ struct Model {
 
 // Validate `in` like read_input_multislice + validate_parameters; throws mtb::Error.
 Model build_model(const mt_input_multislice* in);
+// Line lengths with a compiled FFT plan: 64, 128, 256, 384, 512, 1024, 2048.
+bool line_size_supported(int n);
 // The fields ilc_propagate reads (grid, user wave, E_0, tilt); throws mtb::Error.
 Model build_prop_model(const mt_input_multislice* in);
 

@@ -234,10 +234,11 @@ static int lines_per_cta(int n) {
         case 64: return lines_per_cta<64>();
         case 128: return lines_per_cta<128>();
         case 256: return lines_per_cta<256>();
+        case 384: return lines_per_cta<384>();
         case 512: return lines_per_cta<512>();
         case 1024: return lines_per_cta<1024>();
         case 2048: return lines_per_cta<2048>();
-        default: fail(MT_ERR_UNSUPPORTED, "grid sizes must be one of 64, 128, 256, 512, 1024, 2048");
+        default: fail(MT_ERR_UNSUPPORTED, "grid sizes must be one of 64, 128, 256, 384, 512, 1024, 2048");
     }
     return 0;
 }
@@ -250,10 +251,11 @@ int col_det_width(int nx) {
         case 64: return cols_det_width<64>();
         case 128: return cols_det_width<128>();
         case 256: return cols_det_width<256>();
+        case 384: return cols_det_width<384>();
         case 512: return cols_det_width<512>();
         case 1024: return cols_det_width<1024>();
         case 2048: return cols_det_width<2048>();
-        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 512, 1024, 2048");
+        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 384, 512, 1024, 2048");
     }
     return 0;
 }
@@ -270,10 +272,11 @@ void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStre
         case 64: rows_dispatch_mode<64>(mode, a, grid_ctas, s); break;
         case 128: rows_dispatch_mode<128>(mode, a, grid_ctas, s); break;
         case 256: rows_dispatch_mode<256>(mode, a, grid_ctas, s); break;
+        case 384: rows_dispatch_mode<384>(mode, a, grid_ctas, s); break;
         case 512: rows_dispatch_mode<512>(mode, a, grid_ctas, s); break;
         case 1024: rows_dispatch_mode<1024>(mode, a, grid_ctas, s); break;
         case 2048: rows_dispatch_mode<2048>(mode, a, grid_ctas, s); break;
-        default: fail(MT_ERR_UNSUPPORTED, "ny must be one of 64, 128, 256, 512, 1024, 2048");
+        default: fail(MT_ERR_UNSUPPORTED, "ny must be one of 64, 128, 256, 384, 512, 1024, 2048");
     }
 }
 
@@ -283,10 +286,11 @@ void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_
         case 64: cols_dispatch_flags<64>(flags, a, grid_ctas, s); break;
         case 128: cols_dispatch_flags<128>(flags, a, grid_ctas, s); break;
         case 256: cols_dispatch_flags<256>(flags, a, grid_ctas, s); break;
+        case 384: cols_dispatch_flags<384>(flags, a, grid_ctas, s); break;
         case 512: cols_dispatch_flags<512>(flags, a, grid_ctas, s); break;
         case 1024: cols_dispatch_flags<1024>(flags, a, grid_ctas, s); break;
         case 2048: cols_dispatch_flags<2048>(flags, a, grid_ctas, s); break;
-        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 512, 1024, 2048");
+        default: fail(MT_ERR_UNSUPPORTED, "nx must be one of 64, 128, 256, 384, 512, 1024, 2048");
     }
 }
 

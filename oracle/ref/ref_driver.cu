@@ -188,13 +188,13 @@ void fill_input(const mt_input_multislice* in, mt::Input_Multislice<T>& im, int 
 }
 
 template <class V>
-void copy_real(const V& v, double* dst) {
-    for (size_t i = 0; i < v.size(); i++) dst[i] = (double)v[i];
+void copy_real(const V& v, double* dst, size_t n = (size_t)-1) {
+    for (size_t i = 0; i < v.size() && i < n; i++) dst[i] = (double)v[i];
 }
 
 template <class V>
-void copy_cplx(const V& v, double* dst) {
-    for (size_t i = 0; i < v.size(); i++) {
+void copy_cplx(const V& v, double* dst, size_t n = (size_t)-1) {
+    for (size_t i = 0; i < v.size() && i < n; i++) {
         dst[2 * i] = (double)v[i].real();
         dst[2 * i + 1] = (double)v[i].imag();
     }
@@ -242,12 +242,14 @@ int run(const mt_input_multislice* in, int nthreads, mt_output_multislice* out, 
     for (size_t ithk = 0; ithk < om.thick.size(); ithk++) {
         if (out->image_tot && om.image_tot.size())
             for (int idet = 0; idet < om.ndetector; idet++)
-                copy_real(om.image_tot[ithk].image[idet], out->image_tot + (ithk * om.ndetector + idet) * nxy);
+                copy_real(om.image_tot[ithk].image[idet], out->image_tot + (ithk * om.ndetector + idet) * nxy, nxy);
         if (out->image_coh && om.image_coh.size())
             for (int idet = 0; idet < om.ndetector; idet++)
-                copy_real(om.image_coh[ithk].image[idet], out->image_coh + (ithk * om.ndetector + idet) * nxy);
-        if (out->m2psi_tot && om.m2psi_tot.size()) copy_real(om.m2psi_tot[ithk], out->m2psi_tot + ithk * nxy);
-        if (out->psi_coh && om.psi_coh.size()) copy_cplx(om.psi_coh[ithk], out->psi_coh + 2 * ithk * nxy);
+                copy_real(om.image_coh[ithk].image[idet], out->image_coh + (ithk * om.ndetector + idet) * nxy, nxy);
+        if (out->m2psi_tot && om.m2psi_tot.size()) copy_real(om.m2psi_tot[ithk], out->m2psi_tot + ithk * nxy, nxy);
+        // psi_coh is held at the full grid size; like set_struct_multislice (ilc_multem.cu:382-481)
+        // only the first nx*ny values of the output area are returned
+        if (out->psi_coh && om.psi_coh.size()) copy_cplx(om.psi_coh[ithk], out->psi_coh + 2 * ithk * nxy, nxy);
     }
     return 0;
 }

@@ -25,3 +25,19 @@ def prop_tilt_case():
     p = prop_case()
     p.theta, p.phi = 0.5, 30.0
     return p
+
+
+def ew_384x256():
+    """Exit wave of Si(001) on a 384 x 256 grid (radix-3 rows against radix-2 columns), written to
+    a 128 x 96 output window (cropping and fft-shift of the output area)."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=384, ny=256, na=4, nb=3, nc=4)
+    p.output_area_ix_0, p.output_area_ix_e = 101, 228
+    p.output_area_iy_0, p.output_area_iy_e = 81, 176
+    return p
+
+
+def stem_384():
+    """STEM ADF through SrTiO3(001) on a 384^2 grid, 3 x 3 probes, two phonon configurations."""
+    from multem_b200 import specimens
+    return specimens.stem_srtio3(nx=384, ny=384, na=4, nb=4, nc=4, ns=3, nconf=2, seed=5)

@@ -21,7 +21,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from multem_b200 import specimens  # noqa: E402
-from cases import prop_case, prop_tilt_case  # noqa: E402
+from cases import ew_384x256, prop_case, prop_tilt_case, stem_384  # noqa: E402
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -97,6 +97,15 @@ def main():
                 for prec in ((1, 2) if z != 0 else (1,)):
                     r = R.propagate(q, z, space, prec)
                     rec[f"{name}_z{int(z)}_s{space}_p{prec}"] = r.astype(np.complex64) if prec == 1 else r
+    # full runs on a radix-3 grid (float outputs only, single precision storage)
+    for name, fn in (("ew_384x256", ew_384x256), ("stem_384", stem_384)):
+        p = fn()
+        for prec in (1, 2):
+            out = R.run(p, precision=prec, nthreads=8)
+            for k in ("image_tot", "psi_coh", "m2psi_tot", "thick", "x", "y"):
+                if k in out:
+                    v = out[k]
+                    rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
     # full runs
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
                      ("ew_config1", ew_config1)):
