@@ -199,6 +199,16 @@ mt_status mt_output_query(const mt_input_multislice* in, mt_output_dims* dims);
 mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislice* in,
                             mt_output_multislice* out);
 
+/* Run n independent simulations (different specimens, grids, simulation types), each like
+ * mt_multislice_run on in[i] -> out[i]. The reference runs one input per call
+ * (mex_files_multem/ilc_multem.cu:484-546); this batched form has no counterpart there. Inputs are
+ * taken largest first by several host workers, each with its own engine and CUDA stream on
+ * conf->gpu_device, so small simulations overlap on the GPU (MTB_BATCH_WORKERS, default 4).
+ * status[i] (optional) receives each run's status; the return value is MT_OK or the first failure
+ * in input order, with mt_last_error() naming that input. */
+mt_status mt_multislice_run_batch(const mt_system_conf* conf, int n, const mt_input_multislice* in,
+                                  mt_output_multislice* out, mt_status* status);
+
 /* Handle-based form: set-up once (tables, specimen, buffers), run many times.
  * mt_engine_create = Multislice::set_input_data (src/tem_simulation.cuh:51-69). */
 mt_status mt_engine_create(const mt_system_conf* conf, const mt_input_multislice* in, mt_engine** eng);

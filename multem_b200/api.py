@@ -86,6 +86,31 @@ def ilc_multem(system_conf: SystemConf | None, params: Parameters) -> dict:
     return buf.to_dict()
 
 
+def ilc_multem_batch(system_conf: SystemConf | None, params_list) -> list:
+    """Run several simulations in one call (mt_multislice_run_batch): largest first, overlapping
+    on the GPU. Returns one output dict per input (as ilc_multem); raises on the first failure."""
+    lib = capi.load()
+    n = len(params_list)
+    ins = (capi.MtInputMultislice * max(1, n))()
+    outs = (capi.MtOutputMultislice * max(1, n))()
+    keep, bufs = [], []
+    for i, p in enumerate(params_list):
+        s, k = p.to_c()
+        keep.append((s, k))
+        ins[i] = s
+        b = OutputBuffers(output_dims(p))
+        bufs.append(b)
+        outs[i] = b.c
+    status = (C.c_int * max(1, n))()
+    conf = _conf(system_conf)
+    capi.check(lib.mt_multislice_run_batch(C.byref(conf), n, ins, outs, status))
+    res = []
+    for i, b in enumerate(bufs):
+        b.c = outs[i]
+        res.append(b.to_dict())
+    return res
+
+
 class Engine:
     """Handle-based engine: set-up once, run configurations, read FP64 accumulators."""
 

@@ -99,6 +99,8 @@ SIGNATURES = {
     "mt_output_query": (c_int, [C.POINTER(MtInputMultislice), C.POINTER(MtOutputDims)]),
     "mt_multislice_run": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice),
                                   C.POINTER(MtOutputMultislice)]),
+    "mt_multislice_run_batch": (c_int, [C.POINTER(MtSystemConf), c_int, C.POINTER(MtInputMultislice),
+                                        C.POINTER(MtOutputMultislice), P_int]),
     "mt_engine_create": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), C.POINTER(_VP)]),
     "mt_engine_run": (c_int, [_VP, C.POINTER(MtOutputMultislice)]),
     "mt_engine_run_confs": (c_int, [_VP, c_int, c_int]),

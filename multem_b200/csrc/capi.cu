@@ -1,5 +1,9 @@
 // extern "C" entry points declared in include/multem_b200.h.
+#include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include <exception>
 #include <memory>
@@ -165,6 +169,53 @@ mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislic
         e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
         e.write_output(out);
     });
+}
+
+mt_status mt_multislice_run_batch(const mt_system_conf* conf, int n, const mt_input_multislice* in,
+                                  mt_output_multislice* out, mt_status* status) {
+    std::vector<mt_status> st(n > 0 ? n : 0, MT_OK);
+    std::vector<std::string> msg(st.size());
+    mt_status rc = guarded([&] {
+        if (n < 0 || (n > 0 && (!in || !out))) mtb::fail(MT_ERR_INVALID_ARG, "bad batch arguments");
+        const mt_system_conf c = conf ? *conf : default_conf();
+        // largest first: grid points x probes x configurations x slices (from the box depth)
+        std::vector<double> cost(n);
+        for (int i = 0; i < n; i++) {
+            const mt_input_multislice& q = in[i];
+            double probes = (q.simulation_type == 11) ? (double)std::max(1, q.scanning_ns) * std::max(1, q.scanning_ns) : 1;
+            double slices = (q.spec_dz > 0 && q.spec_lz > 0) ? q.spec_lz / q.spec_dz : 1;
+            cost[i] = (double)q.nx * q.ny * probes * std::max(1, q.pn_nconf) * slices;
+        }
+        std::vector<int> order(n);
+        for (int i = 0; i < n; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        const char* w = std::getenv("MTB_BATCH_WORKERS");
+        const int workers = std::max(1, std::min(n, w ? std::atoi(w) : 4));
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (;;) {
+                const int k = next++;
+                if (k >= n) break;
+                const int i = order[k];
+                st[i] = guarded([&] {
+                    MTB_CUDA(cudaSetDevice(c.gpu_device));
+                    mtb::Engine e(&c, &in[i]);
+                    e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
+                    e.write_output(&out[i]);
+                });
+                if (st[i] != MT_OK) msg[i] = g_last_error;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < workers; t++) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (int i = 0; i < n; i++)
+            if (st[i] != MT_OK) throw mtb::Error(st[i], "input " + std::to_string(i) + ": " + msg[i]);
+    });
+    if (status)
+        for (int i = 0; i < n; i++) status[i] = st[i];
+    return rc;
 }
 
 mt_status mt_projected_potential(const mt_system_conf* conf, const mt_input_multislice* in, int iconf, int islice,

@@ -76,4 +76,14 @@ void dev_free(void* p, int dev) {
     if (cur != dev) cudaSetDevice(cur);
 }
 
+void dev_free_idle(void* p, int dev) {
+    if (!p) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaFreeAsync(p, pool_of(dev).stream);
+    cudaStreamSynchronize(pool_of(dev).stream);
+    if (cur != dev) cudaSetDevice(cur);
+}
+
 }  // namespace mtb

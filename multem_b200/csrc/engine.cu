@@ -132,10 +132,18 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
 Engine::~Engine() {
     if (stream_) {
         cudaStreamSynchronize(stream_);
+        // everything below was used on stream_ only: return it to the pool without a device-wide wait
+        for (auto& cd : confs_) cd.release_idle();
+        for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
+        for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_}) b->release_idle();
+        for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
+        d_err_.release_idle();
+        d_scan_idx_.release_idle();
         for (auto& t : tl_) {
             cudaEventDestroy(t.a);
             cudaEventDestroy(t.b);
         }
+        if (conf_done_) cudaEventDestroy(conf_done_);
         if (run_a_) cudaEventDestroy(run_a_);
         if (run_b_) cudaEventDestroy(run_b_);
         cudaStreamDestroy(stream_);
@@ -389,13 +397,26 @@ void Engine::timing(double* total_ms, double* rows_ms, long long* n_rows, double
 void Engine::run_confs(int c0, int c1) {
     if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
     long long l0 = launches_issued();
+    // configuration c is prepared on the host while c-1 runs; c-1's buffers go back to the pool once
+    // its last launch has completed
+    if (!conf_done_) MTB_CUDA(cudaEventCreateWithFlags(&conf_done_, cudaEventDisableTiming));
+    ConfData prev;
+    bool have_prev = false;
     for (int c = c0; c <= c1; c++) {
         ConfData cd;
         prepare_conf(cd, c);
         run_conf(cd);
+        if (have_prev) {
+            MTB_CUDA(cudaEventSynchronize(conf_done_));
+            prev.release_idle();
+        }
+        MTB_CUDA(cudaEventRecord(conf_done_, stream_));
+        prev = std::move(cd);
+        have_prev = true;
     }
     launches_ = launches_issued() - l0;
     synchronize();
+    prev.release_idle();
 }
 
 void Engine::run_conf(ConfData& cd) {

@@ -40,6 +40,12 @@ struct DevBuf {
         p = static_cast<T*>(dev_alloc(sizeof(T) * (count ? count : 1), &dev));
         n = count;
     }
+    // free now; the owner has synchronised every stream that used the buffer
+    void release_idle() {
+        if (p) dev_free_idle(p, dev);
+        p = nullptr;
+        n = 0;
+    }
     void upload(const T* h, size_t count, cudaStream_t s) {
         alloc(count);
         if (count) cuda_check(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
@@ -64,6 +70,11 @@ struct ConfData {
     DevBuf<float4> atoms;
     DevBuf<int2> ranges;
     DevBuf<float2> prop;            // per slice: Px[nx] then Py[ny]
+    void release_idle() {
+        atoms.release_idle();
+        ranges.release_idle();
+        prop.release_idle();
+    }
 };
 
 mt_output_dims output_dims(const Model& m);
@@ -108,6 +119,7 @@ class Engine {
     std::vector<TimedLaunch> tl_;
     size_t tl_used_ = 0;
     cudaEvent_t run_a_ = nullptr, run_b_ = nullptr;
+    cudaEvent_t conf_done_ = nullptr;  // last launch of the previous configuration in run_confs
     void tl_begin(int kind);
     void tl_end();
     void rows(RowMode mode, const RowArgs& a);

@@ -231,7 +231,7 @@ template <> struct LinePlan<128>  { static constexpr int E = 16, T = 256, B = 2,
 template <> struct LinePlan<256>  { static constexpr int E = 16, T = 256, B = 2, NS = 2; static constexpr int R[3] = {16, 16, 1}; };
 template <> struct LinePlan<384>  { static constexpr int E = 24, T = 256, B = 2, NS = 3; static constexpr int R[3] = {24, 4, 4}; };
 template <> struct LinePlan<512>  { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 16, 1}; };
-template <> struct LinePlan<1024> { static constexpr int E = 32, T = 256, B = 2, NS = 2; static constexpr int R[3] = {32, 32, 1}; };
+template <> struct LinePlan<1024> { static constexpr int E = 32, T = 512, B = 1, NS = 2; static constexpr int R[3] = {32, 32, 1}; };
 template <> struct LinePlan<2048> { static constexpr int E = 32, T = 256, B = 2, NS = 3; static constexpr int R[3] = {32, 8, 8}; };
 
 // Radix of stage s of a transform whose stage order is `rev` ? reversed : plan order.

@@ -28,14 +28,13 @@ long long launches_issued() { return g_launches.load(); }
 void note_launch() { g_launches++; }
 
 void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
         MTB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
         if (q != cudaDriverEntryPointSuccess || !fn) fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
     // float32 [nprobe][nx][2*ldy]; box: 2w floats (w complex columns) x boxr rows x 1 probe
     const cuuint64_t dims[3] = {(cuuint64_t)2 * ldy, (cuuint64_t)nx, (cuuint64_t)nprobe};
     const cuuint64_t strides[2] = {(cuuint64_t)2 * ldy * sizeof(float), (cuuint64_t)2 * ldy * nx * sizeof(float)};

@@ -669,15 +669,16 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
 void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr);
 
 // ---------------------------------------------------------------------------------------------
-// launch helpers
+// launch helpers (the per-kernel occupancy caps are function-local statics, initialised once and
+// thread-safe, so engines on several host threads may launch concurrently)
 template <class K>
 static int max_ctas(K kernel, int threads, size_t smem) {
-    static int nsm = 0;
-    if (nsm == 0) {
-        int dev = 0;
+    static const int nsm = [] {
+        int dev = 0, n = 0;
         MTB_CUDA(cudaGetDevice(&dev));
-        MTB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    }
+        MTB_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+        return n;
+    }();
     MTB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     MTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem));
@@ -697,8 +698,7 @@ static void rows_launch(const RowArgs& a, int grid_ctas, cudaStream_t s) {
         if (a.err && a.nprobe % S::NG == 0) {
             constexpr size_t sm = RP::SMEM;
             auto kern = rows_pipe_kernel<NY, MODE, S::GT, S::NG, S::EARLY>;
-            static int cap = 0;
-            if (cap == 0) cap = max_ctas(kern, S::GT * S::NG, sm);
+            static const int cap = max_ctas(kern, S::GT * S::NG, sm);
             const int units = (a.nx / RP::LPC) * a.nprobe / S::NG;
             int grid = grid_ctas > 0 ? grid_ctas : cap;
             if (grid > units) grid = units;
@@ -709,8 +709,7 @@ static void rows_launch(const RowArgs& a, int grid_ctas, cudaStream_t s) {
         }
     }
     const size_t sm = rows_smem<NY>();
-    static int cap = 0;
-    if (cap == 0) cap = max_ctas(rows_kernel<NY, MODE>, G::THREADS, sm);
+    static const int cap = max_ctas(rows_kernel<NY, MODE>, G::THREADS, sm);
     const int items = (a.nx / G::LPC) * a.nprobe;
     int grid = grid_ctas > 0 ? grid_ctas : cap;
     if (grid > items) grid = items;
@@ -738,8 +737,7 @@ static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
         if (a.err) {
             constexpr size_t sm = CP::SMEM;
             auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG>;
-            static int cap = 0;
-            if (cap == 0) cap = max_ctas(kern, S::GT * S::NG, sm);
+            static const int cap = max_ctas(kern, S::GT * S::NG, sm);
             const int items = (a.ny / CP::W) * a.nprobe;
             int grid = grid_ctas > 0 ? grid_ctas : cap;
             if (grid > items) grid = items;
@@ -752,8 +750,7 @@ static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
         }
     }
     const size_t sm = cols_smem<NX, FLAGS>();
-    static int cap = 0;
-    if (cap == 0) cap = max_ctas(cols_kernel<NX, FLAGS, LDY>, G::THREADS, sm);
+    static const int cap = max_ctas(cols_kernel<NX, FLAGS, LDY>, G::THREADS, sm);
     const int items = (a.ny / G::LPC) * a.nprobe;
     int grid = grid_ctas > 0 ? grid_ctas : cap;
     if (grid > items) grid = items;

@@ -232,8 +232,8 @@ void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& head
     build_tables_kernel<<<n, 128, 3 * nR * sizeof(double), stream>>>(d_coef, d_head, n, nR, d_tab);
     MTB_CUDA(cudaGetLastError());
     MTB_CUDA(cudaStreamSynchronize(stream));
-    dev_free(d_coef, dev);
-    dev_free(d_head, dev);
+    dev_free_idle(d_coef, dev);  // only `stream` used them
+    dev_free_idle(d_head, dev);
 }
 
 // ---------------------------------------------------------------------------------------------

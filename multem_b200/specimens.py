@@ -164,3 +164,61 @@ def stem_srtio3(nx: int = 512, ny: int = 512, na: int = 8, nb: int = 8, nc: int 
     p.detector = {"type": 1, "cir": [{"inner_ang": 40.0, "outer_ang": 80.0},
                                      {"inner_ang": 80.0, "outer_ang": 200.0}]}
     return p
+
+
+FCC_Z = (13, 28, 29, 46, 47, 78, 79)
+
+
+def fcc_batch(n: int = 32, seed: int = 3, grids=(256, 384, 512, 1024), ns: int = 8, nconf: int = 8):
+    """Seeded batch of fcc(001) specimens of uneven size: lattice constant a ~ U[3.8, 4.1] A,
+    Z from FCC_Z, thickness ~ U[5, 30] nm, grids cycling through `grids` (about 0.06 A per pixel,
+    so the box grows with the grid), 200 or 300 kV, alternately plane-wave exit waves (EWRS) and
+    STEM ADF (ns x ns raster over one cell, 21 mrad, detectors 40-80 and 80-200 mrad), `nconf`
+    frozen-phonon configurations with sigma = 0.085 A, dz_Proj slices of a/2."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        a = float(rng.uniform(3.8, 4.1))
+        Z = int(rng.choice(FCC_Z))
+        t_nm = float(rng.uniform(5.0, 30.0))
+        nx = int(grids[i % len(grids)])
+        na = max(1, int(round(nx * 0.06 / a)))
+        nc = max(1, int(round(t_nm * 10.0 / a)))
+        E_0 = 200.0 if rng.uniform() < 0.5 else 300.0
+        cell = fcc_001(Z, a)
+        atoms = crystal(cell, na, na, nc, sigma=0.085)
+        p = Parameters()
+        p.pn_model = 3
+        p.pn_coh_contrib = 0
+        p.pn_single_conf = 0
+        p.pn_nconf = nconf
+        p.pn_dim = 110
+        p.pn_seed = 100 + i
+        p.spec_atoms = atoms
+        p.spec_lx = p.spec_ly = na * a
+        p.spec_lz = nc * a
+        p.spec_dz = a / 2
+        p.potential_slicing = 2
+        p.thick_type = 1
+        p.nx = p.ny = nx
+        p.bwl = 0
+        p.E_0 = E_0
+        if i % 2 == 0:
+            p.simulation_type = 52
+            p.iw_type = 1
+        else:
+            p.simulation_type = 11
+            p.iw_type = 2
+            p.cond_lens_outer_aper_ang = 21.0
+            p.cond_lens_zero_defocus_type = 1
+            p.scanning_type = 2
+            p.scanning_periodic = 1
+            p.scanning_square_pxs = 1
+            p.scanning_ns = ns
+            x0 = (na // 2) * a
+            p.scanning_x0, p.scanning_y0 = x0, x0
+            p.scanning_xe, p.scanning_ye = x0 + a, x0 + a
+            p.detector = {"type": 1, "cir": [{"inner_ang": 40.0, "outer_ang": 80.0},
+                                             {"inner_ang": 80.0, "outer_ang": 200.0}]}
+        out.append(p)
+    return out

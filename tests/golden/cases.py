@@ -41,3 +41,18 @@ def stem_384():
     """STEM ADF through SrTiO3(001) on a 384^2 grid, 3 x 3 probes, two phonon configurations."""
     from multem_b200 import specimens
     return specimens.stem_srtio3(nx=384, ny=384, na=4, nb=4, nc=4, ns=3, nconf=2, seed=5)
+
+
+def ew_1024():
+    """Exit wave of Si(001) on a 1024^2 grid (41.5 x 41.5 A) with a 128 x 128 output window."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=1024, ny=1024, na=8, nb=8, nc=2)
+    p.output_area_ix_0, p.output_area_ix_e = 449, 577
+    p.output_area_iy_0, p.output_area_iy_e = 449, 577
+    return p
+
+
+def stem_1024():
+    """STEM ADF through SrTiO3(001) on a 1024^2 grid, 2 x 2 probes, one phonon configuration."""
+    from multem_b200 import specimens
+    return specimens.stem_srtio3(nx=1024, ny=1024, na=8, nb=8, nc=3, ns=2, nconf=1, seed=9)

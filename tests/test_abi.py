@@ -52,3 +52,27 @@ def test_propagate_host_checks_and_zero_distance_without_gpu():
     q = prop_case()
     with pytest.raises(capi.MtError):
         api.propagate(None, q, 10.0, 3)
+
+
+def test_batch_reports_per_input_status():
+    """A batch with an unsupported input reports it by index and fills every status entry."""
+    import ctypes as C
+    from multem_b200 import specimens
+    lib = capi.load()
+    good = specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    bad = specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    bad.nx = 100
+    ins = (capi.MtInputMultislice * 2)()
+    keep = []
+    for i, p in enumerate((good, bad)):
+        s, k = p.to_c()
+        keep.append((s, k))
+        ins[i] = s
+    outs = (capi.MtOutputMultislice * 2)()
+    status = (C.c_int * 2)(-1, -1)
+    rc = lib.mt_multislice_run_batch(None, 2, ins, outs, status)
+    assert rc != 0
+    assert all(v != -1 for v in status)
+    assert status[1] != 0
+    assert b"input" in lib.mt_last_error()
+    assert lib.mt_multislice_run_batch(None, -1, ins, outs, None) == 1
