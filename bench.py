@@ -15,7 +15,9 @@ max over ranks. The probe batch (512 MiB) exceeds the 126 MB L2, so no flush is 
 steps.
 
 --impl reference times the reference's own CPU path (oracle/_ref: MULTEM's Multislice<float, e_host>
-compiled from its sources with an FFTW-API shim) on a bounded sample of the same workload.
+compiled from its sources with an FFTW-API shim) on a bounded sample of the same workload;
+--impl reference --ref-gpu times the reference's own GPU path (Multislice<float, e_device>, built for
+sm_100a into the same library) on 1024-probe samples instead.
 """
 from __future__ import annotations
 
@@ -140,6 +142,39 @@ def cpu_reference_sample(n_probe_side=2, nthreads=None):
     return n_upd / dt, dt, desc, nthreads
 
 
+def gpu_reference_sample(n_probe_side):
+    """The reference's own GPU path (Multislice<float, e_device>, cuFFT, built for sm_100a into
+    oracle/_ref) on an n x n probe raster x 1 phonon x 50 slices of the workload, through its
+    run_multislice entry (set-up included, as a caller of ilc_multem pays it)."""
+    from oracle import reference as R
+    p = workload(1)
+    p.scanning_ns = n_probe_side
+    a = 3.905
+    p.scanning_xe = p.scanning_ye = p.scanning_x0 + a * n_probe_side / 64.0
+    t0 = time.perf_counter()
+    R.run(p, precision=1, device=True)
+    return time.perf_counter() - t0
+
+
+def run_reference_gpu(args):
+    ns = 32
+    for _ in range(args.warmup):
+        gpu_reference_sample(4)
+    t_all = sum(gpu_reference_sample(ns) for _ in range(args.steps))
+    value = args.steps * ns * ns * N_SLICE / t_all
+    sample = (f"{ns * ns} probes x 1 phonon x {N_SLICE} slices of the 512^2 SrTiO3 workload per step, through the "
+              f"reference's GPU path (float, cuFFT, per-probe slice loop), set-up included")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "SrTiO3 (001) 8x8x25, 512^2, 50 slices, 4096-probe raster, 16 phonons "
+                                   f"(each reference step: {ns * ns} probes x 1 phonon)", "parallelism": "1 gpu"},
+            "impl": "reference", "device": "gpu", "sample": sample,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -148,6 +183,8 @@ def run_reference(args):
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmultem_ref.so is not built"}))
         return 0
+    if args.ref_gpu:
+        return run_reference_gpu(args)
     for _ in range(args.warmup):
         cpu_reference_sample(1)
     vals = []
@@ -290,6 +327,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="with --impl reference: time the reference's own GPU path instead of its CPU path")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

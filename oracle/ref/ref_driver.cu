@@ -19,6 +19,7 @@
 #include "propagator.cuh"
 
 #include <cstring>
+#include <stdexcept>
 #include <exception>
 #include <string>
 
@@ -76,11 +77,21 @@ void fill_lens(const mt_lens& l, mt::Lens<T>& lens, T E_0, mt::Grid_2d<T>& grid)
 // struct instead of a MATLAB struct. The objective lens takes its source-spread fields from the
 // cond_lens_* values, as the reference does at ilc_multem.cu:250-254.
 template <class T>
-void fill_input(const mt_input_multislice* in, mt::Input_Multislice<T>& im, int nthreads) {
+void fill_input(const mt_input_multislice* in, mt::Input_Multislice<T>& im, int nthreads,
+                mt::eDevice dev = mt::e_host) {
     im.system_conf.precision = std::is_same<T, float>::value ? mt::eP_float : mt::eP_double;
-    im.system_conf.device = mt::e_host;
+    im.system_conf.device = dev;
     im.system_conf.cpu_nthread = nthreads;
+    if (dev == mt::e_device) {
+        // read_system_conf (src/matlab_mex.cuh:263-288): one stream, the requested GPU
+        im.system_conf.gpu_device = 0;
+        im.system_conf.gpu_nstream = 0;
+    }
     im.system_conf.validate_parameters();
+    if (dev == mt::e_device) {
+        if (!im.system_conf.is_device()) throw std::runtime_error("no GPU for the reference's device path");
+        im.system_conf.set_device();
+    }
 
     im.simulation_type = static_cast<mt::eTEM_Sim_Type>(in->simulation_type);
     im.interaction_model = static_cast<mt::eElec_Spec_Int_Model>(in->interaction_model);
@@ -200,16 +211,16 @@ void copy_cplx(const V& v, double* dst, size_t n = (size_t)-1) {
     }
 }
 
-template <class T>
+template <class T, mt::eDevice dev = mt::e_host>
 int run(const mt_input_multislice* in, int nthreads, mt_output_multislice* out, mt_output_dims* dims) {
     mt::Input_Multislice<T> im;
-    fill_input(in, im, nthreads);
+    fill_input(in, im, nthreads, dev);
     mt::Output_Multislice<T> om;
-    mt::Stream<mt::e_host> stream(im.system_conf.nstream);
-    mt::FFT<T, mt::e_host> fft_2d;
+    mt::Stream<dev> stream(im.system_conf.nstream);
+    mt::FFT<T, dev> fft_2d;
     fft_2d.create_plan_2d(im.grid_2d.ny, im.grid_2d.nx, im.system_conf.nstream);
-    mt::Multislice<T, mt::e_host>::ext_stop_sim = false;
-    mt::Multislice<T, mt::e_host> sim;
+    mt::Multislice<T, dev>::ext_stop_sim = false;
+    mt::Multislice<T, dev> sim;
     sim.set_input_data(&im, &stream, &fft_2d);
     om.set_input_data(&im);
     if (out != nullptr) {
@@ -293,6 +304,13 @@ const char* mtref_last_error(void) { return g_err.c_str(); }
 // Full simulation; precision 1 = float, 2 = double.
 int mtref_run(const mt_input_multislice* in, int precision, int nthreads, mt_output_multislice* out) {
     return guarded([&] { return precision == 2 ? run<double>(in, nthreads, out, nullptr) : run<float>(in, nthreads, out, nullptr); });
+}
+
+// The reference's own GPU path (run_multislice<float, e_device>, mex_files_multem/ilc_multem.cu:
+// 484-518 and :538-541): Multislice<float, e_device> with cuFFT, one stream, GPU 0. Used only as a
+// timed baseline.
+int mtref_run_device(const mt_input_multislice* in, mt_output_multislice* out) {
+    return guarded([&] { return run<float, mt::e_device>(in, 1, out, nullptr); });
 }
 
 int mtref_output_dims(const mt_input_multislice* in, int precision, mt_output_dims* dims) {

@@ -32,6 +32,7 @@ def lib():
         L.mtref_last_error.restype = C.c_char_p
         L.mtref_run.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, P(capi.MtOutputMultislice)]
         L.mtref_output_dims.argtypes = [P(capi.MtInputMultislice), C.c_int, P(capi.MtOutputDims)]
+        L.mtref_run_device.argtypes = [P(capi.MtInputMultislice), P(capi.MtOutputMultislice)]
         L.mtref_params.argtypes = [P(capi.MtInputMultislice), C.c_int, capi.P_double, C.c_int]
         L.mtref_specimen.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, C.c_int, capi.P_int, capi.P_int,
                                      capi.P_double, C.c_int, capi.P_int, capi.P_double, capi.P_double, capi.P_int,
@@ -68,9 +69,10 @@ def output_dims(params, precision=1):
     return d
 
 
-def run(params, precision=1, nthreads=1):
+def run(params, precision=1, nthreads=1, device=False):
     """Full simulation through the reference; returns a dict shaped like the MATLAB output struct
-    (set_struct_multislice, mex_files_multem/ilc_multem.cu:382-481), arrays as numpy."""
+    (set_struct_multislice, mex_files_multem/ilc_multem.cu:382-481), arrays as numpy. device=True
+    runs the reference's own GPU path (float, cuFFT) instead of its CPU path."""
     d = output_dims(params, precision)
     s, keep = params.to_c()
     nxy = d.nx * d.ny
@@ -92,7 +94,10 @@ def run(params, precision=1, nthreads=1):
     if d.has_psi_coh:
         res["psi_coh_raw"] = np.zeros((d.n_thick, d.nx, d.ny, 2))
         o.psi_coh = _dp(res["psi_coh_raw"])
-    _chk(lib().mtref_run(C.byref(s), precision, nthreads, C.byref(o)))
+    if device:
+        _chk(lib().mtref_run_device(C.byref(s), C.byref(o)))
+    else:
+        _chk(lib().mtref_run(C.byref(s), precision, nthreads, C.byref(o)))
     res["dx"], res["dy"] = o.dx, o.dy
     # arrays are column-major (ix*ny + iy): stored here as [.., ix, iy]; expose MATLAB (iy, ix) order
     if "image_tot" in res:
