@@ -168,15 +168,57 @@ void unique_sorted(std::vector<float>& v) {
     v.erase(std::unique(v.begin(), v.end(), is_equal_f), v.end());
 }
 
-// Slicing::get_z_plane (src/slicing.hpp:130-193) without amorphous layers
+// Atom_Data::validate_amorphous_parameters (src/atomic_data_mt.hpp:539-590) on a copy of the layer
+// list: layers thinner than 1e-4 A are dropped, the rest get the mean region of the atoms strictly
+// inside them (Amorp_Lay_Info::set_region, src/types.cuh:1105-1126), are sorted by z_0, and a zero
+// slice thickness becomes 2 A. (The layer type the reference also sets is not used by slicing.)
+std::vector<AtomsF::Amorp> valid_amorphous_layers(const AtomsF& atoms) {
+    std::vector<AtomsF::Amorp> out;
+    for (const auto& l : atoms.amorp) {
+        if (std::fabs(l.z_e - l.z_0) < 1e-4f) continue;
+        AtomsF::Amorp a = l;
+        int f_region = 0, c_region = 0;
+        for (size_t i = 0; i < atoms.size(); i++) {
+            const float z = atoms.z[i];
+            if ((a.z_0 < z) && (z < a.z_e)) {
+                f_region += atoms.region[i];
+                c_region++;
+            }
+        }
+        c_region = std::max(1, c_region);
+        a.region = (int)std::round((float)f_region / (float)c_region);
+        out.push_back(a);
+    }
+    std::sort(out.begin(), out.end(), [](const AtomsF::Amorp& a, const AtomsF::Amorp& b) { return a.z_0 < b.z_0; });
+    for (auto& a : out)
+        if (is_zero_f(a.dz)) a.dz = 2.0f;
+    return out;
+}
+
+// Slicing::get_z_plane (src/slicing.hpp:130-193): planes of the crystal (region 0) atoms, then, if
+// the specimen extends above / below them, regular planes of the first / last amorphous layer.
 std::vector<float> z_planes(int pot_sli, const AtomsF& atoms) {
     if (atoms.size() == 0) return {0.0f};
+    const auto amorp = valid_amorphous_layers(atoms);
     std::vector<float> z_ct;
     for (size_t i = 0; i < atoms.size(); i++)
         if (atoms.region[i] == 0) z_ct.push_back(atoms.z[i]);
     if (z_ct.empty()) fail(MT_ERR_UNSUPPORTED, "specimen has no atoms in region 0");
     std::sort(z_ct.begin(), z_ct.end());
     std::vector<float> zp = (pot_sli == 1) ? planes_from_values(z_ct) : planes_regular(z_ct.front(), z_ct.back(), atoms.dz);
+    const float z_eps = 1e-3f;
+    if (!amorp.empty() && (std::fabs(atoms.z_min - zp.front()) > z_eps)) {
+        const float dz_b = spacing(1, zp);
+        const auto& a = amorp.front();
+        auto top = planes_regular(a.z_0, a.z_e - dz_b, a.dz);
+        zp.insert(zp.begin(), top.begin(), top.end());
+    }
+    if (!amorp.empty() && (std::fabs(zp.back() - atoms.z_max) > z_eps)) {
+        const float dz_b = spacing(zp.size() - 1, zp);
+        const auto& a = amorp.back();
+        auto bottom = planes_regular(a.z_0 + dz_b, a.z_e, a.dz);
+        zp.insert(zp.end(), bottom.begin(), bottom.end());
+    }
     unique_sorted(zp);
     return zp;
 }
@@ -538,10 +580,11 @@ Model build_model(const mt_input_multislice* in) {
     }
     if (nr == 0) fail(MT_ERR_INVALID_ARG, "specimen has no atoms");
     A.statistic(nullptr);
-    for (int i = 0; i < in->spec_amorp_n; i++) {
-        float z0 = (float)in->spec_amorp_z_0[i], ze = (float)in->spec_amorp_z_e[i];
-        if ((ze - z0) >= 1e-4f) fail(MT_ERR_UNSUPPORTED, "amorphous layer slicing is not implemented");
-    }
+    // Atom_Data::set_amorphous_parameters (src/atomic_data_mt.hpp:313-317)
+    if (in->spec_amorp_n > 0 && (!in->spec_amorp_z_0 || !in->spec_amorp_z_e || !in->spec_amorp_dz))
+        fail(MT_ERR_INVALID_ARG, "spec_amorp_z_0, spec_amorp_z_e and spec_amorp_dz must hold spec_amorp_n values");
+    for (int i = 0; i < in->spec_amorp_n; i++)
+        A.amorp.push_back({(float)in->spec_amorp_z_0[i], (float)in->spec_amorp_z_e[i], (float)in->spec_amorp_dz[i], 0, 0});
     if (!is_zero_f((float)((float)in->spec_rot_theta * kDeg)))
         fail(MT_ERR_UNSUPPORTED, "specimen rotation is not implemented");
     m.thick_type = in->thick_type;
@@ -745,6 +788,7 @@ Specimen::Specimen(const Model& m, const std::vector<float>& R_max_of_Z) : m_(m)
             atoms_u_.charge.push_back(in.charge[i]);
         }
     }
+    atoms_u_.amorp = in.amorp;
     if (atoms_u_.size() == 0) fail(MT_ERR_INVALID_ARG, "no atoms inside the simulation box");
     atoms_u_.statistic(R_max_of_Z_.data());
     atoms_u_.sort_by_z();

@@ -222,3 +222,37 @@ def fcc_batch(n: int = 32, seed: int = 3, grids=(256, 384, 512, 1024), ns: int =
                                              {"inner_ang": 80.0, "outer_ang": 200.0}]}
         out.append(p)
     return out
+
+
+def au110_amorphous_carbon(nx: int = 2048, ny: int = 2048, na: int = 12, nb: int = 17, nc: int = 60,
+                           t_ac: float = 20.0, dz: float = 2.0, nconf: int = 32, seed: int = 1) -> Parameters:
+    """Plane-wave exit wave (EWRS) through Au(110) (a = 4.0782 A; na x nb x nc cells of
+    a/sqrt(2) x a x a/sqrt(2), 34.6 x 69.3 x 173 A at the defaults) under a t_ac-thick amorphous
+    carbon layer (2.0 g/cm^3, minimum spacing 1.4 A, region 1): 200 kV, dz_Proj slices of `dz` in
+    the crystal and in the layer, `nconf` frozen-phonon configurations (sigma 0.085 A)."""
+    a = 4.0782
+    cell = fcc_110(79, a)
+    lx, ly = na * cell[0], nb * cell[1]
+    xtal = crystal(cell, na, nb, nc, sigma=0.085)
+    xtal[:, 3] += t_ac + 0.5 * cell[2]
+    ac = amorphous_layer(6, lx, ly, 0.0, t_ac, 2.0, 12.011, 1.4, 0.085, seed=seed + 1000, region=1)
+    p = Parameters()
+    p.simulation_type = 52
+    p.pn_model = 3
+    p.pn_coh_contrib = 0
+    p.pn_single_conf = 0
+    p.pn_nconf = nconf
+    p.pn_dim = 110
+    p.pn_seed = seed
+    p.spec_atoms = np.vstack([ac, xtal])
+    p.spec_lx, p.spec_ly = lx, ly
+    p.spec_lz = t_ac + nc * cell[2] + cell[2]
+    p.spec_dz = dz
+    p.spec_amorp = [{"z_0": 0.0, "z_e": t_ac, "dz": dz}]
+    p.potential_slicing = 2
+    p.thick_type = 1
+    p.nx, p.ny = nx, ny
+    p.bwl = 0
+    p.E_0 = 200.0
+    p.iw_type = 1
+    return p

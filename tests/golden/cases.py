@@ -56,3 +56,42 @@ def stem_1024():
     """STEM ADF through SrTiO3(001) on a 1024^2 grid, 2 x 2 probes, one phonon configuration."""
     from multem_b200 import specimens
     return specimens.stem_srtio3(nx=1024, ny=1024, na=8, nb=8, nc=3, ns=2, nconf=1, seed=9)
+
+
+def amorph_au110():
+    """Au(110) crystal (6 x 4 x 6 cells, 17.3 x 16.3 x 17.3 A) under a 10 A amorphous carbon layer
+    (2.0 g/cm^3, minimum spacing 1.4 A, region 1, slices of 2 A in the layer), exit wave on a 256^2
+    grid at 200 kV written to a 96 x 96 window, dz_Proj slicing of the crystal with a'/2, two
+    frozen-phonon configurations."""
+    import numpy as np
+    from multem_b200 import Parameters, specimens
+    a = 4.078
+    cell = specimens.fcc_110(79, a)
+    na, nb, nc = 6, 4, 6
+    lx, ly = na * cell[0], nb * cell[1]
+    t_am = 10.0
+    xtal = specimens.crystal(cell, na, nb, nc, sigma=0.085)
+    xtal[:, 3] += t_am + 0.5 * cell[2]
+    am = specimens.amorphous_layer(6, lx, ly, 0.0, t_am, 2.0, 12.011, 1.4, 0.085, seed=5, region=1)
+    p = Parameters()
+    p.simulation_type = 52
+    p.pn_model = 3
+    p.pn_coh_contrib = 0
+    p.pn_single_conf = 0
+    p.pn_nconf = 2
+    p.pn_dim = 110
+    p.pn_seed = 17
+    p.spec_atoms = np.vstack([am, xtal])
+    p.spec_lx, p.spec_ly = lx, ly
+    p.spec_lz = t_am + nc * cell[2] + cell[2]
+    p.spec_dz = cell[2] / 2
+    p.spec_amorp = [{"z_0": 0.0, "z_e": t_am, "dz": 2.0}]
+    p.potential_slicing = 2
+    p.thick_type = 1
+    p.nx = p.ny = 256
+    p.bwl = 0
+    p.E_0 = 200.0
+    p.iw_type = 1
+    p.output_area_ix_0, p.output_area_ix_e = 81, 177
+    p.output_area_iy_0, p.output_area_iy_e = 81, 177
+    return p

@@ -21,7 +21,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from multem_b200 import specimens  # noqa: E402
-from cases import ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384  # noqa: E402
+from cases import amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384  # noqa: E402
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -54,7 +54,7 @@ def main():
     rec = {}
     # specimen host logic: displaced atoms and slicing of two configurations
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
-                     ("ew_config1", ew_config1)):
+                     ("ew_config1", ew_config1), ("amorph_au110", amorph_au110)):
         p = fn()
         for iconf in (1, 2):
             if iconf > p.pn_nconf:
@@ -98,7 +98,8 @@ def main():
                     r = R.propagate(q, z, space, prec)
                     rec[f"{name}_z{int(z)}_s{space}_p{prec}"] = r.astype(np.complex64) if prec == 1 else r
     # full runs on a radix-3 grid and a 1024^2 grid (outputs stored in single precision)
-    for name, fn in (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_1024), ("stem_1024", stem_1024)):
+    for name, fn in (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_1024), ("stem_1024", stem_1024),
+                     ("amorph_au110", amorph_au110)):
         p = fn()
         for prec in (1, 2):
             out = R.run(p, precision=prec, nthreads=8)
