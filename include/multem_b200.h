@@ -193,6 +193,15 @@ const char* mt_last_error(void);
  * (src/input_multislice.cuh:622-796). */
 mt_status mt_output_query(const mt_input_multislice* in, mt_output_dims* dims);
 
+/* The values validate_parameters (src/input_multislice.cuh:622-796) changes without telling the
+ * caller, for `in`: pn_seed below 1, pn_nconf, the z phonon displacement without subslicing,
+ * requested thicknesses matched to slice planes, atoms beyond the last thickness, a caller-given
+ * output area that had to be reordered or clipped. Writes one line per change into buf (NUL
+ * terminated, truncated to n bytes) and their number into *n_changes. Host only. No counterpart in
+ * the reference, which applies them silently; with MTB_STRICT=1 in the environment the run entry
+ * points fail with MT_ERR_INVALID_ARG instead of applying any of them. */
+mt_status mt_input_report(const mt_input_multislice* in, char* buf, size_t n, int* n_changes);
+
 /* One-shot run: create an engine on conf->gpu_device, run, copy results to `out`, destroy.
  * Equivalent of mt_run_multislice (gui_multem/multem.cu:28-50) / run_multislice
  * (mex_files_multem/ilc_multem.cu:484-518). */

@@ -86,6 +86,17 @@ def ilc_multem(system_conf: SystemConf | None, params: Parameters) -> dict:
     return buf.to_dict()
 
 
+def input_report(params: Parameters) -> list:
+    """The changes the reference's validate_parameters would apply silently to `params`
+    (mt_input_report), one string each; host only."""
+    lib = capi.load()
+    s, keep = params.to_c()
+    buf = C.create_string_buffer(1 << 16)
+    n = C.c_int()
+    capi.check(lib.mt_input_report(C.byref(s), buf, len(buf), C.byref(n)))
+    return [line for line in buf.value.decode().split("\n") if line][: n.value]
+
+
 def ilc_multem_batch(system_conf: SystemConf | None, params_list) -> list:
     """Run several simulations in one call (mt_multislice_run_batch): largest first, overlapping
     on the GPU. Returns one output dict per input (as ilc_multem); raises on the first failure."""

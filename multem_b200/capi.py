@@ -99,6 +99,7 @@ SIGNATURES = {
     "mt_output_query": (c_int, [C.POINTER(MtInputMultislice), C.POINTER(MtOutputDims)]),
     "mt_multislice_run": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice),
                                   C.POINTER(MtOutputMultislice)]),
+    "mt_input_report": (c_int, [C.POINTER(MtInputMultislice), C.c_char_p, C.c_size_t, P_int]),
     "mt_multislice_run_batch": (c_int, [C.POINTER(MtSystemConf), c_int, C.POINTER(MtInputMultislice),
                                         C.POINTER(MtOutputMultislice), P_int]),
     "mt_engine_create": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), C.POINTER(_VP)]),

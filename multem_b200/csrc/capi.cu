@@ -162,6 +162,20 @@ mt_status mt_engine_timing(mt_engine* eng, double* total_ms, double* rows_ms, lo
     });
 }
 
+mt_status mt_input_report(const mt_input_multislice* in, char* buf, size_t n, int* n_changes) {
+    return guarded([&] {
+        const mtb::Model m = mtb::build_model(in);
+        std::string r;
+        for (const auto& c : m.clamps) r += c + "\n";
+        if (n_changes) *n_changes = (int)m.clamps.size();
+        if (buf && n > 0) {
+            const size_t k = std::min(n - 1, r.size());
+            std::memcpy(buf, r.data(), k);
+            buf[k] = '\0';
+        }
+    });
+}
+
 mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislice* in, mt_output_multislice* out) {
     return guarded([&] {
         mt_system_conf c = conf ? *conf : default_conf();

@@ -58,13 +58,19 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         if (conf->device != 2) fail(MT_ERR_UNSUPPORTED, "this engine runs on the GPU (system_conf.device must be 2)");
         device_ = conf->gpu_device;
     }
+    // the input is validated on the host first, so its errors do not depend on a GPU
+    m_ = build_model(in);
+    if (!m_.clamps.empty() && env_int("MTB_STRICT", 0) != 0) {
+        std::string r = "MTB_STRICT: the input needs changes the reference would apply silently:";
+        for (const auto& c : m_.clamps) r += " " + c + ";";
+        fail(MT_ERR_INVALID_ARG, r);
+    }
     int ndev = 0;
     MTB_CUDA(cudaGetDeviceCount(&ndev));
     if (device_ < 0 || device_ >= ndev) fail(MT_ERR_INVALID_ARG, "gpu_device out of range");
     MTB_CUDA(cudaSetDevice(device_));
     MTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 
-    m_ = build_model(in);
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     if (!line_size_supported(nx) || !line_size_supported(ny))
         fail(MT_ERR_UNSUPPORTED, "nx and ny must be one of 64, 128, 256, 384, 512, 1024, 2048");

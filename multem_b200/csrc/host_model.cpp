@@ -692,8 +692,11 @@ Model build_model(const mt_input_multislice* in) {
     }
 
     // ---- validate_parameters ----
+    if (m.pn_seed < 1) m.clamps.push_back("pn_seed " + std::to_string(m.pn_seed) + " -> 1");
     m.pn_seed = std::max(1, m.pn_seed);
+    const int nconf_in = m.pn_nconf;
     m.pn_nconf = (!m.is_frozen_phonon()) ? 1 : std::max(1, m.pn_nconf);
+    if (m.pn_nconf != nconf_in) m.clamps.push_back("pn_nconf " + std::to_string(nconf_in) + " -> " + std::to_string(m.pn_nconf));
     m.fp_iconf_0 = (!m.is_frozen_phonon()) ? 1 : (m.pn_single_conf ? m.pn_nconf : 1);
     m.lambda = lambda_f(m.E_0);
     // set_incident_angle (src/input_multislice.cuh:886-890)
@@ -704,6 +707,7 @@ Model build_model(const mt_input_multislice* in) {
     }
     if (m.is_EW()) m.pn_coh_contrib = true;
     if (m.is_STEM() && m.pn_coh_contrib) fail(MT_ERR_UNSUPPORTED, "STEM with pn_coh_contrib = 1 is not implemented");
+    if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 
     // Slicing::match_thickness (src/slicing.hpp:53-71)
@@ -712,8 +716,16 @@ Model build_model(const mt_input_multislice* in) {
     } else {
         auto zp = z_planes(m.potential_slicing, A);
         if (m.thick_type == 3) zp = z_slices(m.potential_slicing, zp, A);
+        const std::vector<float> req = m.thick;
         match_thick(zp, m.thick, (float)(0.25 * A.dz));
         if (m.thick.empty()) fail(MT_ERR_INVALID_ARG, "no requested thickness lies within the specimen");
+        if (m.thick != req) {
+            std::string r = "thick [";
+            for (size_t i = 0; i < req.size(); i++) r += (i ? ", " : "") + std::to_string(req[i]);
+            r += "] -> [";
+            for (size_t i = 0; i < m.thick.size(); i++) r += (i ? ", " : "") + std::to_string(m.thick[i]);
+            m.clamps.push_back(r + "] (matched to slice planes)");
+        }
     }
 
     // remove atoms outside the thickness range (input_multislice.cuh:733-744)
@@ -732,6 +744,7 @@ Model build_model(const mt_input_multislice* in) {
                 }
             }
             B.resize(k);
+            m.clamps.push_back(std::to_string(A.size() - k) + " atoms beyond the last thickness removed");
             A = B;
             A.statistic(nullptr);
         }
@@ -761,6 +774,14 @@ Model build_model(const mt_input_multislice* in) {
     m.out_ix_e = std::max(0, std::min(m.grid.nx, m.out_ix_e));
     m.out_iy_0 = std::max(0, std::min(m.grid.ny, m.out_iy_0));
     m.out_iy_e = std::max(0, std::min(m.grid.ny, m.out_iy_e));
+    // an area given by the caller (not the "whole grid" default ix_0 == ix_e) that had to be
+    // reordered or clipped
+    const bool area_given = in->output_area_ix_0 != in->output_area_ix_e || in->output_area_iy_0 != in->output_area_iy_e;
+    if (m.is_EW() && area_given &&
+        (m.out_ix_0 != in->output_area_ix_0 - 1 || m.out_ix_e != in->output_area_ix_e - 1 ||
+         m.out_iy_0 != in->output_area_iy_0 - 1 || m.out_iy_e != in->output_area_iy_e - 1))
+        m.clamps.push_back("output_area -> ix [" + std::to_string(m.out_ix_0 + 1) + ", " + std::to_string(m.out_ix_e + 1) +
+                           "], iy [" + std::to_string(m.out_iy_0 + 1) + ", " + std::to_string(m.out_iy_e + 1) + "]");
     return m;
 }
 

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <random>
+#include <string>
 #include <vector>
 
 #include "multem_b200.h"
@@ -120,6 +121,7 @@ struct Model {
     // incident wave
     std::vector<float> iw_x, iw_y;
     std::vector<float> iw_psi;  // interleaved complex, user-defined wave
+    std::vector<std::string> clamps;  // values validate_parameters changed silently, as text
 
     // scanning (Scanning<float>::set_grid, src/types.cuh:4294-4390)
     int scan_type = 2;

@@ -74,3 +74,28 @@ def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
     with pytest.raises(capi.MtError) as e:
         api.output_dims(p)
     assert e.value.status == status
+
+
+def test_input_report_lists_silent_changes():
+    """mt_input_report names what validate_parameters would change silently; a plain input has
+    nothing to report."""
+    assert api.input_report(cases()["stem_small"]) == []
+    rep = api.input_report(cases()["stem_thick"])
+    assert any(r.startswith("thick [") for r in rep), rep
+    p = specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    p.pn_seed = 0
+    assert "pn_seed 0 -> 1" in api.input_report(p)
+    p.output_area_ix_0, p.output_area_ix_e = 20, 900
+    p.output_area_iy_0, p.output_area_iy_e = 1, 64
+    assert any(r.startswith("output_area ->") for r in api.input_report(p))
+
+
+def test_strict_mode_rejects_silent_changes(monkeypatch):
+    """With MTB_STRICT=1 a run refuses such an input on the host, before any GPU work."""
+    from multem_b200 import capi
+    p = specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    p.pn_seed = 0
+    monkeypatch.setenv("MTB_STRICT", "1")
+    with pytest.raises(capi.MtError) as e:
+        api.ilc_multem(None, p)
+    assert e.value.status == 1 and "pn_seed" in str(e.value)
