@@ -239,6 +239,7 @@ def run_ours(args):
         eng.run_prepared(c0 + W, c0 + per_rank - 1)  # K timed steps, device-timed inside
         t = eng.timing()
     launches = eng.launch_count()
+    variants = eng.pass_variants()
     ms = t["total_ms"]
     if dist:
         tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
@@ -304,7 +305,9 @@ def run_ours(args):
                "roofline": {"bound": "hbm", "kernel": f"{dom} line pass", "achieved": achieved, "peak": peak,
                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                             "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg,
-                            "rows_avg_ms": rows_avg, "cols_avg_ms": cols_avg},
+                            "rows_avg_ms": rows_avg, "cols_avg_ms": cols_avg,
+                            "pass_variants": {"rows": "bulk-copy fed" if variants & 1 else "per-thread loads",
+                                              "cols": "bulk-copy fed" if variants & 2 else "per-thread loads"}},
                "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "steps": ke, "calls_s": [round(c, 4) for c in calls],

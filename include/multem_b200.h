@@ -245,6 +245,10 @@ mt_status mt_engine_prepare_confs(mt_engine* eng, int iconf_0, int iconf_e);
 mt_status mt_engine_run_prepared(mt_engine* eng, int iconf_0, int iconf_e);
 /* Number of kernel launches the last run issued (own kernels only). */
 mt_status mt_engine_launch_count(mt_engine* eng, long long* n);
+/* Line-pass variants in effect (no counterpart in the reference): bit 0 set = bulk-copy-fed row
+ * pass, bit 1 = bulk-copy-fed column pass; chosen per grid and batch shape by the engine's
+ * autotuner at the first run, or pinned by MTB_PIPE. All variants give bit-identical results. */
+mt_status mt_engine_pass_variants(mt_engine* eng, int* variants);
 /* Device timing (no counterpart in the reference): with timing on, each run records CUDA events on
  * the engine's stream around the whole run and around every line-pass launch. mt_engine_timing
  * returns the last run's device time and the summed durations and counts of the contiguous-line

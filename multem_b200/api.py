@@ -174,6 +174,12 @@ class Engine:
         capi.check(self.lib.mt_engine_launch_count(self.h, C.byref(n)))
         return n.value
 
+    def pass_variants(self) -> int:
+        """Bit 0: bulk-copy-fed row pass, bit 1: column pass (autotuned or MTB_PIPE)."""
+        v = C.c_int()
+        capi.check(self.lib.mt_engine_pass_variants(self.h, C.byref(v)))
+        return v.value
+
     def cancel(self):
         capi.check(self.lib.mt_engine_cancel(self.h))
 

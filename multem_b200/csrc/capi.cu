@@ -147,6 +147,13 @@ mt_status mt_engine_launch_count(mt_engine* eng, long long* n) {
     });
 }
 
+mt_status mt_engine_pass_variants(mt_engine* eng, int* variants) {
+    return guarded([&] {
+        if (!eng || !variants) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        *variants = eng->eng->pass_variants();
+    });
+}
+
 mt_status mt_engine_set_timing(mt_engine* eng, int on) {
     return guarded([&] {
         if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");

@@ -14,6 +14,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.hpp"
 #include "engine.hpp"
@@ -131,7 +134,10 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
     d_err_.alloc(1);
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
-    pipe_ = env_int("MTB_PIPE", 3);  // bit 0: row pass, bit 1: column pass
+    // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns), else tune_passes picks
+    pipe_ = env_int("MTB_PIPE", -1);
+    tune_ = pipe_ < 0;
+    if (tune_) pipe_ = 3;
     reset();
 }
 
@@ -443,6 +449,69 @@ void Engine::run_conf(ConfData& cd) {
     if (m_.is_STEM()) run_stem(cd); else run_ew(cd);
 }
 
+// Autotuner of the line passes: for each (nx, ny, probes per launch) the process times, once, the
+// per-thread-load and the bulk-copy-fed variant of the row pass and of the column pass (one warm-up
+// and three timed launches each, on this engine's probe buffer, transmission function and
+// propagator) and keeps the faster of each. The variants compute bit-identical results (same
+// transforms, same rounding), so the choice affects only the speed.
+int Engine::tune_passes(int nprobe, ConfData& cd) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, int> chosen;
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const auto key = std::make_tuple(nx, ny, nprobe);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = chosen.find(key);
+        if (it != chosen.end()) return it->second;
+    }
+    const size_t nxy = (size_t)nx * ny;
+    MTB_CUDA(cudaMemsetAsync(d_psi_.p, 0, sizeof(float2) * nxy * nprobe, stream_));
+    cudaEvent_t a, b;
+    MTB_CUDA(cudaEventCreate(&a));
+    MTB_CUDA(cudaEventCreate(&b));
+    auto time_of = [&](auto launch) {
+        launch();
+        MTB_CUDA(cudaEventRecord(a, stream_));
+        for (int i = 0; i < 3; i++) launch();
+        MTB_CUDA(cudaEventRecord(b, stream_));
+        MTB_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        MTB_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    };
+    RowArgs ra{};
+    ra.in = d_psi_.p;
+    ra.out = d_psi_.p;
+    ra.trans = d_trans_.p;
+    ra.nx = nx;
+    ra.nprobe = nprobe;
+    ra.scale = 1.0f;
+    ColArgs ca{};
+    ca.in = d_psi_.p;
+    ca.out = d_psi_.p;
+    ca.ny = ny;
+    ca.nprobe = nprobe;
+    ca.g = gdev_;
+    ca.Px = cd.prop.p;
+    ca.Py = cd.prop.p + nx;
+    ca.det_w = col_det_width(nx);
+    const int step = COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE;
+    auto rows_t = [&](bool pipe) {
+        ra.err = pipe ? d_err_.p : nullptr;
+        return time_of([&] { launch_rows(ny, ROW_STEP, ra, 0, stream_); });
+    };
+    auto cols_t = [&](bool pipe) {
+        ca.err = pipe ? d_err_.p : nullptr;
+        return time_of([&] { launch_cols(nx, step, ca, 0, stream_); });
+    };
+    const int bits = (rows_t(true) < rows_t(false) ? 1 : 0) | (cols_t(true) < cols_t(false) ? 2 : 0);
+    MTB_CUDA(cudaEventDestroy(a));
+    MTB_CUDA(cudaEventDestroy(b));
+    synchronize();
+    std::lock_guard<std::mutex> lk(mu);
+    return chosen.emplace(key, bits).first->second;
+}
+
 void Engine::run_stem(ConfData& cd) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const size_t nxy = (size_t)nx * ny;
@@ -470,6 +539,7 @@ void Engine::run_stem(ConfData& cd) {
     ra.nx = nx;
     ra.scale = 1.0f;
 
+    if (tune_) pipe_ = tune_passes(std::min(batch_, n_scan), cd);
     for (int p0 = 0; p0 < n_scan; p0 += batch_) {
         const int nb = std::min(batch_, n_scan - p0);
         ca.nprobe = nb;
@@ -523,6 +593,7 @@ void Engine::run_ew(ConfData& cd) {
     ca.nprobe = 1;
     ca.g = gdev_;
     ca.n_det = 0;
+    if (tune_) pipe_ = tune_passes(1, cd);
     for (int k = 0; k <= cd.last_slice; k++) {
         ra.in = d_psi_.p;
         ra.out = d_psi_.p;

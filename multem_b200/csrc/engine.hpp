@@ -108,6 +108,7 @@ class Engine {
 
     // device timing
     void set_timing(bool on) { timing_ = on; }
+    int pass_variants() const { return pipe_; }
     void timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols);
 
   private:
@@ -144,6 +145,7 @@ class Engine {
     int batch_ = 1;
     DevBuf<int> d_err_;              // set by a line pass whose bounded wait gave up
     int pipe_ = 3;                   // bulk-copy-fed line passes where they fit (bit 0 rows, bit 1 cols)
+    bool tune_ = true;               // choose pipe_ per shape with tune_passes (MTB_PIPE unset)
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;
     DevBuf<float2> d_tmp_;
@@ -161,6 +163,7 @@ class Engine {
     void build_types();
     void prepare_conf(ConfData& cd, int iconf);
     void run_conf(ConfData& cd);
+    int tune_passes(int nprobe, ConfData& cd);
     void run_stem(ConfData& cd);
     void run_ew(ConfData& cd);
     void prop_tables(float dz, float2* px, float2* py, bool output) const;

@@ -85,11 +85,14 @@ constexpr double cx_trig2pi(long long k, long long n, bool c) {
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex products with their rounding fixed (one rounded product, one fused multiply-add per
+// component), so that every kernel variant computes bit-identical results whatever the compiler
+// would otherwise contract.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
-    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+    return make_float2(__fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)), __fmaf_rn(a.y, b.x, -__fmul_rn(a.x, b.y)));
 }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
@@ -109,11 +112,11 @@ __device__ __forceinline__ float2 twiddle_const(float2 v) {
         constexpr float h = 0.70710678118654752440f;
         constexpr float c = (8 * k == R || 8 * k == 7 * R) ? h : -h;
         constexpr float s = (float)(DIR * ((8 * k == R || 8 * k == 3 * R) ? 1 : -1)) * h;
-        return make_float2((v.x * c - v.y * s), (v.x * s + v.y * c));
+        return cmul(v, make_float2(c, s));
     } else {
         constexpr float c = (float)cx_trig2pi(k, R, true);
         constexpr float s = (float)(DIR * cx_trig2pi(k, R, false));
-        return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+        return cmul(v, make_float2(c, s));
     }
 }
 
@@ -122,8 +125,9 @@ template <int DIR>
 __device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
     constexpr float h = 0.86602540378443864676f;  // sqrt(3)/2
     const float2 t1 = cadd(b, c), t2 = csub(b, c);
-    const float2 m = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
-    const float2 s = DIR > 0 ? make_float2(-h * t2.y, h * t2.x) : make_float2(h * t2.y, -h * t2.x);
+    const float2 m = make_float2(__fmaf_rn(-0.5f, t1.x, a.x), __fmaf_rn(-0.5f, t1.y, a.y));
+    const float2 s = DIR > 0 ? make_float2(-__fmul_rn(h, t2.y), __fmul_rn(h, t2.x))
+                             : make_float2(__fmul_rn(h, t2.y), -__fmul_rn(h, t2.x));
     a = cadd(a, t1);
     b = cadd(m, s);
     c = csub(m, s);
