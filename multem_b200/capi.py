@@ -127,6 +127,13 @@ SIGNATURES = {
                                  C.POINTER(C.c_float)]),
     "mt_spline_tables_noalloc": (c_int, [P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
                                          C.c_void_p]),
+    # learned surrogate kernels (include/multem_b200_surrogate.h); tensors are device pointers
+    "mt_sg_conv3x3_forward": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, c_int, _VP]),
+    "mt_sg_conv3x3_backward_data": (c_int, [_VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),
+    "mt_sg_conv3x3_backward_weight": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),
+    "mt_sg_loss": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, C.c_float, _VP]),
+    "mt_sg_adam": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, C.c_float, C.c_float, C.c_float, C.c_float, c_int, _VP]),
+    "mt_sg_to_bf16": (c_int, [_VP, _VP, c_int, _VP]),
     "mt_specimen_info": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_int, P_int]),
     "mt_specimen_atoms": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_double, c_int]),
     "mt_specimen_slices": (c_int, [C.POINTER(MtInputMultislice), c_int, P_double, P_double, P_int, P_int, P_int,

@@ -1,4 +1,4 @@
-"""The C-ABI library loads without a GPU and exports every entry point include/multem_b200.h declares."""
+"""The C-ABI library loads without a GPU and exports every entry point include/*.h declares."""
 import re
 from pathlib import Path
 
@@ -7,11 +7,11 @@ import pytest
 
 from multem_b200 import capi
 
-HDR = Path(__file__).resolve().parents[1] / "include" / "multem_b200.h"
+HDRS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
 
 
 def declared():
-    src = HDR.read_text()
+    src = "\n".join(h.read_text() for h in HDRS)
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(mt_[a-z0-9_]+)\s*\(", src)))
 

@@ -1,0 +1,102 @@
+"""Kernels of the learned surrogate (include/multem_b200_surrogate.h) against a PyTorch FP32
+reference of the same operations on the same BF16-rounded values, and a short training run.
+
+Bounds: forward and data gradient 1e-5 relative (FP32 sums of the same products in a different
+order), weight gradient 1e-4 (long sums over the batch and image)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from multem_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _rel(a, b):
+    return float((a - b).norm() / b.norm())
+
+
+@pytest.mark.parametrize("B,Cin,Cout,H,W", [(2, 3, 5, 20, 37), (3, 8, 16, 32, 32), (1, 16, 2, 16, 16)])
+def test_conv3x3_forward_and_gradients_match_torch(B, Cin, Cout, H, W):
+    torch = pytest.importorskip("torch")
+    F = torch.nn.functional
+    lib = capi.load()
+    g = torch.Generator().manual_seed(B * 100 + Cin)
+    x = torch.randn(B, Cin, H, W, generator=g).to(torch.bfloat16).cuda()
+    w = (torch.randn(Cout, Cin, 3, 3, generator=g) * 0.3).to(torch.bfloat16).cuda()
+    b = torch.randn(Cout, generator=g).cuda()
+    # forward with ReLU, bf16 and fp32 outputs
+    yb = torch.empty(B, Cout, H, W, device="cuda", dtype=torch.bfloat16)
+    yf = torch.empty(B, Cout, H, W, device="cuda")
+    capi.check(lib.mt_sg_conv3x3_forward(_p(x), _p(w), _p(b), _p(yb), _p(yf), B, Cin, Cout, H, W, 1, None))
+    torch.cuda.synchronize()
+    ref = F.relu(F.conv2d(x.float(), w.float(), b, padding=1))
+    assert _rel(yf, ref) < 1e-5
+    assert _rel(yb.float(), ref) < 1e-2  # BF16 storage
+    # gradients through the ReLU: dout masked where the (bf16) output is not positive
+    dout = torch.randn(B, Cout, H, W, generator=g).to(torch.bfloat16).cuda()
+    xr = x.float().clone().requires_grad_(True)
+    wr = w.float().clone().requires_grad_(True)
+    br = b.clone().requires_grad_(True)
+    out = F.conv2d(xr, wr, br, padding=1)
+    mask = (yb.float() > 0).float()
+    out.backward(dout.float() * mask)
+    din = torch.empty_like(x)
+    capi.check(lib.mt_sg_conv3x3_backward_data(_p(dout), _p(yb), _p(w), _p(din), B, Cin, Cout, H, W, None))
+    dw = torch.empty(Cout, Cin, 3, 3, device="cuda")
+    db = torch.empty(Cout, device="cuda")
+    capi.check(lib.mt_sg_conv3x3_backward_weight(_p(x), _p(dout), _p(yb), _p(dw), _p(db), B, Cin, Cout, H, W, None))
+    torch.cuda.synchronize()
+    assert _rel(din.float(), xr.grad) < 1e-2  # din stored in BF16
+    assert _rel(dw, wr.grad) < 1e-4
+    assert _rel(db, br.grad) < 1e-4
+
+
+def test_loss_and_adam_match_their_formulas():
+    torch = pytest.importorskip("torch")
+    lib = capi.load()
+    B, H, W, lam = 2, 16, 16, 0.5
+    g = torch.Generator().manual_seed(3)
+    head = torch.randn(B, 2, H, W, generator=g).cuda()
+    x = torch.rand(B, 1, H, W, generator=g).to(torch.bfloat16).cuda()
+    t = torch.rand(B, 1, H, W, generator=g).cuda()
+    dh = torch.empty(B, 2, H, W, device="cuda", dtype=torch.bfloat16)
+    terms = torch.empty(B, H, W, device="cuda")
+    capi.check(lib.mt_sg_loss(_p(head), _p(x), _p(t), _p(dh), _p(terms), B, H, W, lam, None))
+    d = x.float()[:, 0] + head[:, 0] - t[:, 0]
+    e = head[:, 1]
+    n = B * H * W
+    assert _rel(terms, d * d + lam * (e - d.abs()) ** 2) < 1e-6
+    assert _rel(dh.float()[:, 0], 2 * d / n) < 1e-2 and _rel(dh.float()[:, 1], 2 * lam * (e - d.abs()) / n) < 1e-2
+    w = torch.randn(100, generator=g).cuda()
+    w0 = w.clone()
+    gr = torch.randn(100, generator=g).cuda()
+    m = torch.zeros(100, device="cuda")
+    v = torch.zeros(100, device="cuda")
+    capi.check(lib.mt_sg_adam(_p(w), None, _p(gr), _p(m), _p(v), 100, 1e-2, 0.9, 0.999, 1e-8, 1, None))
+    torch.cuda.synchronize()
+    mh, vh = gr, gr * gr  # first step: bias-corrected moments are the gradient and its square
+    assert _rel(w, w0 - 1e-2 * mh / (vh.sqrt() + 1e-8)) < 1e-5
+
+
+def test_training_reduces_the_loss():
+    """A few hundred steps on synthetic data (noisy copies of smooth images) cut the loss."""
+    torch = pytest.importorskip("torch")
+    from multem_b200.surrogate import Net
+    rng = np.random.default_rng(0)
+    yy, xx = np.mgrid[0:32, 0:32] / 32.0
+    clean = np.stack([1 + 0.5 * np.cos(2 * np.pi * (k % 3 + 1) * xx) * np.cos(2 * np.pi * (k % 2 + 1) * yy)
+                      for k in range(64)])
+    noisy = clean * (1 + 0.05 * rng.standard_normal(clean.shape))
+    X = torch.from_numpy(noisy[:, None].astype(np.float32)).cuda().to(torch.bfloat16)
+    T = torch.from_numpy(clean[:, None].astype(np.float32)).cuda()
+    net = Net(width=16, depth=4)
+    first = np.mean([net.train_step(X, T, lr=2e-3) for _ in range(5)])
+    for _ in range(300):
+        last = net.train_step(X, T, lr=2e-3)
+    assert last < 0.5 * first
