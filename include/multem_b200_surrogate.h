@@ -38,6 +38,14 @@ mt_status mt_sg_loss(const float* head, const void* x, const float* target, void
  * w_bf16 when not NULL. */
 mt_status mt_sg_adam(float* w, void* w_bf16, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
                      float eps, int step, void* stream);
+/* out (bf16 [B,C,H/2,W/2]) = scale * sum of each 2x2 block of in (bf16 [B,C,H,W]); H and W even.
+ * scale 1/4 is average pooling, scale 1 the gradient of mt_sg_upsample2. */
+mt_status mt_sg_pool2(const void* in, void* out, int B, int C, int H, int W, float scale, void* stream);
+/* out (bf16 [B,C,2H,2W]) = scale * in[b,c,y/2,x/2] (in: bf16 [B,C,H,W]). scale 1 is nearest-neighbour
+ * upsampling, scale 1/4 the gradient of average pooling. */
+mt_status mt_sg_upsample2(const void* in, void* out, int B, int C, int H, int W, float scale, void* stream);
+/* out = a + b, n bf16 values (skip connections and the sum of two gradients). */
+mt_status mt_sg_add(const void* a, const void* b, void* out, long long n, void* stream);
 /* b (bf16) = a (float), n values. */
 mt_status mt_sg_to_bf16(const float* a, void* b, int n, void* stream);
 

@@ -134,6 +134,9 @@ SIGNATURES = {
     "mt_sg_loss": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, C.c_float, _VP]),
     "mt_sg_adam": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, C.c_float, C.c_float, C.c_float, C.c_float, c_int, _VP]),
     "mt_sg_to_bf16": (c_int, [_VP, _VP, c_int, _VP]),
+    "mt_sg_pool2": (c_int, [_VP, _VP, c_int, c_int, c_int, c_int, C.c_float, _VP]),
+    "mt_sg_upsample2": (c_int, [_VP, _VP, c_int, c_int, c_int, c_int, C.c_float, _VP]),
+    "mt_sg_add": (c_int, [_VP, _VP, _VP, C.c_longlong, _VP]),
     "mt_specimen_info": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_int, P_int]),
     "mt_specimen_atoms": (c_int, [C.POINTER(MtInputMultislice), c_int, P_int, P_double, c_int]),
     "mt_specimen_slices": (c_int, [C.POINTER(MtInputMultislice), c_int, P_double, P_double, P_int, P_int, P_int,

@@ -108,13 +108,14 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         d_scan_idx_.upload(idx.data(), idx.size(), stream_);
         // probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
         // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
-        // aperture's pixel count (aperture test in the kernel's float arithmetic).
+        // aperture's pixel count (aperture test in the kernel's float arithmetic; no tilt offset
+        // in the simulation's probes).
         const LensF& L = m_.cond_lens;
         double count = 0;
         for (int ix = 0; ix < nx; ix++) {
-            float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx + m_.gx_0();
+            float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx;
             for (int iy = 0; iy < ny; iy++) {
-                float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy + m_.gy_0();
+                float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy;
                 float g2 = gx * gx + gy * gy;
                 if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
             }
@@ -131,6 +132,11 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         niter_ = m_.number_conf();
     }
     d_psi_.alloc((size_t)batch_ * nxy);
+    if (m_.tilted()) {
+        build_tilt_ramp();
+        // STEM outputs at intermediate thicknesses apply the ramp to a copy of the batch
+        if (m_.is_STEM() && n_thk > 1) d_tmp_.alloc((size_t)batch_ * nxy);
+    }
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
     d_err_.alloc(1);
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
@@ -147,7 +153,7 @@ Engine::~Engine() {
         // everything below was used on stream_ only: return it to the pool without a device-wide wait
         for (auto& cd : confs_) cd.release_idle();
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
-        for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_}) b->release_idle();
+        for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
         d_err_.release_idle();
         d_scan_idx_.release_idle();
@@ -206,6 +212,32 @@ void Engine::build_types() {
     synchronize();
 }
 
+// Tilted beam: Wave_Function::get_psi (src/wave_function.cuh:96-105) multiplies the wave by
+// exp(i*(gx*Rx + gy*Ry)), gx = 2*pi*(-gx_0), gy = 2*pi*(-gy_0), before the output propagation
+// (phase_multiplication :77-94, exp_r_factor_2d src/cgpu_fcns.cuh:1869-1878, unscaled), with
+// Rx = Rx_shift(ix) - Rx_c and Rx_c = int(lx/2) (Grid_2d::Rx_c returns an int, src/types.cuh:2284).
+// Applied as a row step whose "transmission" is this table; the table carries the row pass's 1/ny
+// so the result is in the layout the output propagator tables expect. Stored [ix][iy].
+void Engine::build_tilt_ramp() {
+    const GridF& g = m_.grid;
+    const int nx = g.nx, ny = g.ny;
+    const float gx = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gx_0()));
+    const float gy = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gy_0()));
+    const float rxc = (float)(int)(g.Rx_0 + 0.5f * g.lx), ryc = (float)(int)(g.Ry_0 + 0.5f * g.ly);
+    const double s = 1.0 / (double)ny;
+    std::vector<float2> ramp((size_t)nx * ny);
+    for (int ix = 0; ix < nx; ix++) {
+        const float rx = (float)((ix < g.nxh) ? ix + g.nxh : ix - g.nxh) * g.dRx + g.Rx_0 - rxc;
+        for (int iy = 0; iy < ny; iy++) {
+            const float ry = (float)((iy < g.nyh) ? iy + g.nyh : iy - g.nyh) * g.dRy + g.Ry_0 - ryc;
+            volatile float a = gx * rx, b = gy * ry;  // two roundings and a sum, no fused multiply-add
+            const double th = (double)(float)(a + b);
+            ramp[(size_t)ix * ny + iy] = make_float2((float)(std::cos(th) * s), (float)(std::sin(th) * s));
+        }
+    }
+    d_ramp_.upload(ramp.data(), ramp.size(), stream_);
+}
+
 // Fresnel propagator factors for distance dz, separable in x and y:
 // P(ix, iy) = exp(i*w*(gx^2 + gy^2))/N, w = -pi*lambda*dz (propagate, src/cgpu_fcns.cuh:1837-1845;
 // get_propagator_factor, src/input_multislice.cuh:909-912). Phases in double, stored as float.
@@ -232,7 +264,10 @@ void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output)
 
 void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const { mtb::prop_tables(m_, dz, px, py, output); }
 
-ProbeDev Engine::probe_params(float c_c_10, int nz_c10) const {
+// gxu/gyu: the beam-tilt offset of exp_i_chi (src/cgpu_fcns.cuh:1950-1980). The simulations build
+// their probes with gxu = gyu = 0 (Wave_Function::set_incident_wave, src/wave_function.cuh:300-307);
+// only the incident-wave operator passes gx_0/gy_0 (Incident_Wave::operator(), src/incident_wave.cuh:117-121).
+ProbeDev Engine::probe_params(float c_c_10, int nz_c10, bool tilt_offset) const {
     const LensF& L = m_.cond_lens;
     ProbeDev p{};
     p.c_c_10 = c_c_10;
@@ -243,8 +278,8 @@ ProbeDev Engine::probe_params(float c_c_10, int nz_c10) const {
     p.nz_c50 = !is_zero_f(L.c_50);
     p.g2_min = L.g2_min;
     p.g2_max = L.g2_max;
-    p.gxu = m_.gx_0();
-    p.gyu = m_.gy_0();
+    p.gxu = tilt_offset ? m_.gx_0() : 0.0f;
+    p.gyu = tilt_offset ? m_.gy_0() : 0.0f;
     p.norm = probe_norm_;
     p.phi_required = L.is_phi_required();
     p.m = L.m;
@@ -525,7 +560,7 @@ void Engine::run_stem(ConfData& cd) {
     ColArgs ca{};
     ca.ny = ny;
     ca.g = gdev_;
-    ca.probe = probe_params(cd.probe_c_c_10, cd.probe_nz_c10);
+    ca.probe = probe_params(cd.probe_c_c_10, cd.probe_nz_c10, false);
     ca.n_det = n_det;
     for (int d = 0; d < n_det; d++) {
         // sum_square_over_Det bounds: g2 = pow(g, 2) stored as float (src/cpu_fcns.hpp:1168-1169)
@@ -535,6 +570,7 @@ void Engine::run_stem(ConfData& cd) {
     ca.gx_0 = 0;
     ca.gy_0 = 0;
     ca.det_w = col_det_width(nx);
+    const bool tilt = d_ramp_.p != nullptr;
     RowArgs ra{};
     ra.nx = nx;
     ra.scale = 1.0f;
@@ -558,14 +594,28 @@ void Engine::run_stem(ConfData& cd) {
             rows(ROW_STEP, ra);
             const int ithk = cd.slice_ithk[k];
             int flags = COL_LOAD | COL_PROP;
-            if (ithk >= 0) flags |= COL_DETECT;
-            if (k < cd.last_slice) flags |= COL_INVERSE | COL_STORE;
+            if (ithk >= 0 && !tilt) flags |= COL_DETECT;
+            if (k < cd.last_slice || tilt) flags |= COL_INVERSE | COL_STORE;
             ca.in = d_psi_.p;
             ca.out = d_psi_.p;
             ca.Px = cd.prop.p + (size_t)k * pl;
             ca.Py = ca.Px + nx;
             ca.det_partial = d_partial_.p + (size_t)(ithk >= 0 ? ithk : 0) * batch_ * tiles * n_det;
             cols(flags, ca);
+            if (tilt && ithk >= 0) {
+                // get_psi: phase ramp, then the detectors on the transform (the output
+                // propagator's phase does not change |psi_hat|^2)
+                RowArgs rr = ra;
+                rr.out = (k < cd.last_slice) ? d_tmp_.p : d_psi_.p;
+                rr.trans = d_ramp_.p;
+                rows(ROW_STEP, rr);
+                ColArgs cc = ca;
+                cc.in = rr.out;
+                cc.out = rr.out;
+                cc.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
+                cc.Py = cc.Px + nx;
+                cols(COL_LOAD | COL_PROP | COL_DETECT, cc);
+            }
         }
         for (int t = 0; t < n_thk; t++)
             launch_det_reduce(d_partial_.p + (size_t)t * batch_ * tiles * n_det, nb, tiles, n_det, d_scan_idx_.p + p0, w,
@@ -608,8 +658,18 @@ void Engine::run_ew(ConfData& cd) {
         if (ithk < 0) continue;
         // wave at this thickness (Wave_Function::get_psi, src/wave_function.cuh:96-105)
         const float zbp = cd.thick_z_back_prop[ithk];
+        float2* src = d_psi_.p;
+        if (d_ramp_.p) {
+            // tilted beam: phase ramp before the output propagation
+            RowArgs rr = ra;
+            rr.in = d_psi_.p;
+            rr.out = d_tmp_.p;
+            rr.trans = d_ramp_.p;
+            rows(ROW_STEP, rr);
+            src = d_tmp_.p;
+        }
         ColArgs cb = ca;
-        cb.in = d_psi_.p;
+        cb.in = src;
         cb.out = d_tmp_.p;
         cb.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
         cb.Py = cb.Px + nx;
@@ -620,7 +680,7 @@ void Engine::run_ew(ConfData& cd) {
                 rb.in = d_tmp_.p;
                 rb.scale = 1.0f;
             } else {
-                rb.in = d_psi_.p;
+                rb.in = src;
                 rb.scale = 1.0f;
             }
             rb.out = d_tmp_.p;
@@ -746,7 +806,7 @@ void Engine::incident_wave(int space, double* psi) {
     const size_t nxy = (size_t)nx * ny;
     const int nb = (int)m_.iw_x.size();
     if (nb <= 0) fail(MT_ERR_INVALID_ARG, "iw_x/iw_y are empty");
-    // probe normalisation as in the STEM constructor
+    // probe normalisation as in the STEM constructor, with the tilt offset of this operator
     const LensF& L = m_.cond_lens;
     double count = 0;
     for (int ix = 0; ix < nx; ix++) {
@@ -757,7 +817,7 @@ void Engine::incident_wave(int space, double* psi) {
             if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
         }
     }
-    probe_norm_ = (float)std::sqrt(1.0 / (double)(float)count);
+    const float norm = (float)std::sqrt(1.0 / (double)(float)count);
     const float f_s = m_.cond_lens.c_10 - (m_.cond_lens.zero_defocus_plane - 0.0f);
     LensF Lp = m_.cond_lens;
     Lp.set_defocus(f_s);
@@ -771,7 +831,8 @@ void Engine::incident_wave(int space, double* psi) {
     ca.nprobe = nb;
     ca.g = gdev_;
     ca.beam = dbeam.p;
-    ca.probe = probe_params(Lp.c_c_10, !is_zero_f(f_s));
+    ca.probe = probe_params(Lp.c_c_10, !is_zero_f(f_s), true);
+    ca.probe.norm = norm;
     ca.out = dpsi.p;
     if (space == 2) {
         cols(COL_STORE, ca);

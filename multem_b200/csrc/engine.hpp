@@ -156,18 +156,20 @@ class Engine {
     DevBuf<double> d_ew_psi_;        // [n_thk][out_nxy][2]
     DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
+    DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
     std::vector<ConfData> confs_;
     GridDev gdev_{};
     float probe_norm_ = 1.0f;
 
     void build_types();
+    void build_tilt_ramp();
     void prepare_conf(ConfData& cd, int iconf);
     void run_conf(ConfData& cd);
     int tune_passes(int nprobe, ConfData& cd);
     void run_stem(ConfData& cd);
     void run_ew(ConfData& cd);
     void prop_tables(float dz, float2* px, float2* py, bool output) const;
-    ProbeDev probe_params(float c_c_10, int nz_c10) const;
+    ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
     void check_cancel();
     ConfData* find_conf(int iconf);
 };

@@ -471,6 +471,21 @@ void AtomsF::sort_by_z() {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Input_Multislice::set_incident_angle (src/input_multislice.cuh:891-895, applied at :655): the
+// tilt is snapped so that sin(theta)/lambda is a whole number of Fourier pixels dg_min.
+void snap_incident_angle(Model& m) {
+    if (is_zero_f(m.theta)) {
+        m.theta = 0;
+    } else {
+        const float dg = m.grid.dg_min();
+        const float n = std::round(std::sin(m.theta) / (m.lambda * dg));
+        m.theta = std::asin(n * m.lambda * dg);
+    }
+}
+
+// isZero(gx_0, gy_0) of Wave_Function::phase_multiplication (src/wave_function.cuh:79)
+bool Model::tilted() const { return !(is_zero_f(gx_0()) && is_zero_f(gy_0())); }
+
 float Model::gx_0() const { return (float)(std::sin(theta) * std::cos(phi) / lambda); }
 float Model::gy_0() const { return (float)(std::sin(theta) * std::sin(phi) / lambda); }
 // Input_Multislice::Vr_factor (src/input_multislice.cuh:914-917)
@@ -513,15 +528,7 @@ Model build_prop_model(const mt_input_multislice* in) {
     m.phi = (float)((float)in->phi * kDeg);
     m.lambda = lambda_f(m.E_0);
     m.mul_sign = 1;
-    // set_incident_angle (src/input_multislice.cuh:891-895): the tilt is snapped so that
-    // sin(theta)/lambda is a whole number of Fourier pixels
-    if (is_zero_f(m.theta)) {
-        m.theta = 0;
-    } else {
-        const float dg = m.grid.dg_min();
-        const float n = std::round(std::sin(m.theta) / (m.lambda * dg));
-        m.theta = std::asin(n * m.lambda * dg);
-    }
+    snap_incident_angle(m);
     return m;
 }
 
@@ -699,12 +706,7 @@ Model build_model(const mt_input_multislice* in) {
     if (m.pn_nconf != nconf_in) m.clamps.push_back("pn_nconf " + std::to_string(nconf_in) + " -> " + std::to_string(m.pn_nconf));
     m.fp_iconf_0 = (!m.is_frozen_phonon()) ? 1 : (m.pn_single_conf ? m.pn_nconf : 1);
     m.lambda = lambda_f(m.E_0);
-    // set_incident_angle (src/input_multislice.cuh:886-890)
-    if (is_zero_f(m.theta)) {
-        m.theta = 0;
-    } else {
-        fail(MT_ERR_UNSUPPORTED, "tilted illumination (theta != 0) is not implemented");
-    }
+    snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
     if (m.is_STEM() && m.pn_coh_contrib) fail(MT_ERR_UNSUPPORTED, "STEM with pn_coh_contrib = 1 is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");

@@ -152,6 +152,7 @@ struct Model {
     int n_scan() const { return scan_nx * scan_ny; }
     float gx_0() const;
     float gy_0() const;
+    bool tilted() const;
     float Vr_factor() const;
     float propagator_factor(float z) const;
     float phonon_weight() const;
@@ -163,6 +164,7 @@ Model build_model(const mt_input_multislice* in);
 bool line_size_supported(int n);
 // The fields ilc_propagate reads (grid, user wave, E_0, tilt); throws mtb::Error.
 Model build_prop_model(const mt_input_multislice* in);
+void snap_incident_angle(Model& m);
 
 // Per-element spline-table header needed on the host (R_max drives statistics and footprints).
 struct AtomTypeHead {

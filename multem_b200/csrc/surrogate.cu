@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "common.hpp"
@@ -174,6 +175,42 @@ __global__ void adam_kernel(float* __restrict__ wm, __nv_bfloat16* __restrict__ 
     if (wb) wb[i] = __float2bfloat16_rn(w);
 }
 
+// 2 x 2 block sum times `scale` ([B*C, H, W] -> [B*C, H/2, W/2]): average pooling with scale 1/4,
+// the gradient of nearest-neighbour upsampling with scale 1.
+__global__ void pool2_kernel(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ out, int planes, int H,
+                             int W, float scale) {
+    const int Ho = H / 2, Wo = W / 2;
+    const size_t n = (size_t)planes * Ho * Wo;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t pl = k / ((size_t)Ho * Wo);
+        const int r = (int)(k % ((size_t)Ho * Wo)), y = r / Wo, x = r % Wo;
+        const __nv_bfloat16* s = in + (pl * H + 2 * y) * W + 2 * x;
+        const float v = (bf(s[0]) + bf(s[1])) + (bf(s[W]) + bf(s[W + 1]));
+        out[k] = __float2bfloat16_rn(v * scale);
+    }
+}
+
+// Nearest-neighbour 2x upsampling times `scale` ([B*C, H, W] -> [B*C, 2H, 2W]): upsampling with
+// scale 1, the gradient of average pooling with scale 1/4.
+__global__ void upsample2_kernel(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ out, int planes,
+                                 int H, int W, float scale) {
+    const int Ho = 2 * H, Wo = 2 * W;
+    const size_t n = (size_t)planes * Ho * Wo;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t pl = k / ((size_t)Ho * Wo);
+        const int r = (int)(k % ((size_t)Ho * Wo)), y = r / Wo, x = r % Wo;
+        out[k] = __float2bfloat16_rn(bf(in[(pl * H + y / 2) * W + x / 2]) * scale);
+    }
+}
+
+__global__ void add_kernel(const __nv_bfloat16* __restrict__ a, const __nv_bfloat16* __restrict__ b,
+                           __nv_bfloat16* __restrict__ out, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        out[k] = __float2bfloat16_rn(bf(a[k]) + bf(b[k]));
+}
+
+unsigned elem_grid(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
 __global__ void to_bf16_kernel(const float* __restrict__ a, __nv_bfloat16* __restrict__ b, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = __float2bfloat16_rn(a[i]);
@@ -260,6 +297,39 @@ mt_status mt_sg_adam(float* w, void* w_bf16, const float* g, float* m, float* v,
         const float c1 = 1.0f - std::pow(b1, (float)step), c2 = 1.0f - std::pow(b2, (float)step);
         adam_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(w, (__nv_bfloat16*)w_bf16, g, m, v, n, lr, b1, b2,
                                                                         eps, c1, c2);
+        MTB_CUDA(cudaGetLastError());
+    });
+}
+
+mt_status mt_sg_pool2(const void* in, void* out, int B, int C, int H, int W, float scale, void* stream) {
+    return run([&] {
+        check_shape(B, C, 1, H, W);
+        if (H % 2 || W % 2) mtb::fail(MT_ERR_INVALID_ARG, "pooling needs even H and W");
+        if (!in || !out) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
+        const size_t n = (size_t)B * C * (H / 2) * (W / 2);
+        pool2_kernel<<<elem_grid(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, (__nv_bfloat16*)out, B * C,
+                                                                     H, W, scale);
+        MTB_CUDA(cudaGetLastError());
+    });
+}
+
+mt_status mt_sg_upsample2(const void* in, void* out, int B, int C, int H, int W, float scale, void* stream) {
+    return run([&] {
+        check_shape(B, C, 1, 2 * H, 2 * W);
+        if (!in || !out) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
+        const size_t n = (size_t)B * C * (2 * H) * (2 * W);
+        upsample2_kernel<<<elem_grid(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, (__nv_bfloat16*)out,
+                                                                         B * C, H, W, scale);
+        MTB_CUDA(cudaGetLastError());
+    });
+}
+
+mt_status mt_sg_add(const void* a, const void* b, void* out, long long n, void* stream) {
+    return run([&] {
+        if (n < 0 || (n > 0 && (!a || !b || !out))) mtb::fail(MT_ERR_INVALID_ARG, "bad add arguments");
+        if (n == 0) return;
+        add_kernel<<<elem_grid((size_t)n), 256, 0, (cudaStream_t)stream>>>(
+            (const __nv_bfloat16*)a, (const __nv_bfloat16*)b, (__nv_bfloat16*)out, (size_t)n);
         MTB_CUDA(cudaGetLastError());
     });
 }

@@ -38,7 +38,6 @@ namespace {
 #include "atomic_params.inc"
 
 constexpr double kPotf = 47.877645145863056;
-constexpr double kPi = 3.141592653589793238463;
 constexpr double kPi2 = 9.869604401089358618834;
 constexpr double k2Pi = 6.283185307179586476925;
 constexpr double kHalfPi = 1.570796326794896619231;

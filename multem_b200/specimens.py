@@ -30,6 +30,27 @@ def fcc_001(Z: int, a: float):
     return (a, a, a, [(Z, 0.0, 0.0, 0.0), (Z, 0.5, 0.5, 0.0), (Z, 0.0, 0.5, 0.5), (Z, 0.5, 0.0, 0.5)])
 
 
+def haadf_fcc001(Z: int, a: float, nc: int, nx: int = 512, ns: int = 32, scan_cells: int = 2, nconf: int = 64,
+                 seed: int = 1, theta: float = 0.0, phi: float = 0.0, sigma: float = 0.085) -> "Parameters":
+    """HAADF STEM through fcc(001) (6 x 6 x nc cells, lattice constant a, element Z): 300 kV,
+    25 mrad probe, one annular detector 70-200 mrad, ns x ns periodic raster over scan_cells x
+    scan_cells unit cells, `nconf` frozen-phonon configurations (isotropic sigma), dz_Proj slices of
+    a/2, beam tilt theta (deg) at azimuth phi (deg). On 512^2 the sampling is 6a/512 <= 0.048 A, so
+    lambda * g_max reaches the 200 mrad detector edge."""
+    p = stem_srtio3(nx=nx, ny=nx, na=6, nb=6, nc=nc, ns=ns, nconf=nconf, seed=seed)
+    p.spec_atoms = crystal(fcc_001(Z, a), 6, 6, nc, sigma=sigma)
+    p.spec_lx = p.spec_ly = 6 * a
+    p.spec_lz = nc * a
+    p.spec_dz = a / 2
+    p.cond_lens_outer_aper_ang = 25.0
+    x0 = (3 - scan_cells // 2) * a
+    p.scanning_x0, p.scanning_y0 = x0, x0
+    p.scanning_xe, p.scanning_ye = x0 + scan_cells * a, x0 + scan_cells * a
+    p.detector = {"type": 1, "cir": [{"inner_ang": 70.0, "outer_ang": 200.0}]}
+    p.theta, p.phi = theta, phi
+    return p
+
+
 def fcc_110(Z: int, a: float):
     # (110) orientation: a' = a/sqrt(2), b' = a, c' = a/sqrt(2), two layers
     ap = a / np.sqrt(2.0)

@@ -95,3 +95,26 @@ def amorph_au110():
     p.output_area_ix_0, p.output_area_ix_e = 81, 177
     p.output_area_iy_0, p.output_area_iy_e = 81, 177
     return p
+
+
+def stem_tilt_au001():
+    """HAADF (70-200 mrad) STEM through fcc Au(001), 6 x 6 x 5 cells, 512^2 grid, 300 kV, 25 mrad
+    probe, beam tilted 1.5 deg at azimuth 30 deg, 2 x 2 probes, two phonon configurations."""
+    from multem_b200 import specimens
+    return specimens.haadf_fcc001(79, 4.078, 5, nx=512, ns=2, scan_cells=1, nconf=2, seed=7, theta=1.5, phi=30.0)
+
+
+def ew_tilt_si001():
+    """Exit wave (EWRS) of Si(001) on a 256^2 grid with the beam tilted 0.8 deg at azimuth 20 deg
+    (propagator offset g0, transmission strength / cos(theta) and the output phase ramp)."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.theta, p.phi = 0.8, 20.0
+    return p
+
+
+def ewfs_tilt_si001():
+    """ew_tilt_si001 with the exit wave in Fourier space (EWFS)."""
+    p = ew_tilt_si001()
+    p.simulation_type = 51
+    return p

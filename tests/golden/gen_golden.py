@@ -21,7 +21,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from multem_b200 import specimens  # noqa: E402
-from cases import amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384  # noqa: E402
+from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384,  # noqa: E402
+                   stem_tilt_au001, ew_tilt_si001, ewfs_tilt_si001)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -48,9 +49,40 @@ def ew_config1():
     return specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=8)
 
 
+FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_1024), ("stem_1024", stem_1024),
+             ("amorph_au110", amorph_au110), ("stem_tilt_au001", stem_tilt_au001), ("ew_tilt_si001", ew_tilt_si001),
+             ("ewfs_tilt_si001", ewfs_tilt_si001))
+
+
+def full_runs(rec, names=None):
+    """Full reference runs (outputs stored in single precision) of FULL_RUNS, or of `names`."""
+    for name, fn in FULL_RUNS:
+        if names is not None and name not in names:
+            continue
+        p = fn()
+        for prec in (1, 2):
+            out = R.run(p, precision=prec, nthreads=8)
+            for k in ("image_tot", "psi_coh", "m2psi_tot", "thick", "x", "y"):
+                if k in out:
+                    v = out[k]
+                    rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
+
+
+def add_only(names):
+    """Adds the full runs of `names` to the existing fixture file (other arrays kept)."""
+    path = OUT / "reference_fixtures.npz"
+    old = np.load(path)
+    rec = {k: old[k] for k in old.files}
+    full_runs(rec, names)
+    np.savez_compressed(path, **rec)
+    print("wrote", path, len(rec), "arrays")
+
+
 def main():
     if not R.available():
         raise SystemExit("oracle/_ref not built: make -C oracle")
+    if "--only" in sys.argv:
+        return add_only(sys.argv[sys.argv.index("--only") + 1].split(","))
     rec = {}
     # specimen host logic: displaced atoms and slicing of two configurations
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
@@ -97,16 +129,8 @@ def main():
                 for prec in ((1, 2) if z != 0 else (1,)):
                     r = R.propagate(q, z, space, prec)
                     rec[f"{name}_z{int(z)}_s{space}_p{prec}"] = r.astype(np.complex64) if prec == 1 else r
-    # full runs on a radix-3 grid and a 1024^2 grid (outputs stored in single precision)
-    for name, fn in (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_1024), ("stem_1024", stem_1024),
-                     ("amorph_au110", amorph_au110)):
-        p = fn()
-        for prec in (1, 2):
-            out = R.run(p, precision=prec, nthreads=8)
-            for k in ("image_tot", "psi_coh", "m2psi_tot", "thick", "x", "y"):
-                if k in out:
-                    v = out[k]
-                    rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
+    # full runs on a radix-3 grid, a 1024^2 grid, an amorphous layer and a tilted beam
+    full_runs(rec)
     # full runs
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
                      ("ew_config1", ew_config1)):

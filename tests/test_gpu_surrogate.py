@@ -1,5 +1,6 @@
 """Kernels of the learned surrogate (include/multem_b200_surrogate.h) against a PyTorch FP32
-reference of the same operations on the same BF16-rounded values, and a short training run.
+reference of the same operations on the same BF16-rounded values, the whole encoder-decoder's
+gradients against PyTorch CPU autograd, and a short training run.
 
 Bounds: forward and data gradient 1e-5 relative (FP32 sums of the same products in a different
 order), weight gradient 1e-4 (long sums over the batch and image)."""
@@ -84,6 +85,92 @@ def test_loss_and_adam_match_their_formulas():
     assert _rel(w, w0 - 1e-2 * mh / (vh.sqrt() + 1e-8)) < 1e-5
 
 
+class _RoundBF16:
+    """Rounds activations to BF16 in the forward pass (the kernels store them in BF16); gradients
+    pass unchanged."""
+
+    @staticmethod
+    def apply(x):
+        import torch
+        return x + (x.to(torch.bfloat16).float() - x).detach()
+
+
+def _torch_reference(net, x, t, lam):
+    """The network of multem_b200.surrogate.Net in PyTorch FP32 autograd on the CPU, on the same
+    BF16 weights; returns (head, weight gradients, bias gradients)."""
+    import torch
+    F = torch.nn.functional
+    R = _RoundBF16.apply
+    W = [w.float().cpu().requires_grad_(True) for w in net.wb]
+    Bs = [b.cpu().requires_grad_(True) for b in net.b]
+    x, t = x.cpu(), t.cpu()
+
+    def conv(k, h, relu=True):
+        y = F.conv2d(h, W[k], Bs[k], padding=1)
+        return R(F.relu(y)) if relu else y
+
+    L = net.L
+    enc, h = [], x.float()
+    for l in range(L):
+        if l > 0:
+            h = R(F.avg_pool2d(h, 2))
+        h = conv(2 * l + 1, conv(2 * l, h))
+        enc.append(h)
+    k = 2 * L
+    for l in range(L - 2, -1, -1):
+        u = F.interpolate(h, scale_factor=2, mode="nearest")
+        h = conv(k + 1, R(conv(k, u) + enc[l]))
+        k += 2
+    head = conv(k, h, relu=False)
+    d = x.float()[:, 0] + head[:, 0] - t[:, 0]
+    loss = (d * d + lam * (head[:, 1] - d.abs().detach()) ** 2).mean()
+    loss.backward()
+    return head.detach(), [w.grad for w in W], [b.grad for b in Bs]
+
+
+def test_encoder_decoder_gradients_match_torch_autograd():
+    """Forward and every weight/bias gradient of a 3-level encoder-decoder (pooling, upsampling,
+    additive skips, ReLU masks) against PyTorch FP32 autograd. Activations and activation
+    gradients are BF16 in the kernels, so the bound is 3e-2 relative L2 per tensor; a wrong index,
+    mask or missing skip gradient gives errors of order 1."""
+    torch = pytest.importorskip("torch")
+    from multem_b200.surrogate import Net
+    net = Net(widths=(8, 16, 32), seed=4)
+    for b in net.b:  # non-zero biases so that the ReLU masks matter
+        b.copy_(torch.randn(b.shape, generator=torch.Generator().manual_seed(b.numel())).cuda() * 0.1)
+    g = torch.Generator().manual_seed(5)
+    x = (1 + 0.3 * torch.rand(4, 1, 16, 16, generator=g)).to(torch.bfloat16).cuda()
+    t = (1 + 0.3 * torch.rand(4, 1, 16, 16, generator=g)).cuda()
+    saved, head = net.forward(x)
+    dhead, _ = net.loss_grad(head, x, t, 0.5)
+    gw, gb = net.backward(saved, dhead)
+    torch.cuda.synchronize()
+    ref_head, rw, rb = _torch_reference(net, x, t, 0.5)
+    head, gw, gb = head.cpu(), [v.cpu() for v in gw], [v.cpu() for v in gb]
+    assert _rel(head, ref_head) < 1e-2
+    for k in range(len(net.layers)):
+        assert _rel(gw[k], rw[k]) < 3e-2, f"weight gradient of conv {k}: {_rel(gw[k], rw[k]):.3e}"
+        assert _rel(gb[k], rb[k]) < 3e-2, f"bias gradient of conv {k}: {_rel(gb[k], rb[k]):.3e}"
+
+
+def test_pool_upsample_add_kernels():
+    torch = pytest.importorskip("torch")
+    F = torch.nn.functional
+    lib = capi.load()
+    x = torch.randn(2, 3, 8, 12, generator=torch.Generator().manual_seed(1)).to(torch.bfloat16).cuda()
+    y = torch.empty(2, 3, 4, 6, device="cuda", dtype=torch.bfloat16)
+    capi.check(lib.mt_sg_pool2(_p(x), _p(y), 2, 3, 8, 12, 0.25, None))
+    u = torch.empty(2, 3, 16, 24, device="cuda", dtype=torch.bfloat16)
+    capi.check(lib.mt_sg_upsample2(_p(x), _p(u), 2, 3, 8, 12, 1.0, None))
+    z = torch.empty_like(x)
+    capi.check(lib.mt_sg_add(_p(x), _p(x), _p(z), x.numel(), None))
+    torch.cuda.synchronize()
+    assert _rel(y.float(), F.avg_pool2d(x.float(), 2)) < 4e-3
+    assert torch.equal(u.float(), F.interpolate(x.float(), scale_factor=2, mode="nearest"))
+    assert torch.equal(z.float(), 2 * x.float())
+    assert lib.mt_sg_pool2(_p(x), _p(y), 2, 3, 7, 12, 0.25, None) != 0  # odd height refused
+
+
 def test_training_reduces_the_loss():
     """A few hundred steps on synthetic data (noisy copies of smooth images) cut the loss."""
     torch = pytest.importorskip("torch")
@@ -95,7 +182,7 @@ def test_training_reduces_the_loss():
     noisy = clean * (1 + 0.05 * rng.standard_normal(clean.shape))
     X = torch.from_numpy(noisy[:, None].astype(np.float32)).cuda().to(torch.bfloat16)
     T = torch.from_numpy(clean[:, None].astype(np.float32)).cuda()
-    net = Net(width=16, depth=4)
+    net = Net(widths=(16, 32))
     first = np.mean([net.train_step(X, T, lr=2e-3) for _ in range(5)])
     for _ in range(300):
         last = net.train_step(X, T, lr=2e-3)
