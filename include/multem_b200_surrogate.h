@@ -29,11 +29,13 @@ mt_status mt_sg_conv3x3_backward_data(const void* dout, const void* out_mask, co
  * above). */
 mt_status mt_sg_conv3x3_backward_weight(const void* in, const void* dout, const void* out_mask, float* dw, float* db,
                                         int B, int Cin, int Cout, int H, int W, void* stream);
-/* Loss of the two-channel head (float [B,2,H,W]): channel 0 corrects the input image x (bf16
- * [B,1,H,W]) towards target (float [B,1,H,W]), channel 1 estimates |x + head0 - target|. Writes
- * dloss/dhead (bf16 [B,2,H,W]) and the per-pixel loss terms (float [B,H,W]). */
-mt_status mt_sg_loss(const float* head, const void* x, const float* target, void* dhead, float* terms, int B, int H,
-                     int W, float lambda, void* stream);
+/* Loss of the two-channel head (float [B,2,H,W]) in units of a per-item scale s_b (float [B], or
+ * NULL for 1): channel 0 corrects the input image x (bf16 [B,1,H,W]) towards target (float
+ * [B,1,H,W]) as x + s_b * head0, channel 1 estimates |x + s_b * head0 - target| / s_b. Per pixel
+ * dn^2 + lambda * (head1 - |dn|)^2 with dn = (x + s_b * head0 - target) / s_b. Writes dloss/dhead
+ * (bf16 [B,2,H,W], mean over pixels) and the per-pixel loss terms (float [B,H,W]). */
+mt_status mt_sg_loss(const float* head, const void* x, const float* target, const float* scale, void* dhead,
+                     float* terms, int B, int H, int W, float lambda, void* stream);
 /* Adam step (1-based `step`) on float master weights w with moments m, v; also writes the bf16 copy
  * w_bf16 when not NULL. */
 mt_status mt_sg_adam(float* w, void* w_bf16, const float* g, float* m, float* v, int n, float lr, float b1, float b2,

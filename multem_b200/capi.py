@@ -131,7 +131,7 @@ SIGNATURES = {
     "mt_sg_conv3x3_forward": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, c_int, _VP]),
     "mt_sg_conv3x3_backward_data": (c_int, [_VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),
     "mt_sg_conv3x3_backward_weight": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),
-    "mt_sg_loss": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, C.c_float, _VP]),
+    "mt_sg_loss": (c_int, [_VP, _VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, C.c_float, _VP]),
     "mt_sg_adam": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, C.c_float, C.c_float, C.c_float, C.c_float, c_int, _VP]),
     "mt_sg_to_bf16": (c_int, [_VP, _VP, c_int, _VP]),
     "mt_sg_pool2": (c_int, [_VP, _VP, c_int, c_int, c_int, c_int, C.c_float, _VP]),

@@ -142,6 +142,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
     // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns), else tune_passes picks
     pipe_ = env_int("MTB_PIPE", -1);
+    graphs_ = env_int("MTB_GRAPH", 1) != 0;
     tune_ = pipe_ < 0;
     if (tune_) pipe_ = 3;
     reset();
@@ -152,6 +153,9 @@ Engine::~Engine() {
         cudaStreamSynchronize(stream_);
         // everything below was used on stream_ only: return it to the pool without a device-wide wait
         for (auto& cd : confs_) cd.release_idle();
+        for (auto& cd : slot_) cd.release_idle();
+        for (auto& g : graph_)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -358,7 +362,7 @@ void Engine::prepare_confs(int c0, int c1) {
 }
 
 void Engine::check_cancel() {
-    if (cancel_) {
+    if (cancel_ && !capturing_) {
         synchronize();
         fail(MT_ERR_CANCELLED, "run cancelled");
     }
@@ -444,6 +448,21 @@ void Engine::timing(double* total_ms, double* rows_ms, long long* n_rows, double
 void Engine::run_confs(int c0, int c1) {
     if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
     long long l0 = launches_issued();
+    // graphs where launch overhead matters: passes of at most 4 Mi points per launch (above that
+    // one launch runs for tens of microseconds and a recapture would cost more than it saves)
+    const size_t per_launch = (size_t)m_.grid.nx * m_.grid.ny * (m_.is_STEM() ? std::min(batch_, m_.n_scan()) : 1);
+    if (graphs_ && !timing_ && per_launch <= ((size_t)1 << 22)) {
+        // configuration c is prepared in slot c % 2 (prepare_conf waits for the stream, so the
+        // slot's previous user, c - 2, has finished) and runs as that slot's graph
+        for (int c = c0; c <= c1; c++) {
+            ConfData& cd = slot_[c & 1];
+            prepare_conf(cd, c);
+            run_conf_graph(cd, graph_[c & 1]);
+        }
+        launches_ = launches_issued() - l0;
+        synchronize();
+        return;
+    }
     // configuration c is prepared on the host while c-1 runs; c-1's buffers go back to the pool once
     // its last launch has completed
     if (!conf_done_) MTB_CUDA(cudaEventCreateWithFlags(&conf_done_, cudaEventDisableTiming));
@@ -464,6 +483,64 @@ void Engine::run_confs(int c0, int c1) {
     launches_ = launches_issued() - l0;
     synchronize();
     prev.release_idle();
+}
+
+// Everything a captured run_conf bakes into its launches besides the engine's own buffers.
+std::vector<char> Engine::graph_signature(const ConfData& cd) const {
+    std::vector<char> sig;
+    auto put = [&](const void* p, size_t n) { sig.insert(sig.end(), (const char*)p, (const char*)p + n); };
+    const void* ptrs[3] = {cd.atoms.p, cd.ranges.p, cd.prop.p};
+    put(ptrs, sizeof(ptrs));
+    const int ints[4] = {cd.n_slice, cd.last_slice, cd.probe_nz_c10, pipe_};
+    put(ints, sizeof(ints));
+    put(&cd.probe_c_c_10, sizeof(float));
+    put(cd.slice_ithk.data(), cd.slice_ithk.size() * sizeof(int));
+    // the back-propagation distances live in the device tables; only whether each is zero
+    // changes the launches (run_ew)
+    for (float z : cd.thick_z_back_prop) sig.push_back(z != 0.0f);
+    return sig;
+}
+
+// run_conf as a CUDA graph: captured once, then replayed for every configuration with the same
+// launch sequence and arguments (same slot buffers, slice count, thickness map and probe defocus).
+// The line-pass autotuner runs before the capture (it times launches and waits for them).
+void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
+    if (tune_) pipe_ = tune_passes(m_.is_STEM() ? std::min(batch_, m_.n_scan()) : 1, cd);
+    std::vector<char> sig = graph_signature(cd);
+    if (!g.exec || sig != g.sig) {
+        if (g.exec) {
+            MTB_CUDA(cudaGraphExecDestroy(g.exec));
+            g.exec = nullptr;
+        }
+        const int it0 = iter_;
+        const long long l0 = launches_issued();
+        cudaGraph_t graph = nullptr;
+        MTB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        capturing_ = true;
+        try {
+            run_conf(cd);
+        } catch (...) {
+            capturing_ = false;
+            cudaStreamEndCapture(stream_, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            iter_ = it0;
+            throw;
+        }
+        capturing_ = false;
+        MTB_CUDA(cudaStreamEndCapture(stream_, &graph));
+        cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        MTB_CUDA(e);
+        g.sig = std::move(sig);
+        g.iters = iter_ - it0;
+        g.launches = launches_issued() - l0;
+        iter_ = it0;
+        add_launches(-g.launches);
+    }
+    MTB_CUDA(cudaGraphLaunch(g.exec, stream_));
+    iter_ += g.iters;
+    add_launches(g.launches);
+    check_cancel();
 }
 
 void Engine::run_conf(ConfData& cd) {

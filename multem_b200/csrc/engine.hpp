@@ -172,6 +172,21 @@ class Engine {
     ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
     void check_cancel();
     ConfData* find_conf(int iconf);
+
+    // CUDA graphs of run_conf, one per configuration slot (run_confs alternates two slots whose
+    // buffers keep their addresses), replayed while the launch sequence and its arguments match
+    struct ConfGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<char> sig;  // launch-shaping data the graph was captured with
+        int iters = 0;          // progress iterations it advances
+        long long launches = 0;  // kernel launches it holds
+    };
+    bool graphs_ = true;
+    bool capturing_ = false;
+    ConfData slot_[2];
+    ConfGraph graph_[2];
+    std::vector<char> graph_signature(const ConfData& cd) const;
+    void run_conf_graph(ConfData& cd, ConfGraph& g);
 };
 
 }  // namespace mtb

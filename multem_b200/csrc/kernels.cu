@@ -23,9 +23,12 @@
 
 namespace mtb {
 
-static std::atomic<long long> g_launches{0};
-long long launches_issued() { return g_launches.load(); }
+// Kernel launches issued by the calling thread (an engine runs on one host thread). A CUDA graph
+// replay adds the launches it holds through add_launches.
+static thread_local long long g_launches = 0;
+long long launches_issued() { return g_launches; }
 void note_launch() { g_launches++; }
+void add_launches(long long n) { g_launches += n; }
 
 void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr) {
     static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {

@@ -105,5 +105,6 @@ void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, i
 
 // Device-side counters of this library's launches (for reporting).
 long long launches_issued();
+void add_launches(long long n);
 
 }  // namespace mtb

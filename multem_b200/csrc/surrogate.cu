@@ -139,24 +139,28 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_kernel(const __nv_bfloat16*
     }
 }
 
-// Loss of the two-channel head. Channel 0 is a correction r added to the input image x
-// (prediction yh = x + r), channel 1 an estimate e of |yh - t| per pixel. Per pixel:
-//   loss = (yh - t)^2 + lambda * (e - |yh - t|)^2   (the error target is not differentiated)
+// Loss of the two-channel head in units of a per-item scale s_b (the item's noise level; 1 when
+// no scales are given). Channel 0 is a correction r to the input image x (prediction
+// yh = x + s_b * r), channel 1 an estimate e of |yh - t| / s_b per pixel. Per pixel, with
+// dn = (yh - t) / s_b:
+//   loss = dn^2 + lambda * (e - |dn|)^2   (the error target is not differentiated)
 // gradients (scaled by 1/n) go to dhead as BF16; per-pixel losses to `terms` for a fixed-order sum.
 __global__ void surrogate_loss_kernel(const float* __restrict__ head, const __nv_bfloat16* __restrict__ x,
-                                      const float* __restrict__ t, __nv_bfloat16* __restrict__ dhead, float* __restrict__ terms,
-                                      int B, int HW, float lambda) {
+                                      const float* __restrict__ t, const float* __restrict__ scale,
+                                      __nv_bfloat16* __restrict__ dhead, float* __restrict__ terms, int B, int HW,
+                                      float lambda) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= B * HW) return;
     const int b = p / HW, q = p % HW;
+    const float sc = scale ? scale[b] : 1.0f;
     const float r = head[(size_t)b * 2 * HW + q], e = head[(size_t)b * 2 * HW + HW + q];
-    const float yh = bf(x[p]) + r;
-    const float d = yh - t[p];
-    const float ad = fabsf(d);
+    const float yh = __fmaf_rn(sc, r, bf(x[p]));
+    const float dn = __fdiv_rn(yh - t[p], sc);
+    const float ad = fabsf(dn);
     const float n = (float)(B * HW);
-    dhead[(size_t)b * 2 * HW + q] = __float2bfloat16_rn(2.0f * d / n);
+    dhead[(size_t)b * 2 * HW + q] = __float2bfloat16_rn(2.0f * dn / n);
     dhead[(size_t)b * 2 * HW + HW + q] = __float2bfloat16_rn(2.0f * lambda * (e - ad) / n);
-    terms[p] = d * d + lambda * (e - ad) * (e - ad);
+    terms[p] = dn * dn + lambda * (e - ad) * (e - ad);
 }
 
 // Adam step on FP32 master weights; writes the BF16 copy the kernels read.
@@ -279,13 +283,14 @@ mt_status mt_sg_conv3x3_backward_weight(const void* in, const void* dout, const 
     });
 }
 
-mt_status mt_sg_loss(const float* head, const void* x, const float* target, void* dhead, float* terms, int B, int H,
-                     int W, float lambda, void* stream) {
+mt_status mt_sg_loss(const float* head, const void* x, const float* target, const float* scale, void* dhead,
+                     float* terms, int B, int H, int W, float lambda, void* stream) {
     return run([&] {
         check_shape(B, 1, 2, H, W);
+        if (!head || !x || !target || !dhead || !terms) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
         const int n = B * H * W;
         surrogate_loss_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-            head, (const __nv_bfloat16*)x, target, (__nv_bfloat16*)dhead, terms, B, H * W, lambda);
+            head, (const __nv_bfloat16*)x, target, scale, (__nv_bfloat16*)dhead, terms, B, H * W, lambda);
         MTB_CUDA(cudaGetLastError());
     });
 }

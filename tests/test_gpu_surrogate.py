@@ -68,8 +68,10 @@ def test_loss_and_adam_match_their_formulas():
     t = torch.rand(B, 1, H, W, generator=g).cuda()
     dh = torch.empty(B, 2, H, W, device="cuda", dtype=torch.bfloat16)
     terms = torch.empty(B, H, W, device="cuda")
-    capi.check(lib.mt_sg_loss(_p(head), _p(x), _p(t), _p(dh), _p(terms), B, H, W, lam, None))
-    d = x.float()[:, 0] + head[:, 0] - t[:, 0]
+    sc = torch.tensor([1.0, 0.5], device="cuda")
+    capi.check(lib.mt_sg_loss(_p(head), _p(x), _p(t), _p(sc), _p(dh), _p(terms), B, H, W, lam, None))
+    s = sc[:, None, None]
+    d = (x.float()[:, 0] + s * head[:, 0] - t[:, 0]) / s
     e = head[:, 1]
     n = B * H * W
     assert _rel(terms, d * d + lam * (e - d.abs()) ** 2) < 1e-6
@@ -135,14 +137,14 @@ def test_encoder_decoder_gradients_match_torch_autograd():
     mask or missing skip gradient gives errors of order 1."""
     torch = pytest.importorskip("torch")
     from multem_b200.surrogate import Net
-    net = Net(widths=(8, 16, 32), seed=4)
+    net = Net(widths=(8, 16, 32), in_ch=2, seed=4)
     for b in net.b:  # non-zero biases so that the ReLU masks matter
         b.copy_(torch.randn(b.shape, generator=torch.Generator().manual_seed(b.numel())).cuda() * 0.1)
     g = torch.Generator().manual_seed(5)
-    x = (1 + 0.3 * torch.rand(4, 1, 16, 16, generator=g)).to(torch.bfloat16).cuda()
+    x = (1 + 0.3 * torch.rand(4, 2, 16, 16, generator=g)).to(torch.bfloat16).cuda()
     t = (1 + 0.3 * torch.rand(4, 1, 16, 16, generator=g)).cuda()
     saved, head = net.forward(x)
-    dhead, _ = net.loss_grad(head, x, t, 0.5)
+    dhead, _ = net.loss_grad(head, x, t, lam=0.5)
     gw, gb = net.backward(saved, dhead)
     torch.cuda.synchronize()
     ref_head, rw, rb = _torch_reference(net, x, t, 0.5)
@@ -182,7 +184,7 @@ def test_training_reduces_the_loss():
     noisy = clean * (1 + 0.05 * rng.standard_normal(clean.shape))
     X = torch.from_numpy(noisy[:, None].astype(np.float32)).cuda().to(torch.bfloat16)
     T = torch.from_numpy(clean[:, None].astype(np.float32)).cuda()
-    net = Net(widths=(16, 32))
+    net = Net(widths=(16, 32), in_ch=1)
     first = np.mean([net.train_step(X, T, lr=2e-3) for _ in range(5)])
     for _ in range(300):
         last = net.train_step(X, T, lr=2e-3)
