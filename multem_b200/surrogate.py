@@ -62,10 +62,11 @@ class Net:
         self.L = L
         g = torch.Generator().manual_seed(seed)
         self.w, self.b = [], []
-        for i, (ci, co) in enumerate(convs):
-            std = (2.0 / (ci * 9)) ** 0.5 * (0.1 if i == len(convs) - 1 else 1.0)
-            self.w.append((torch.randn(co, ci, 3, 3, generator=g) * std).to(device))
-            self.b.append(torch.zeros(co, device=device))
+        for ci, co in convs:
+            # uniform in +-1/sqrt(fan_in) for weights and biases (PyTorch's default for Conv2d)
+            bound = 1.0 / (ci * 9) ** 0.5
+            self.w.append(((torch.rand(co, ci, 3, 3, generator=g) * 2 - 1) * bound).to(device))
+            self.b.append(((torch.rand(co, generator=g) * 2 - 1) * bound).to(device))
         self.wb = [w.to(torch.bfloat16) for w in self.w]
         self.m = [torch.zeros_like(t) for t in self.w + self.b]
         self.v = [torch.zeros_like(t) for t in self.w + self.b]
@@ -200,7 +201,10 @@ class Net:
         return xn + sc[:, None, None] * h[:, 0], np.abs(h[:, 1]) * sc[:, None, None]
 
     def save(self, path=WEIGHTS, **meta):
-        d = {f"w{i}": w.cpu().numpy() for i, w in enumerate(self.w)}
+        """Weights as their BF16 bit patterns (what inference uses; half the size of FP32), biases
+        in FP32, the layer widths and a JSON record of how the network was trained and measured."""
+        torch = self.torch
+        d = {f"w{i}": w.to(torch.bfloat16).view(torch.int16).cpu().numpy() for i, w in enumerate(self.w)}
         d.update({f"b{i}": b.cpu().numpy() for i, b in enumerate(self.b)})
         d["widths"] = np.array(self.widths)
         d["in_ch"] = np.array(self.in_ch)
@@ -213,7 +217,8 @@ class Net:
         z = np.load(path)
         net = cls(widths=tuple(int(v) for v in z["widths"]), in_ch=int(z["in_ch"]), device=device)
         for i in range(len(net.layers)):
-            net.w[i] = torch.from_numpy(z[f"w{i}"]).to(device)
+            w = torch.from_numpy(z[f"w{i}"])
+            net.w[i] = (w.view(torch.bfloat16) if w.dtype == torch.int16 else w).float().to(device)
             net.b[i] = torch.from_numpy(z[f"b{i}"]).to(device)
         net.wb = [w.to(torch.bfloat16) for w in net.w]
         net.meta = json.loads(str(z["meta"]))
@@ -345,8 +350,10 @@ def _torch_fold(x, period):
 
 def _batches(P, F, rng, bs, tiers, period):
     """Random training batch: per item a specimen, a tier n and n distinct configurations of the
-    specimen, the lattice fold on every other item; one of the 8 symmetries of the square applied
-    to the whole batch (the fold commutes with them). Returns (input, target, per-item scale)."""
+    specimen, the lattice fold on every other item; one of the 8 symmetries of the square and one
+    lattice translation (whole or half cells) applied to the whole batch (the fold commutes with
+    both; with zero padding at the image edge the translations are new inputs). Returns (input,
+    target, per-item scale)."""
     import torch
     S, nconf, H, W = P.shape
     idx = torch.from_numpy(rng.integers(0, S, bs)).cuda()
@@ -367,6 +374,10 @@ def _batches(P, F, rng, bs, tiers, period):
     x, t = torch.rot90(x, k, (2, 3)), torch.rot90(t, k, (2, 3))
     if rng.integers(0, 2):
         x, t = x.flip(3), t.flip(3)
+    h = period // 2
+    sy = int(rng.integers(0, H // h))
+    sx = int(rng.integers(0, W // h // 2)) * 2 + sy % 2  # whole cells, or the (h, h) half-cell shift
+    x, t = torch.roll(x, (sy * h, sx * h), (2, 3)), torch.roll(t, (sy * h, sx * h), (2, 3))
     return x.contiguous().to(torch.bfloat16), t.contiguous(), torch.from_numpy(lv).cuda()
 
 
@@ -422,11 +433,12 @@ def main():
     ap.add_argument("--test-ns", type=int, default=64, help="evaluation raster (over test-ns/16 unit cells)")
     ap.add_argument("--data", default=None, help="per-configuration images: read if present, else generated here")
     ap.add_argument("--generate-only", action="store_true")
-    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--gate", type=float, default=0.02)
     ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--weights", default=None, help="evaluate these trained weights instead of training")
     args = ap.parse_args()
     import torch
 
@@ -444,16 +456,21 @@ def main():
     P = torch.from_numpy(np.ascontiguousarray(imgs[:imgs.shape[0] - n_val])).cuda()
     F = P.mean(dim=1)
 
-    net = Net()
-    rng = np.random.default_rng(0)
-    losses = []
-    t1 = time.perf_counter()
-    for s in range(args.steps):
-        x, t, sc = _batches(P, F, rng, args.batch, TIERS[:-1], PERIOD)
-        lr = args.lr * 0.5 * (1 + np.cos(np.pi * s / args.steps))
-        losses.append(net.train_step(x, t, lr=lr, scale=sc))
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t1
+    losses = [float("nan")]
+    t_train = 0.0
+    if args.weights:
+        net = Net.load(args.weights)
+        args.steps = net.meta.get("train_steps", None)
+    else:
+        net = Net()
+        rng = np.random.default_rng(0)
+        t1 = time.perf_counter()
+        for s in range(args.steps):
+            x, t, sc = _batches(P, F, rng, args.batch, TIERS[:-1], PERIOD)
+            lr = args.lr * 0.5 * (1 + np.cos(np.pi * s / args.steps))
+            losses.append(net.train_step(x, t, lr=lr, scale=sc))
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t1
 
     # gate calibration on held-out specimens: disjoint n-configuration inputs per tier and mode;
     # the factor makes the estimate cover the true error on 95 % of them
@@ -485,7 +502,7 @@ def main():
         "final_loss": float(np.mean(losses[-200:])), "training_s": round(t_train, 1),
         "data_generation_s": None if t_gen is None else round(t_gen, 1),
     }
-    net.save(args.out, calib=calib, gate=args.gate, workload=summary["workload"],
+    net.save(args.out, calib=calib, gate=args.gate, workload=summary["workload"], train_steps=args.steps,
              **{f"{m}_{k}": v for m in modes for k, v in modes[m].items() if k != "per_specimen"})
     for m in modes:
         summary[m] = {k: v for k, v in modes[m].items() if k != "per_specimen"}
@@ -508,7 +525,9 @@ def evaluate(sg, tests, test_times, test_meta, period):
             torch.cuda.synchronize()
             ti = time.perf_counter()
             pred, est, ok = sg.predict(small, n, period)
-            t_inf += time.perf_counter() - ti
+            dt = time.perf_counter() - ti
+            t_inf += dt
+            row[f"t_inference{n}_s"] = dt
             row[f"err_plain{n}"] = rel_rms(small, full)
             row[f"err_learned{n}"] = rel_rms(pred, full)
             row[f"est{n}"] = est
@@ -522,6 +541,7 @@ def evaluate(sg, tests, test_times, test_meta, period):
                 row[f"err_plain{n}"], row[f"err_learned{n}"], row[f"est{n}"] = rel_rms(small, full), rel_rms(pred, full), est
         row["configurations_run"] = used
         row["err_final"] = rel_rms(final, full)
+        row["t_plain4_s"] = float(tc[:4].sum())
         row["t_plain64_s"] = float(tc.sum())
         row["t_learned_s"] = float(tc[:used].sum()) + t_inf
         row["t_inference_s"] = t_inf
@@ -540,6 +560,8 @@ def summarize(res):
         "rel_rms_error_floor4": float(np.mean([r["err_floor_4"] for r in res])),
         "accepted_at": {str(n): float(np.mean([r["configurations_run"] == n for r in res])) for n in TIERS},
         "fallback_rate": float(np.mean([r["configurations_run"] == TIERS[-1] for r in res])),
+        # ungated: every image from 4 configurations + one inference, at rel_rms_error_learned4
+        "learned4_updates_per_s": upd / sum(r["t_plain4_s"] + r["t_inference4_s"] for r in res),
     }
     for n in TIERS[:-1]:
         out[f"rel_rms_error_plain{n}"] = float(np.mean([r[f"err_plain{n}"] for r in res]))
