@@ -314,13 +314,33 @@ def run_ours(args):
                        "api": "mt_multislice_run (C ABI), host in/out, includes engine set-up; median of 3 calls "
                               "after one warm-up call"},
                "gpu_launches": launches,
-               "clocks": clk.summary()}
+               "clocks": clk.summary(),
+               "learned": learned_record()}
         print(json.dumps(out), flush=True)
     eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def learned_record():
+    """The learned path's figures as measured when the committed surrogate was evaluated (HAADF,
+    fcc(001) Au/Pt, 512^2 grid, 10 unseen specimens, 64 configurations as the reference result);
+    they are not re-timed in this run."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "multem_b200", "surrogate_weights.npz")
+    if not os.path.exists(path):
+        return None
+    import numpy as np
+    meta = json.loads(str(np.load(path)["meta"]))
+    keys = ("plain_updates_per_s", "learned_updates_per_s", "learned4_updates_per_s", "rel_rms_error_learned4",
+            "rel_rms_error_learned16", "rel_rms_error_plain4", "max_rel_rms_error_after_gate", "fallback_rate",
+            "rel_rms_error_floor4")
+    return {"source": "recorded by python -m multem_b200.surrogate (profiles/surrogate_haadf_fcc001_512.md); "
+                      "not timed in this run",
+            "workload": meta.get("workload"), "gate": meta.get("gate"),
+            "crystal_mode": {k: meta.get(f"crystal_{k}") for k in keys},
+            "generic_mode": {k: meta.get(f"generic_{k}") for k in keys}}
 
 
 def main():
