@@ -122,7 +122,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         }
         if (count <= 0) fail(MT_ERR_INVALID_ARG, "condenser aperture contains no Fourier pixel");
         probe_norm_ = (float)std::sqrt(1.0 / (double)(float)count);
-        niter_ = m_.n_scan() * m_.number_conf();
+        niter_ = m_.n_scan() * m_.number_conf() * (int)m_.ti_x.size();
     } else {
         batch_ = 1;
         const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
@@ -334,13 +334,19 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     for (size_t t = 0; t < TH.size(); t++)
         prop_tables(TH[t].z_back_prop, &prop[(S.size() + t) * pl], &prop[(S.size() + t) * pl + nx], true);
     // incident-wave defocus relative to the first slice (Incident_Wave::operator(),
-    // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0))
+    // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0)), with c_10 moved
+    // by each defocus-spread point (cond_lens.set_defocus(c_10_0 + qt.x), src/tem_simulation.cuh:155-157)
     const float z_init = (float)(0.5 * (S[0].z_0 + S[0].z_e));
-    const float f_s = m_.cond_lens.c_10 - (m_.cond_lens.zero_defocus_plane - z_init);
-    LensF L = m_.cond_lens;
-    L.set_defocus(f_s);
-    cd.probe_c_c_10 = L.c_c_10;
-    cd.probe_nz_c10 = !is_zero_f(f_s);
+    cd.probe_c_c_10.clear();
+    cd.probe_nz_c10.clear();
+    for (double dx : m_.ti_x) {
+        const float c_10 = (float)((double)m_.cond_lens.c_10 + dx);
+        const float f_s = c_10 - (m_.cond_lens.zero_defocus_plane - z_init);
+        LensF L = m_.cond_lens;
+        L.set_defocus(f_s);
+        cd.probe_c_c_10.push_back(L.c_c_10);
+        cd.probe_nz_c10.push_back(!is_zero_f(f_s));
+    }
     cd.atoms.upload(at.data(), at.size(), stream_);
     cd.ranges.upload(rg.data(), rg.size(), stream_);
     cd.prop.upload(prop.data(), prop.size(), stream_);
@@ -491,9 +497,10 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
     auto put = [&](const void* p, size_t n) { sig.insert(sig.end(), (const char*)p, (const char*)p + n); };
     const void* ptrs[3] = {cd.atoms.p, cd.ranges.p, cd.prop.p};
     put(ptrs, sizeof(ptrs));
-    const int ints[4] = {cd.n_slice, cd.last_slice, cd.probe_nz_c10, pipe_};
+    const int ints[3] = {cd.n_slice, cd.last_slice, pipe_};
     put(ints, sizeof(ints));
-    put(&cd.probe_c_c_10, sizeof(float));
+    put(cd.probe_nz_c10.data(), cd.probe_nz_c10.size() * sizeof(int));
+    put(cd.probe_c_c_10.data(), cd.probe_c_c_10.size() * sizeof(float));
     put(cd.slice_ithk.data(), cd.slice_ithk.size() * sizeof(int));
     // the back-propagation distances live in the device tables; only whether each is zero
     // changes the launches (run_ew)
@@ -632,12 +639,9 @@ void Engine::run_stem(ConfData& cd) {
     const int n_thk = (int)m_.thick.size();
     const int tiles = col_tiles(nx, ny);
     const size_t pl = (size_t)nx + ny;
-    const double w = (double)m_.phonon_weight();
-
     ColArgs ca{};
     ca.ny = ny;
     ca.g = gdev_;
-    ca.probe = probe_params(cd.probe_c_c_10, cd.probe_nz_c10, false);
     ca.n_det = n_det;
     for (int d = 0; d < n_det; d++) {
         // sum_square_over_Det bounds: g2 = pow(g, 2) stored as float (src/cpu_fcns.hpp:1168-1169)
@@ -653,6 +657,11 @@ void Engine::run_stem(ConfData& cd) {
     ra.scale = 1.0f;
 
     if (tune_) pipe_ = tune_passes(std::min(batch_, n_scan), cd);
+    // defocus-spread points (one without full integration), each over every probe, weighted
+    // w_pr_0 * qt.w as a float (Multislice::STEM_ISTEM, src/tem_simulation.cuh:146-176)
+    for (size_t it = 0; it < m_.ti_x.size(); it++) {
+    ca.probe = probe_params(cd.probe_c_c_10[it], cd.probe_nz_c10[it], false);
+    const double w = (double)(float)((double)m_.phonon_weight() * m_.ti_w[it]);
     for (int p0 = 0; p0 < n_scan; p0 += batch_) {
         const int nb = std::min(batch_, n_scan - p0);
         ca.nprobe = nb;
@@ -699,6 +708,7 @@ void Engine::run_stem(ConfData& cd) {
                               d_image_.p + (size_t)t * n_det * n_scan, n_scan, stream_);
         iter_ += nb;
         check_cancel();
+    }
     }
 }
 

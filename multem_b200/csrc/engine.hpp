@@ -65,8 +65,8 @@ struct ConfData {
     int last_slice = 0;             // last slice that carries a thickness
     std::vector<int> slice_ithk;    // per slice
     std::vector<float> thick_z_back_prop;
-    float probe_c_c_10 = 0;
-    int probe_nz_c10 = 0;
+    std::vector<float> probe_c_c_10;  // per point of the defocus-spread quadrature
+    std::vector<int> probe_nz_c10;
     DevBuf<float4> atoms;
     DevBuf<int2> ranges;
     DevBuf<float2> prop;            // per slice: Px[nx] then Py[ny]

@@ -352,12 +352,21 @@ void LensF::from_input(const mt_lens& l) {
     inner_aper_ang = (float)((float)l.inner_aper_ang * kMrad);
     outer_aper_ang = (float)((float)l.outer_aper_ang * kMrad);
     si_sigma = (float)l.si_sigma;
+    ti_a = (float)l.ti_a;
+    ti_sigma = (float)l.ti_sigma;
+    ti_beta = (float)l.ti_beta;
+    ti_npts = l.ti_npts;
     zero_defocus_type = l.zero_defocus_type;
     zero_defocus_plane = (float)l.zero_defocus_plane;
 }
 
 // Lens<float>::set_input_data (src/types.cuh:2936-2985)
 void LensF::set_input_data(float E_0, const GridF& grid) {
+    // Lens::set_input_data (src/types.cuh:2953-2956)
+    ti_a = std::max(0.0f, std::min(1.0f, ti_a));
+    ti_sigma = std::max(0.0f, ti_sigma);
+    ti_beta = std::max(0.0f, ti_beta);
+    ti_npts = std::max(1, ti_npts);
     lambda = lambda_f(E_0);
     const double L = (double)lambda;
     auto cc = [&](float c, double f) -> float { return is_zero_f(c) ? 0.0f : (float)(f * (double)c); };
@@ -480,6 +489,73 @@ void snap_incident_angle(Model& m) {
         const float dg = m.grid.dg_min();
         const float n = std::round(std::sin(m.theta) / (m.lambda * dg));
         m.theta = std::asin(n * m.lambda * dg);
+    }
+}
+
+// Gauss-Hermite rule for the weight exp(-t^2) on the real line (n points). The nodes are the
+// eigenvalues of the Jacobi matrix of the orthonormal Hermite polynomials (zero diagonal,
+// off-diagonal sqrt(k/2)), found by bisection on Sturm counts; the weights are the Christoffel
+// numbers 1 / sum_{k<n} p_k(x)^2. The weights sum to sqrt(pi).
+void gauss_hermite(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    auto below = [&](double s) {  // eigenvalues below s: negative pivots of (J - s I) = L D L^T
+        int c = 0;
+        double d = 1.0;
+        for (int k = 0; k < n; k++) {
+            d = -s - (k > 0 ? 0.5 * k / d : 0.0);
+            if (d == 0.0) d = -1e-300;
+            if (d < 0.0) c++;
+        }
+        return c;
+    };
+    const double R = std::sqrt(2.0 * n) + 2.0;  // every eigenvalue lies in (-R, R) (Gershgorin)
+    for (int i = 0; i < n; i++) {
+        double lo = -R, hi = R;
+        for (int it = 0; it < 200 && hi - lo > 1e-15 * std::max(1.0, std::fabs(lo)); it++) {
+            const double mid = 0.5 * (lo + hi);
+            if (below(mid) > i) hi = mid; else lo = mid;
+        }
+        const double t = 0.5 * (lo + hi);
+        double p0 = std::pow(3.141592653589793238463, -0.25), p1 = std::sqrt(2.0) * t * p0;
+        double sum = p0 * p0 + (n > 1 ? p1 * p1 : 0.0);
+        for (int k = 1; k + 1 < n; k++) {
+            const double p2 = std::sqrt(2.0 / (k + 1)) * t * p1 - std::sqrt((double)k / (k + 1)) * p0;
+            sum += p2 * p2;
+            p0 = p1;
+            p1 = p2;
+        }
+        x[i] = t;
+        w[i] = 1.0 / sum;
+    }
+}
+
+// Temporal part of cond_lens_temporal_spatial_quadratures (src/cpu_fcns.hpp:1540-1571): the
+// defocus spread is a Gaussian (height ti_a, sigma ti_sigma) plus an exponential (ti_beta)
+// component, integrated with the generalized Hermite rule of weight exp(-b_q x^2), b_q =
+// 1/(2 sigma_t^2), sigma_t^2 = ti_a ti_sigma^2 + 2 (1 - ti_a) ti_beta^2 (quadrature type 26 with
+// alpha = 0: Gauss-Hermite nodes / sqrt(b_q), weights / sqrt(b_q)), each weight times the ratio
+// of the spread function to that weight at the node.
+void temporal_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& w) {
+    if (!(L.ti_npts > 1 && !is_zero_f(L.ti_sigma))) {
+        x.assign(1, 0.0);
+        w.assign(1, 1.0);
+        return;
+    }
+    const double s2 = (double)L.ti_sigma * L.ti_sigma, b2 = (double)L.ti_beta * L.ti_beta;
+    const double a = L.ti_a / (std::sqrt(2.0 * 3.141592653589793238463) * L.ti_sigma);
+    const double b = 0.5 / s2;
+    const double c = is_zero_f(L.ti_beta) ? 0.0 : (1.0 - L.ti_a) / (2.0 * L.ti_beta);
+    const double d = is_zero_f(L.ti_beta) ? 0.0 : 1.0 / L.ti_beta;
+    const double sigma_t = std::sqrt(L.ti_a * s2 + 2.0 * (1.0 - L.ti_a) * b2);
+    const double b_q = 0.5 / (sigma_t * sigma_t);
+    gauss_hermite(L.ti_npts, x, w);
+    const double sc = 1.0 / std::sqrt(b_q);
+    for (int i = 0; i < L.ti_npts; i++) {
+        x[i] *= sc;
+        w[i] *= sc;
+        const double r = std::fabs(x[i]);
+        w[i] *= a * std::exp(-b * r * r + b_q * r * r) + c * std::exp(-d * r + b_q * r * r);
     }
 }
 
@@ -630,6 +706,8 @@ Model build_model(const mt_input_multislice* in) {
 
     m.cond_lens.from_input(in->cond_lens);
     m.cond_lens.set_input_data(m.E_0, m.grid);
+    m.illumination_model = in->illumination_model;
+    m.temporal_spatial_incoh = in->temporal_spatial_incoh;
     mt_lens obj = in->obj_lens;
     obj.si_sigma = in->cond_lens.si_sigma;  // ilc_multem.cu:251 reads the condenser's value
     m.obj_lens.from_input(obj);
@@ -752,7 +830,16 @@ Model build_model(const mt_input_multislice* in) {
         }
     }
 
+    // illumination (src/input_multislice.cuh:672-676, 747-776): exit waves are coherent; without
+    // full integration, or with spatial incoherence only, the condenser has one defocus point
+    if (m.is_EW()) m.illumination_model = 1;
+    if (is_zero_f(m.cond_lens.si_sigma)) m.temporal_spatial_incoh = 2;
+    const bool full_integration = (m.illumination_model == 4);
+    if (!full_integration || m.temporal_spatial_incoh == 3) m.cond_lens.ti_npts = 1;
     m.cond_lens.set_input_data(m.E_0, m.grid);
+    // Multislice::STEM_ISTEM integrates the defocus spread only under full integration
+    // (src/tem_simulation.cuh:136-176)
+    if (m.is_STEM() && full_integration) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
     m.cond_lens.zero_defocus_plane = A.size() ? m.cond_lens.get_zero_defocus_plane(A.z_min, A.z_max) : 0.0f;
     m.cond_lens.zero_defocus_type = 4;
     m.obj_lens.set_input_data(m.E_0, m.grid);

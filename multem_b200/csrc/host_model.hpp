@@ -49,6 +49,8 @@ struct LensF {
     float c_50 = 0, c_52 = 0, phi_52 = 0, c_54 = 0, phi_54 = 0, c_56 = 0, phi_56 = 0;
     float inner_aper_ang = 0, outer_aper_ang = 0;
     float si_sigma = 0;
+    float ti_a = 1, ti_sigma = 0, ti_beta = 0;  // defocus spread (temporal incoherence)
+    int ti_npts = 1;
     int zero_defocus_type = 1;
     float zero_defocus_plane = 0;
     float lambda = 0;
@@ -103,6 +105,10 @@ struct Model {
     int interaction_model = 1;
     int potential_type = 6;
     int pn_model = 1;
+    int illumination_model = 1, temporal_spatial_incoh = 1;
+    // defocus offsets (A) and weights of the condenser's temporal-incoherence quadrature; one
+    // point (0, 1) unless STEM integrates the illumination in full
+    std::vector<double> ti_x{0.0}, ti_w{1.0};
     bool pn_coh_contrib = false, pn_single_conf = false;
     int pn_nconf = 1, fp_iconf_0 = 1, pn_seed = 300183;
     bool pn_x = true, pn_y = true, pn_z = false;
@@ -165,6 +171,8 @@ bool line_size_supported(int n);
 // The fields ilc_propagate reads (grid, user wave, E_0, tilt); throws mtb::Error.
 Model build_prop_model(const mt_input_multislice* in);
 void snap_incident_angle(Model& m);
+void gauss_hermite(int n, std::vector<double>& x, std::vector<double>& w);
+void temporal_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& w);
 
 // Per-element spline-table header needed on the host (R_max drives statistics and footprints).
 struct AtomTypeHead {

@@ -118,3 +118,20 @@ def ewfs_tilt_si001():
     p = ew_tilt_si001()
     p.simulation_type = 51
     return p
+
+
+def stem_incoh_srtio3():
+    """STEM ADF through SrTiO3(001) on a 256^2 grid with the condenser's defocus spread integrated
+    (illumination_model 4, full integration): 5 defocus points of a Gaussian (sigma 32 A, height
+    0.8) plus exponential (beta 10 A) spread around c_10 = 20 A, 3 x 3 probes, two phonon
+    configurations."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=6)
+    p.illumination_model = 4
+    p.temporal_spatial_incoh = 2
+    p.cond_lens_c_10 = 20.0
+    p.cond_lens_ti_npts = 5
+    p.cond_lens_ti_sigma = 32.0
+    p.cond_lens_ti_a = 0.8
+    p.cond_lens_ti_beta = 10.0
+    return p
