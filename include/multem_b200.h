@@ -144,10 +144,14 @@ typedef struct mt_input_multislice {
     int scanning_ns;
     double scanning_x0, scanning_y0, scanning_xe, scanning_ye;
 
-    int detector_type;           /* 1 circular */
+    int detector_type;           /* 1 circular, 3 matrix */
     int n_detector;
-    const double* detector_inner_ang;   /* mrad */
-    const double* detector_outer_ang;   /* mrad */
+    const double* detector_inner_ang;   /* type 1: mrad */
+    const double* detector_outer_ang;   /* type 1: mrad */
+    /* type 3: n_detector sensitivity maps over the Fourier grid, centred (zero frequency at
+     * (nx/2, ny/2)) as the reference's detector.matrix(d).fR; value (ix, iy) of map d at
+     * [(d * nx + ix) * ny + iy] (ilc_multem.cu:316-335) */
+    const double* detector_fR;
 
     int output_area_ix_0, output_area_iy_0, output_area_ix_e, output_area_iy_e;  /* 1-based */
 } mt_input_multislice;

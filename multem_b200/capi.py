@@ -69,7 +69,7 @@ class MtInputMultislice(C.Structure):
         ("scanning_ns", c_int), ("scanning_x0", c_double), ("scanning_y0", c_double),
         ("scanning_xe", c_double), ("scanning_ye", c_double),
         ("detector_type", c_int), ("n_detector", c_int), ("detector_inner_ang", P_double),
-        ("detector_outer_ang", P_double),
+        ("detector_outer_ang", P_double), ("detector_fR", P_double),
         ("output_area_ix_0", c_int), ("output_area_iy_0", c_int), ("output_area_ix_e", c_int),
         ("output_area_iy_e", c_int),
     ]

@@ -105,6 +105,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
             idx[i] = i;
         }
         d_beam_.upload(beam.data(), beam.size(), stream_);
+        if (m_.det_type == 3) d_detmat_.upload(m_.det_fR.data(), m_.det_fR.size(), stream_);
         d_scan_idx_.upload(idx.data(), idx.size(), stream_);
         // probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
         // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
@@ -158,6 +159,7 @@ Engine::~Engine() {
             if (g.exec) cudaGraphExecDestroy(g.exec);
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
+        d_detmat_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
         d_err_.release_idle();
         d_scan_idx_.release_idle();
@@ -650,6 +652,7 @@ void Engine::run_stem(ConfData& cd) {
     }
     ca.gx_0 = 0;
     ca.gy_0 = 0;
+    ca.det_mat = d_detmat_.p;
     ca.det_w = col_det_width(nx);
     const bool tilt = d_ramp_.p != nullptr;
     RowArgs ra{};

@@ -157,6 +157,7 @@ class Engine {
     DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
+    DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)
     std::vector<ConfData> confs_;
     GridDev gdev_{};
     float probe_norm_ = 1.0f;

@@ -764,13 +764,32 @@ Model build_model(const mt_input_multislice* in) {
                 }
         }
         if (m.scan_nx <= 0 || m.scan_ny <= 0) fail(MT_ERR_INVALID_ARG, "empty scan");
-        if (in->detector_type != 1) fail(MT_ERR_UNSUPPORTED, "only circular detectors (type 1) are implemented");
+        if (in->detector_type != 1 && in->detector_type != 3)
+            fail(MT_ERR_UNSUPPORTED, "only circular (type 1) and matrix (type 3) detectors are implemented");
+        m.det_type = in->detector_type;
         float lam = lambda_f(m.E_0);
-        for (int i = 0; i < in->n_detector; i++) {
-            double ia = (double)(float)in->detector_inner_ang[i] * kMrad;
-            double oa = (double)(float)in->detector_outer_ang[i] * kMrad;
-            m.det_g_inner.push_back((float)(std::sin(ia) / lam));
-            m.det_g_outer.push_back((float)(std::sin(oa) / lam));
+        if (m.det_type == 1) {
+            for (int i = 0; i < in->n_detector; i++) {
+                double ia = (double)(float)in->detector_inner_ang[i] * kMrad;
+                double oa = (double)(float)in->detector_outer_ang[i] * kMrad;
+                m.det_g_inner.push_back((float)(std::sin(ia) / lam));
+                m.det_g_outer.push_back((float)(std::sin(oa) / lam));
+            }
+        } else if (in->n_detector > 0) {
+            // matrix detectors: fR as float, fft2-shifted to the FFT order the waves use
+            // (Wave_Function::set_input_data, src/wave_function.cuh:55-61)
+            if (!in->detector_fR) fail(MT_ERR_INVALID_ARG, "matrix detectors need detector_fR");
+            const int nx = m.grid.nx, ny = m.grid.ny, nxh = nx / 2, nyh = ny / 2;
+            const size_t nxy = (size_t)nx * ny;
+            m.det_fR.assign((size_t)in->n_detector * nxy, 0.0f);
+            for (int d = 0; d < in->n_detector; d++) {
+                m.det_g_inner.push_back(0.0f);
+                m.det_g_outer.push_back(0.0f);
+                for (int ix = 0; ix < nx; ix++)
+                    for (int iy = 0; iy < ny; iy++)
+                        m.det_fR[d * nxy + (size_t)((ix + nxh) % nx) * ny + (iy + nyh) % ny] =
+                            (float)in->detector_fR[d * nxy + (size_t)ix * ny + iy];
+            }
         }
         if (m.det_g_inner.empty()) fail(MT_ERR_INVALID_ARG, "STEM needs at least one detector");
         if (m.det_g_inner.size() > 8) fail(MT_ERR_UNSUPPORTED, "at most 8 detectors are supported");

@@ -137,7 +137,9 @@ struct Model {
     std::vector<float> scan_x, scan_y;  // every scan position, index ix*ny + iy
 
     // circular detectors (g in 1/A, float)
-    std::vector<float> det_g_inner, det_g_outer;
+    std::vector<float> det_g_inner, det_g_outer;  // one entry per detector (zeros for matrices)
+    int det_type = 1;                              // 1 circular, 3 matrix
+    std::vector<float> det_fR;                     // type 3: [d][ix][iy] in FFT order
 
     // output area (0-based, [ix_0, ix_e) x [iy_0, iy_e))
     int out_ix_0 = 0, out_ix_e = 0, out_iy_0 = 0, out_iy_e = 0;

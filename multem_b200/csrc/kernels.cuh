@@ -85,6 +85,7 @@ struct ColArgs {
     // detectors
     int n_det;
     float det_g2_min[kMaxDet], det_g2_max[kMaxDet];
+    const float* det_mat;      // matrix detectors: [n_det][nx][ny] sensitivity in FFT order, else NULL
     float gx_0, gy_0;
     double* det_partial;       // [nprobe][ny / det_w][n_det]
     int det_w;                 // columns per detector partial (col_det_width)

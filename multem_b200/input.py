@@ -172,7 +172,11 @@ class Parameters:
         det = self.detector or {"type": 1, "cir": []}
         s.detector_type = int(det.get("type", 1))
         cir = det.get("cir", []) if s.detector_type == 1 else []
-        s.n_detector = len(cir)
+        mats = det.get("matrix", []) if s.detector_type == 3 else []
+        s.n_detector = len(mats) if s.detector_type == 3 else len(cir)
         s.detector_inner_ang, _ = darr([c["inner_ang"] for c in cir] or [0.0])
         s.detector_outer_ang, _ = darr([c["outer_ang"] for c in cir] or [0.0])
+        # matrix detectors: fR is (ny, nx) as in MATLAB; stored x-major ([ix][iy])
+        fr = [np.asarray(m["fR"], dtype=np.float64).T.ravel() for m in mats]
+        s.detector_fR, _ = darr(np.concatenate(fr) if fr else [0.0])
         return s, keep

@@ -187,6 +187,14 @@ void fill_input(const mt_input_multislice* in, mt::Input_Multislice<T>& im, int 
                 auto outer_ang = in->detector_outer_ang[i] * mt::c_mrad_2_rad;
                 im.detector.g_outer[i] = sin(outer_ang) / lambda;
             }
+        } else if (im.detector.type == mt::eDT_Matrix && in->n_detector > 0) {
+            // as ilc_multem.cu:316-335: each map is assigned linearly (column-major ny x nx)
+            im.detector.resize(in->n_detector);
+            const size_t nxy = (size_t)in->nx * in->ny;
+            for (int i = 0; i < in->n_detector; i++) {
+                im.detector.fR[i].resize(nxy);
+                for (size_t k = 0; k < nxy; k++) im.detector.fR[i][k] = (T)in->detector_fR[i * nxy + k];
+            }
         }
     }
 

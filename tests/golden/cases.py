@@ -135,3 +135,21 @@ def stem_incoh_srtio3():
     p.cond_lens_ti_a = 0.8
     p.cond_lens_ti_beta = 10.0
     return p
+
+
+def stem_matrix_srtio3():
+    """STEM through SrTiO3(001) on a 256^2 grid with two matrix detectors given on the centred
+    Fourier grid (ny x nx, as detector.matrix(d).fR): a soft-edged annulus 30-90 mrad and one
+    quadrant (gx > 0, gy > 0) below 60 mrad, which pins the orientation and the fft-shift; 3 x 3
+    probes, one phonon configuration."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=1, seed=8)
+    lam = 0.019687  # A at 300 kV
+    gx = (np.arange(p.nx) - p.nx // 2) / p.spec_lx
+    gy = (np.arange(p.ny) - p.ny // 2) / p.spec_ly
+    GY, GX = np.meshgrid(gy, gx, indexing="ij")  # (ny, nx)
+    th = lam * np.hypot(GX, GY) * 1e3  # mrad
+    ring = 1 / (1 + np.exp(-(th - 30) / 2)) * 1 / (1 + np.exp((th - 90) / 2))
+    quad = ((GX > 0) & (GY > 0) & (th < 60)).astype(float)
+    p.detector = {"type": 3, "matrix": [{"fR": ring}, {"fR": quad}]}
+    return p
