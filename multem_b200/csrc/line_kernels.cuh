@@ -126,21 +126,6 @@ static size_t rows_smem() {
 __device__ __forceinline__ int ig_shift(int i, int nh, int n) { return (i < nh) ? i : (i - n); }
 
 // exp_i_chi (src/cgpu_fcns.cuh:1951-1980) for one Fourier-space pixel, times the normalisation.
-// One pixel's contribution to the detector sums (sum_square_over_Det, src/cgpu_fcns.cuh:1796-1814):
-// |psi_hat|^2 where g2_min <= |g|^2 < g2_max (rings), or weighted by each sensitivity map.
-__device__ __forceinline__ void det_add(const ColArgs& a, int ix, int iy, float g2, float v2, double* acc) {
-    if (a.det_mat) {
-        const size_t nxy = (size_t)a.g.nx * a.g.ny, p = (size_t)ix * a.g.ny + iy;
-#pragma unroll
-        for (int d = 0; d < kMaxDet; d++)
-            if (d < a.n_det) acc[d] += (double)__fmul_rn(__ldg(a.det_mat + d * nxy + p), v2);
-    } else {
-#pragma unroll
-        for (int d = 0; d < kMaxDet; d++)
-            if (d < a.n_det && a.det_g2_min[d] <= g2 && g2 < a.det_g2_max[d]) acc[d] += (double)v2;
-    }
-}
-
 __device__ __forceinline__ float2 probe_value(const ProbeDev& pr, const GridDev& g, int ix, int iy, float2 beam) {
     const float gx = __fadd_rn(__fmul_rn((float)ig_shift(ix, g.nxh, g.nx), g.dgx), pr.gxu);
     const float gy = __fadd_rn(__fmul_rn((float)ig_shift(iy, g.nyh, g.ny), g.dgy), pr.gyu);
@@ -187,6 +172,40 @@ __device__ __forceinline__ void write_det_partials(const ColArgs& a, int b, int 
     for (int i = tid; i < nsub * a.n_det; i += nthreads) {
         const int sub = i / a.n_det, d = i % a.n_det;
         a.det_partial[base + (size_t)sub * a.n_det + d] = (sub == 0) ? sum(d) : 0.0;
+    }
+}
+
+// A thread's contribution to the detector sums from its E pixels of column iy, in the layout the
+// last stage leaves (sum_square_over_Det, src/cgpu_fcns.cuh:1796-1814): |psi_hat|^2 where
+// g2_min <= |g|^2 < g2_max (rings), or weighted by each sensitivity map (matrix detectors).
+template <int NX>
+__device__ __forceinline__ void det_pixels(const ColArgs& a, const float2 (&x)[LineGeom<NX>::E], int t, int iy,
+                                           double* acc) {
+    using G = LineGeom<NX>;
+    if (a.det_mat) {
+        const size_t nxy = (size_t)a.g.nx * a.g.ny;
+#pragma unroll
+        for (int i = 0; i < G::E; i++) {
+            const int ix = reg_pos<NX, G::RL>(i, t);
+            const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
+            const float* m = a.det_mat + (size_t)ix * a.g.ny + iy;
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++)
+                if (d < a.n_det) acc[d] += (double)__fmul_rn(__ldg(m + d * nxy), v2);
+        }
+        return;
+    }
+    const float gy = __fsub_rn(__fmul_rn((float)ig_shift(iy, a.g.nyh, a.g.ny), a.g.dgy), 0.0f);
+    const float gy2 = __fmul_rn(gy, gy);
+#pragma unroll
+    for (int i = 0; i < G::E; i++) {
+        const int ix = reg_pos<NX, G::RL>(i, t);
+        const float gx = __fmul_rn((float)ig_shift(ix, a.g.nxh, a.g.nx), a.g.dgx);
+        const float g2 = __fadd_rn(__fmul_rn(gx, gx), gy2);
+        const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
+#pragma unroll
+        for (int d = 0; d < kMaxDet; d++)
+            if (d < a.n_det && a.det_g2_min[d] <= g2 && g2 < a.det_g2_max[d]) acc[d] += (double)v2;
     }
 }
 
@@ -257,16 +276,7 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
             double acc[kMaxDet];
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
-            const float gy = __fsub_rn(__fmul_rn((float)ig_shift(iy, a.g.nyh, a.g.ny), a.g.dgy), 0.0f);
-            const float gy2 = __fmul_rn(gy, gy);
-#pragma unroll
-            for (int i = 0; i < E; i++) {
-                const int ix = reg_pos<NX, G::RL>(i, t);
-                const float gx = __fmul_rn((float)ig_shift(ix, a.g.nxh, a.g.nx), a.g.dgx);
-                const float g2 = __fadd_rn(__fmul_rn(gx, gx), gy2);
-                const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
-                det_add(a, ix, iy, g2, v2, acc);
-            }
+            det_pixels<NX>(a, x, t, iy, acc);
             // deterministic block reduction: warp shuffles, then warps in order
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) {
@@ -639,16 +649,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             double acc[kMaxDet];
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
-            const float gy = __fsub_rn(__fmul_rn((float)ig_shift(iy, a.g.nyh, a.g.ny), a.g.dgy), 0.0f);
-            const float gy2 = __fmul_rn(gy, gy);
-#pragma unroll
-            for (int i = 0; i < E; i++) {
-                const int ix = reg_pos<NX, G::RL>(i, t);
-                const float gx = __fmul_rn((float)ig_shift(ix, a.g.nxh, a.g.nx), a.g.dgx);
-                const float g2 = __fadd_rn(__fmul_rn(gx, gx), gy2);
-                const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
-                det_add(a, ix, iy, g2, v2, acc);
-            }
+            det_pixels<NX>(a, x, t, iy, acc);
             // deterministic group reduction: warp shuffles, then the group's warps in order
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) {
