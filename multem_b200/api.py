@@ -44,12 +44,15 @@ class OutputBuffers:
         self.y = np.zeros(max(1, d.n_y))
         self.thick = np.zeros(max(1, d.n_thick))
         self.image_tot = np.zeros(max(1, d.n_thick * d.n_detector * nxy)) if d.has_image_tot else None
+        self.image_coh = np.zeros(max(1, d.n_thick * d.n_detector * nxy)) if d.has_image_coh else None
         self.m2psi_tot = np.zeros(max(1, d.n_thick * nxy)) if d.has_m2psi_tot else None
         self.psi_coh = np.zeros(max(1, 2 * d.n_thick * nxy)) if d.has_psi_coh else None
         o = capi.MtOutputMultislice()
         o.x, o.y, o.thick = _dp(self.x), _dp(self.y), _dp(self.thick)
         if self.image_tot is not None:
             o.image_tot = _dp(self.image_tot)
+        if self.image_coh is not None:
+            o.image_coh = _dp(self.image_coh)
         if self.m2psi_tot is not None:
             o.m2psi_tot = _dp(self.m2psi_tot)
         if self.psi_coh is not None:
@@ -66,6 +69,9 @@ class OutputBuffers:
             if self.image_tot is not None:
                 imgs = self.image_tot.reshape(d.n_thick, d.n_detector, nx, ny)[it]
                 e["image_tot"] = [imgs[k].T.copy() for k in range(d.n_detector)]
+            if self.image_coh is not None:
+                imgs = self.image_coh.reshape(d.n_thick, d.n_detector, nx, ny)[it]
+                e["image_coh"] = [imgs[k].T.copy() for k in range(d.n_detector)]
             if self.m2psi_tot is not None:
                 e["m2psi_tot"] = self.m2psi_tot.reshape(d.n_thick, nx, ny)[it].T.copy()
             if self.psi_coh is not None:

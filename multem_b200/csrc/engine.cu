@@ -106,6 +106,14 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         }
         d_beam_.upload(beam.data(), beam.size(), stream_);
         if (m_.det_type == 3) d_detmat_.upload(m_.det_fR.data(), m_.det_fR.size(), stream_);
+        if (m_.pn_coh_contrib) {
+            // the coherent part keeps every probe's transformed wave summed over configurations
+            const size_t n = (size_t)n_thk * m_.n_scan() * nxy;
+            if (n * sizeof(float2) > ((size_t)96 << 30))
+                fail(MT_ERR_UNSUPPORTED, "pn_coh_contrib: the probes' coherent waves need more than 96 GiB");
+            d_coh_.alloc(n);
+            d_image_coh_.alloc((size_t)n_thk * n_det * m_.n_scan());
+        }
         d_scan_idx_.upload(idx.data(), idx.size(), stream_);
         // probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
         // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
@@ -160,6 +168,8 @@ Engine::~Engine() {
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         d_detmat_.release_idle();
+        d_coh_.release_idle();
+        d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
         d_err_.release_idle();
         d_scan_idx_.release_idle();
@@ -188,6 +198,7 @@ void Engine::synchronize() {
 
 void Engine::reset() {
     if (d_image_.p) MTB_CUDA(cudaMemsetAsync(d_image_.p, 0, sizeof(double) * d_image_.n, stream_));
+    if (d_coh_.p) MTB_CUDA(cudaMemsetAsync(d_coh_.p, 0, sizeof(float2) * d_coh_.n, stream_));
     if (d_ew_psi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_psi_.p, 0, sizeof(double) * d_ew_psi_.n, stream_));
     if (d_ew_m2_.p) MTB_CUDA(cudaMemsetAsync(d_ew_m2_.p, 0, sizeof(double) * d_ew_m2_.n, stream_));
     iter_ = 0;
@@ -633,6 +644,22 @@ int Engine::tune_passes(int nprobe, ConfData& cd) {
     return chosen.emplace(key, bits).first->second;
 }
 
+ColArgs Engine::det_args() const {
+    ColArgs ca{};
+    ca.ny = m_.grid.ny;
+    ca.g = gdev_;
+    ca.n_det = (int)m_.det_g_inner.size();
+    for (int d = 0; d < ca.n_det; d++) {
+        // sum_square_over_Det bounds: g2 = pow(g, 2) stored as float (src/cpu_fcns.hpp:1168-1169)
+        ca.det_g2_min[d] = (float)std::pow((double)m_.det_g_inner[d], 2);
+        ca.det_g2_max[d] = (float)std::pow((double)m_.det_g_outer[d], 2);
+    }
+    ca.gx_0 = 0;
+    ca.gy_0 = 0;
+    ca.det_mat = d_detmat_.p;
+    return ca;
+}
+
 void Engine::run_stem(ConfData& cd) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const size_t nxy = (size_t)nx * ny;
@@ -641,19 +668,9 @@ void Engine::run_stem(ConfData& cd) {
     const int n_thk = (int)m_.thick.size();
     const int tiles = col_tiles(nx, ny);
     const size_t pl = (size_t)nx + ny;
-    ColArgs ca{};
-    ca.ny = ny;
-    ca.g = gdev_;
-    ca.n_det = n_det;
-    for (int d = 0; d < n_det; d++) {
-        // sum_square_over_Det bounds: g2 = pow(g, 2) stored as float (src/cpu_fcns.hpp:1168-1169)
-        ca.det_g2_min[d] = (float)std::pow((double)m_.det_g_inner[d], 2);
-        ca.det_g2_max[d] = (float)std::pow((double)m_.det_g_outer[d], 2);
-    }
-    ca.gx_0 = 0;
-    ca.gy_0 = 0;
-    ca.det_mat = d_detmat_.p;
+    ColArgs ca = det_args();
     ca.det_w = col_det_width(nx);
+    ca.coh_w = (float)m_.phonon_weight();
     const bool tilt = d_ramp_.p != nullptr;
     RowArgs ra{};
     ra.nx = nx;
@@ -690,6 +707,7 @@ void Engine::run_stem(ConfData& cd) {
             ca.Px = cd.prop.p + (size_t)k * pl;
             ca.Py = ca.Px + nx;
             ca.det_partial = d_partial_.p + (size_t)(ithk >= 0 ? ithk : 0) * batch_ * tiles * n_det;
+            ca.coh = (d_coh_.p && ithk >= 0) ? d_coh_.p + ((size_t)ithk * n_scan + p0) * nxy : nullptr;
             cols(flags, ca);
             if (tilt && ithk >= 0) {
                 // get_psi: phase ramp, then the detectors on the transform (the output
@@ -797,6 +815,7 @@ mt_output_dims output_dims(const Model& m_) {
         d.nx = m_.scan_nx;
         d.ny = m_.scan_ny;
         d.has_image_tot = 1;
+        d.has_image_coh = m_.pn_coh_contrib ? 1 : 0;
         d.n_x = (int)m_.scan_x.size();
         d.n_y = (int)m_.scan_y.size();
     } else {
@@ -834,6 +853,11 @@ void Engine::write_output(mt_output_multislice* out) {
             for (size_t i = 0; i < m_.scan_y.size(); i++) out->y[i] = m_.scan_y[i];
         if (out->image_tot)
             MTB_CUDA(cudaMemcpy(out->image_tot, d_image_.p, sizeof(double) * d_image_.n, cudaMemcpyDeviceToHost));
+        if (out->image_coh && d_coh_.p) {
+            launch_coh_detect(d_coh_.p, (int)m_.thick.size(), m_.n_scan(), det_args(), d_image_coh_.p, stream_);
+            synchronize();
+            MTB_CUDA(cudaMemcpy(out->image_coh, d_image_coh_.p, sizeof(double) * d_image_coh_.n, cudaMemcpyDeviceToHost));
+        }
     } else {
         const bool rs = m_.is_EWRS();
         out->dx = rs ? m_.grid.dRx : m_.grid.dgx;

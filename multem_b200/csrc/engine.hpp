@@ -158,6 +158,9 @@ class Engine {
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)
+    DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
+    DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
+    ColArgs det_args() const;        // detector description for the column pass
     std::vector<ConfData> confs_;
     GridDev gdev_{};
     float probe_norm_ = 1.0f;

@@ -805,7 +805,6 @@ Model build_model(const mt_input_multislice* in) {
     m.lambda = lambda_f(m.E_0);
     snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
-    if (m.is_STEM() && m.pn_coh_contrib) fail(MT_ERR_UNSUPPORTED, "STEM with pn_coh_contrib = 1 is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 
@@ -856,9 +855,9 @@ Model build_model(const mt_input_multislice* in) {
     const bool full_integration = (m.illumination_model == 4);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.cond_lens.ti_npts = 1;
     m.cond_lens.set_input_data(m.E_0, m.grid);
-    // Multislice::STEM_ISTEM integrates the defocus spread only under full integration
-    // (src/tem_simulation.cuh:136-176)
-    if (m.is_STEM() && full_integration) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
+    // Multislice::STEM_ISTEM integrates the defocus spread only under full integration, and not
+    // in its coherent-contribution branch, which comes first (src/tem_simulation.cuh:115-176)
+    if (m.is_STEM() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
     m.cond_lens.zero_defocus_plane = A.size() ? m.cond_lens.get_zero_defocus_plane(A.z_min, A.z_max) : 0.0f;
     m.cond_lens.zero_defocus_type = 4;
     m.obj_lens.set_input_data(m.E_0, m.grid);

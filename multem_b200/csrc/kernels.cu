@@ -318,6 +318,53 @@ void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det
 }
 
 // =============================================================================================
+// One CTA per (thickness, scan position): detector sums of |psi_coh|^2 over the grid, per-thread
+// partials in FP64 reduced in a fixed order.
+__global__ void coh_detect_kernel(const float2* __restrict__ coh, int n_scan, ColArgs a, double* __restrict__ image) {
+    const int ithk = blockIdx.x / n_scan, iscan = blockIdx.x % n_scan;
+    const size_t nxy = (size_t)a.g.nx * a.g.ny;
+    const float2* c = coh + ((size_t)ithk * n_scan + iscan) * nxy;
+    double acc[kMaxDet];
+#pragma unroll
+    for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
+    for (size_t p = threadIdx.x; p < nxy; p += blockDim.x) {
+        const int ix = (int)(p / a.g.ny), iy = (int)(p % a.g.ny);
+        const float2 v = c[p];
+        const float v2 = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+        if (a.det_mat) {
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++)
+                if (d < a.n_det) acc[d] += (double)__fmul_rn(a.det_mat[d * nxy + p], v2);
+        } else {
+            const float gx = __fmul_rn((float)((ix < a.g.nxh) ? ix : ix - a.g.nx), a.g.dgx);
+            const float gy = __fmul_rn((float)((iy < a.g.nyh) ? iy : iy - a.g.ny), a.g.dgy);
+            const float g2 = __fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy));
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++)
+                if (d < a.n_det && a.det_g2_min[d] <= g2 && g2 < a.det_g2_max[d]) acc[d] += (double)v2;
+        }
+    }
+    __shared__ double red[kMaxDet][256];
+#pragma unroll
+    for (int d = 0; d < kMaxDet; d++) red[d][threadIdx.x] = acc[d];
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+#pragma unroll
+            for (int d = 0; d < kMaxDet; d++) red[d][threadIdx.x] += red[d][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < (unsigned)a.n_det)
+        image[((size_t)ithk * a.n_det + threadIdx.x) * n_scan + iscan] = red[threadIdx.x][0];
+}
+
+void launch_coh_detect(const float2* coh, int n_thk, int n_scan, const ColArgs& det, double* image_coh,
+                       cudaStream_t s) {
+    coh_detect_kernel<<<(unsigned)(n_thk * n_scan), 256, 0, s>>>(coh, n_scan, det, image_coh);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
 // EW output accumulation with fft-shift and crop (add_scale_crop_shift_2d /
 // add_scale_square_crop_shift_2d / assign_crop_shift_2d, src/cgpu_fcns.cuh:1681-1780).
 __global__ void ew_accumulate_kernel(const float2* __restrict__ psi, int nx, int ny, int ix0, int ix1, int iy0,

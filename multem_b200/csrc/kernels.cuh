@@ -86,6 +86,8 @@ struct ColArgs {
     int n_det;
     float det_g2_min[kMaxDet], det_g2_max[kMaxDet];
     const float* det_mat;      // matrix detectors: [n_det][nx][ny] sensitivity in FFT order, else NULL
+    float2* coh;               // coherent part: [nprobe][nx][ny] sums of coh_w * psi_hat, else NULL
+    float coh_w;
     float gx_0, gy_0;
     double* det_partial;       // [nprobe][ny / det_w][n_det]
     int det_w;                 // columns per detector partial (col_det_width)
@@ -98,6 +100,12 @@ int col_tiles(int nx, int ny);  // detector partials per probe per detector (ny 
 // Sum detector partials over tiles and add w * sum into image[(idet*n_scan) + scan_index].
 void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det, const int* scan_index,
                        double w, double* image, int n_scan, cudaStream_t s);
+
+// STEM coherent images (Wave_Function::set_m2psi_coh, src/wave_function.cuh:189-209): for each
+// thickness and scan position, the detector sums of |psi_coh|^2 (weight 1) into
+// image_coh[(ithk*n_det + idet)*n_scan + iscan]; coh is [n_thk][n_scan][nx][ny] in FFT order.
+void launch_coh_detect(const float2* coh, int n_thk, int n_scan, const ColArgs& det, double* image_coh,
+                       cudaStream_t s);
 
 // EW output: out[(ix-ix0)*oy + (iy-iy0)] accumulates psi (complex) and |psi|^2 over the output
 // area after an fft-shift by (nx/2, ny/2) (add_scale_crop_shift_2d, src/cgpu_fcns.cuh:1701-1739).

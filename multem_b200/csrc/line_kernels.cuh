@@ -209,6 +209,20 @@ __device__ __forceinline__ void det_pixels(const ColArgs& a, const float2 (&x)[L
     }
 }
 
+// Coherent part of STEM (Output_Multislice::add_scale_psi_coh, src/output_multislice.hpp:770-780):
+// psi_coh += coh_w * psi_hat at this probe's pixels, in FP32 like the reference.
+template <int NX>
+__device__ __forceinline__ void coh_add(const ColArgs& a, int b, const float2 (&x)[LineGeom<NX>::E], int t, int iy) {
+    using G = LineGeom<NX>;
+    float2* c = a.coh + (size_t)b * a.g.nx * a.g.ny + iy;
+#pragma unroll
+    for (int i = 0; i < G::E; i++) {
+        float2* q = c + (size_t)reg_pos<NX, G::RL>(i, t) * a.g.ny;
+        const float2 v = *q;
+        *q = make_float2(__fadd_rn(__fmul_rn(a.coh_w, x[i].x), v.x), __fadd_rn(__fmul_rn(a.coh_w, x[i].y), v.y));
+    }
+}
+
 // LDY is the line stride (= ny) when known at compile time (square grids), 0 for a runtime stride.
 template <int NX, int FLAGS, int LDY>
 __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_kernel(ColArgs a) {
@@ -277,6 +291,7 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
             det_pixels<NX>(a, x, t, iy, acc);
+            if (a.coh) coh_add<NX>(a, b, x, t, iy);
             // deterministic block reduction: warp shuffles, then warps in order
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) {
@@ -650,6 +665,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
             det_pixels<NX>(a, x, t, iy, acc);
+            if (a.coh) coh_add<NX>(a, b, x, t, iy);
             // deterministic group reduction: warp shuffles, then the group's warps in order
 #pragma unroll
             for (int d = 0; d < kMaxDet; d++) {

@@ -153,3 +153,13 @@ def stem_matrix_srtio3():
     quad = ((GX > 0) & (GY > 0) & (th < 60)).astype(float)
     p.detector = {"type": 3, "matrix": [{"fR": ring}, {"fR": quad}]}
     return p
+
+
+def stem_coh_srtio3():
+    """STEM ADF through SrTiO3(001) on a 256^2 grid with the coherent contribution
+    (pn_coh_contrib = 1: image_coh from the configuration-averaged transformed wave), 3 x 3 probes,
+    three phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=3, seed=10)
+    p.pn_coh_contrib = 1
+    return p

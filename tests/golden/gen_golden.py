@@ -22,7 +22,8 @@ sys.path.insert(0, str(ROOT))
 
 from multem_b200 import specimens  # noqa: E402
 from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384,  # noqa: E402
-                   stem_tilt_au001, ew_tilt_si001, ewfs_tilt_si001, stem_incoh_srtio3, stem_matrix_srtio3)
+                   stem_tilt_au001, ew_tilt_si001, ewfs_tilt_si001, stem_incoh_srtio3, stem_matrix_srtio3,
+                   stem_coh_srtio3)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -52,7 +53,7 @@ def ew_config1():
 FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_1024), ("stem_1024", stem_1024),
              ("amorph_au110", amorph_au110), ("stem_tilt_au001", stem_tilt_au001), ("ew_tilt_si001", ew_tilt_si001),
              ("ewfs_tilt_si001", ewfs_tilt_si001), ("stem_incoh_srtio3", stem_incoh_srtio3),
-             ("stem_matrix_srtio3", stem_matrix_srtio3))
+             ("stem_matrix_srtio3", stem_matrix_srtio3), ("stem_coh_srtio3", stem_coh_srtio3))
 
 
 def full_runs(rec, names=None):
@@ -63,7 +64,7 @@ def full_runs(rec, names=None):
         p = fn()
         for prec in (1, 2):
             out = R.run(p, precision=prec, nthreads=8)
-            for k in ("image_tot", "psi_coh", "m2psi_tot", "thick", "x", "y"):
+            for k in ("image_tot", "image_coh", "psi_coh", "m2psi_tot", "thick", "x", "y"):
                 if k in out:
                     v = out[k]
                     rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
