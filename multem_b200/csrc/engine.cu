@@ -77,7 +77,8 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     if (!line_size_supported(nx) || !line_size_supported(ny))
         fail(MT_ERR_UNSUPPORTED, "nx and ny must be one of 64, 128, 256, 384, 512, 1024, 2048");
-    if (m_.is_EW() && !m_.is_plane_wave()) fail(MT_ERR_UNSUPPORTED, "EW simulations need a plane incident wave");
+    if (m_.is_plane_sim() && !m_.is_plane_wave())
+        fail(MT_ERR_UNSUPPORTED, "EW, ED and HRTEM simulations need a plane incident wave");
 
     gdev_ = grid_dev(m_.grid);
 
@@ -135,12 +136,13 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     } else {
         batch_ = 1;
         const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
-        d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
+        if (m_.is_EW()) d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
         niter_ = m_.number_conf();
     }
     d_psi_.alloc((size_t)batch_ * nxy);
+    if (m_.is_HRTEM()) build_ctf_tables();
     if (m_.tilted()) {
         build_tilt_ramp();
         // STEM outputs at intermediate thicknesses apply the ramp to a copy of the batch
@@ -168,6 +170,7 @@ Engine::~Engine() {
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         d_detmat_.release_idle();
+        d_ctf_.release_idle();
         d_coh_.release_idle();
         d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -253,6 +256,62 @@ void Engine::build_tilt_ramp() {
         }
     }
     d_ramp_.upload(ramp.data(), ramp.size(), stream_);
+}
+
+// HRTEM: the objective's transfer function per defocus point (Microscope_Effects, see
+// hrtem_ctf_points), as [nx][ny] tables in FFT order that the output column pass multiplies in
+// after the back-propagation factors (get_psi then apply_CTF / apply_PCTF).
+void Engine::build_ctf_tables() {
+    const size_t nxy = (size_t)m_.grid.nx * m_.grid.ny;
+    const size_t np = m_.obj_c10.size();
+    d_ctf_.alloc(np * nxy);
+    for (size_t j = 0; j < np; j++) {
+        LensF L = m_.obj_lens;
+        if (m_.ctf_mode == 2) {
+            // PCTF_LI_WPO_TEM (src/microscope_effects.cuh:124-151): temporal only drops the
+            // source spread, spatial only the defocus spread
+            const float si = (m_.temporal_spatial_incoh == 2) ? 0.0f : L.si_sigma;
+            const float ti = (m_.temporal_spatial_incoh == 3) ? 0.0f : L.ti_sigma;
+            PctfArgs p{};
+            p.g2_min = L.g2_min;
+            p.g2_max = L.g2_max;
+            p.c_c_10 = L.c_c_10;
+            p.c_c_30 = L.c_c_30;
+            p.c_10 = L.c_10;
+            p.c_30 = L.c_30;
+            p.lambda = L.lambda;
+            p.lambda2 = (float)std::pow((double)L.lambda, 2);
+            p.ti_iehwgd = (float)(1.414213562373095048802 * (double)ti);
+            p.si_theta_c = std::asin((float)(1.414213562373095048802 * (double)si) * L.lambda);
+            launch_pctf_table(p, gdev_, d_ctf_.p + j * nxy, stream_);
+        } else {
+            L.set_defocus(m_.obj_c10[j]);
+            ProbeDev pr{};
+            pr.c_c_10 = L.c_c_10;
+            pr.nz_c10 = !is_zero_f(L.c_10);
+            pr.c_c_30 = L.c_c_30;
+            pr.nz_c30 = !is_zero_f(L.c_30);
+            pr.c_c_50 = L.c_c_50;
+            pr.nz_c50 = !is_zero_f(L.c_50);
+            pr.g2_min = L.g2_min;
+            pr.g2_max = L.g2_max;
+            pr.norm = 1.0f;
+            pr.phi_required = L.is_phi_required();
+            pr.m = L.m;
+            pr.c_c_12 = L.c_c_12; pr.phi_12 = L.phi_12;
+            pr.c_c_21 = L.c_c_21; pr.phi_21 = L.phi_21;
+            pr.c_c_23 = L.c_c_23; pr.phi_23 = L.phi_23;
+            pr.c_c_32 = L.c_c_32; pr.phi_32 = L.phi_32;
+            pr.c_c_34 = L.c_c_34; pr.phi_34 = L.phi_34;
+            pr.c_c_41 = L.c_c_41; pr.phi_41 = L.phi_41;
+            pr.c_c_43 = L.c_c_43; pr.phi_43 = L.phi_43;
+            pr.c_c_45 = L.c_c_45; pr.phi_45 = L.phi_45;
+            pr.c_c_52 = L.c_c_52; pr.phi_52 = L.phi_52;
+            pr.c_c_54 = L.c_c_54; pr.phi_54 = L.phi_54;
+            pr.c_c_56 = L.c_c_56; pr.phi_56 = L.phi_56;
+            launch_ctf_table(pr, gdev_, d_ctf_.p + j * nxy, stream_);
+        }
+    }
 }
 
 // Fresnel propagator factors for distance dz, separable in x and y:
@@ -781,6 +840,24 @@ void Engine::run_ew(ConfData& cd) {
         cb.out = d_tmp_.p;
         cb.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
         cb.Py = cb.Px + nx;
+        if (m_.is_HRTEM()) {
+            // image formation: transfer function per defocus point, inverse transform, |psi|^2
+            // weighted (Microscope_Effects::operator(), src/microscope_effects.cuh:56-85)
+            for (size_t j = 0; j < m_.obj_c10.size(); j++) {
+                ColArgs cj = cb;
+                cj.P2 = d_ctf_.p + j * nxy;
+                cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cj);
+                RowArgs rb = ra;
+                rb.in = d_tmp_.p;
+                rb.out = d_tmp_.p;
+                rb.scale = 1.0f;
+                rows(ROW_INVERSE, rb);
+                launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e,
+                                     (double)(float)(w * m_.obj_w[j]), 0, nullptr, d_ew_m2_.p + (size_t)ithk * onxy,
+                                     stream_);
+            }
+            continue;
+        }
         if (m_.is_EWRS()) {
             RowArgs rb = ra;
             if (zbp != 0.0f) {
@@ -796,9 +873,10 @@ void Engine::run_ew(ConfData& cd) {
         } else {
             cols(COL_LOAD | COL_PROP | COL_STORE, cb);
         }
+        // ED keeps only |psi_hat|^2 (add_scale_crop_shift_m2psi_tot_from_psi, wave_function.cuh:172-184)
         launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
-                             d_ew_psi_.p + (size_t)ithk * onxy * 2, sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy,
-                             stream_);
+                             m_.is_ED() ? nullptr : d_ew_psi_.p + (size_t)ithk * onxy * 2,
+                             sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
     }
     iter_ += 1;
     check_cancel();
@@ -821,7 +899,7 @@ mt_output_dims output_dims(const Model& m_) {
     } else {
         d.nx = m_.out_ix_e - m_.out_ix_0;
         d.ny = m_.out_iy_e - m_.out_iy_0;
-        d.has_psi_coh = 1;
+        d.has_psi_coh = m_.is_EW() ? 1 : 0;
         d.has_m2psi_tot = m_.is_EW_SC() ? 0 : 1;
         d.n_x = d.nx;
         d.n_y = d.ny;
@@ -859,7 +937,7 @@ void Engine::write_output(mt_output_multislice* out) {
             MTB_CUDA(cudaMemcpy(out->image_coh, d_image_coh_.p, sizeof(double) * d_image_coh_.n, cudaMemcpyDeviceToHost));
         }
     } else {
-        const bool rs = m_.is_EWRS();
+        const bool rs = !m_.is_grid_FS();
         out->dx = rs ? m_.grid.dRx : m_.grid.dgx;
         out->dy = rs ? m_.grid.dRy : m_.grid.dgy;
         if (out->x)
@@ -868,7 +946,7 @@ void Engine::write_output(mt_output_multislice* out) {
         if (out->y)
             for (int iy = m_.out_iy_0; iy < m_.out_iy_e; iy++)
                 out->y[iy - m_.out_iy_0] = rs ? m_.grid.Ry(iy) : m_.grid.gy(iy);
-        if (out->psi_coh)
+        if (out->psi_coh && d.has_psi_coh)
             MTB_CUDA(cudaMemcpy(out->psi_coh, d_ew_psi_.p, sizeof(double) * d_ew_psi_.n, cudaMemcpyDeviceToHost));
         if (out->m2psi_tot && d.has_m2psi_tot)
             MTB_CUDA(cudaMemcpy(out->m2psi_tot, d_ew_m2_.p, sizeof(double) * d_ew_m2_.n, cudaMemcpyDeviceToHost));

@@ -158,6 +158,7 @@ class Engine {
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)
+    DevBuf<float2> d_ctf_;           // HRTEM transfer functions, one [nx][ny] table per defocus point
     DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
     DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
     ColArgs det_args() const;        // detector description for the column pass
@@ -174,6 +175,7 @@ class Engine {
     void run_ew(ConfData& cd);
     void prop_tables(float dz, float2* px, float2* py, bool output) const;
     ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
+    void build_ctf_tables();
     void check_cancel();
     ConfData* find_conf(int iconf);
 

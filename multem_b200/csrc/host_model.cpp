@@ -559,6 +559,43 @@ void temporal_quadrature(const LensF& L, std::vector<double>& x, std::vector<dou
     }
 }
 
+// Microscope_Effects (src/microscope_effects.cuh:32-200) for HRTEM: the coherent CTF
+// (illumination 1), the partially coherent CTF with temporal and spatial envelopes (2), or the
+// sum over the objective's defocus spread (4: Gauss-Hermite points of
+// obj_lens_temporal_spatial_quadratures, src/cpu_fcns.hpp:1504-1510, weights / sqrt(pi), defocus
+// c_10 + sqrt(2) ti_sigma x). The reference's spatial quadrature for 4 ends empty (its qs.resize(0),
+// cpu_fcns.hpp:1535, so those images are zero) and 3 computes nothing; both are refused.
+void hrtem_ctf_points(Model& m) {
+    const LensF& L = m.obj_lens;
+    m.obj_c10.assign(1, L.c_10);
+    m.obj_w.assign(1, 1.0);
+    switch (m.illumination_model) {
+        case 1:
+        case 2:
+            m.ctf_mode = m.illumination_model;
+            return;
+        case 4:
+            if (m.temporal_spatial_incoh != 2)
+                fail(MT_ERR_UNSUPPORTED, "HRTEM full integration with spatial incoherence: the reference's spatial "
+                                         "quadrature is empty (zero images); use temporal_spatial_incoh 2");
+            m.ctf_mode = 4;
+            {
+                std::vector<double> x, w;
+                gauss_hermite(L.ti_npts, x, w);
+                const float iehwgd = (float)(1.414213562373095048802 * (double)L.ti_sigma);
+                m.obj_c10.clear();
+                m.obj_w.clear();
+                for (int j = 0; j < L.ti_npts; j++) {
+                    m.obj_c10.push_back((float)((double)iehwgd * (float)x[j] + (double)L.c_10));
+                    m.obj_w.push_back((double)(float)(w[j] / std::sqrt(3.141592653589793238463)));
+                }
+            }
+            return;
+        default:
+            fail(MT_ERR_UNSUPPORTED, "HRTEM needs illumination_model 1, 2 or 4 (3 computes nothing in the reference)");
+    }
+}
+
 // isZero(gx_0, gy_0) of Wave_Function::phase_multiplication (src/wave_function.cuh:79)
 bool Model::tilted() const { return !(is_zero_f(gx_0()) && is_zero_f(gy_0())); }
 
@@ -612,9 +649,10 @@ Model build_model(const mt_input_multislice* in) {
     if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
     Model m;
     m.simulation_type = in->simulation_type;
-    if (!(m.is_STEM() || m.is_EW()))
+    if (!(m.is_STEM() || m.is_plane_sim()))
         fail(MT_ERR_UNSUPPORTED, "simulation_type " + std::to_string(in->simulation_type) +
-                                     " is outside the plain multislice path (supported: 11 STEM, 51 EWFS, 52 EWRS)");
+                                     " is outside the plain multislice path (supported: 11 STEM, 31 ED, 32 HRTEM, "
+                                     "51 EWFS, 52 EWRS)");
     m.interaction_model = in->interaction_model;
     if (m.interaction_model != 1) fail(MT_ERR_UNSUPPORTED, "only interaction_model 1 (multislice) is implemented");
     m.potential_type = in->potential_type;
@@ -805,6 +843,8 @@ Model build_model(const mt_input_multislice* in) {
     m.lambda = lambda_f(m.E_0);
     snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
+    if ((m.is_ED() || m.is_HRTEM()) && m.pn_coh_contrib)
+        fail(MT_ERR_UNSUPPORTED, "ED/HRTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 
@@ -855,6 +895,9 @@ Model build_model(const mt_input_multislice* in) {
     const bool full_integration = (m.illumination_model == 4);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.cond_lens.ti_npts = 1;
     m.cond_lens.set_input_data(m.E_0, m.grid);
+    if (!full_integration || m.temporal_spatial_incoh == 3) m.obj_lens.ti_npts = 1;
+    m.obj_lens.set_input_data(m.E_0, m.grid);
+    if (m.is_HRTEM()) hrtem_ctf_points(m);
     // Multislice::STEM_ISTEM integrates the defocus spread only under full integration, and not
     // in its coherent-contribution branch, which comes first (src/tem_simulation.cuh:115-176)
     if (m.is_STEM() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
@@ -884,7 +927,7 @@ Model build_model(const mt_input_multislice* in) {
     // an area given by the caller (not the "whole grid" default ix_0 == ix_e) that had to be
     // reordered or clipped
     const bool area_given = in->output_area_ix_0 != in->output_area_ix_e || in->output_area_iy_0 != in->output_area_iy_e;
-    if (m.is_EW() && area_given &&
+    if (m.is_plane_sim() && area_given &&
         (m.out_ix_0 != in->output_area_ix_0 - 1 || m.out_ix_e != in->output_area_ix_e - 1 ||
          m.out_iy_0 != in->output_area_iy_0 - 1 || m.out_iy_e != in->output_area_iy_e - 1))
         m.clamps.push_back("output_area -> ix [" + std::to_string(m.out_ix_0 + 1) + ", " + std::to_string(m.out_ix_e + 1) +

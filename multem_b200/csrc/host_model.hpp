@@ -109,6 +109,12 @@ struct Model {
     // defocus offsets (A) and weights of the condenser's temporal-incoherence quadrature; one
     // point (0, 1) unless STEM integrates the illumination in full
     std::vector<double> ti_x{0.0}, ti_w{1.0};
+    // HRTEM image formation (Microscope_Effects): 1 coherent CTF, 2 partially coherent CTF
+    // (envelopes), 4 numerical integration over the objective's defocus spread; obj_c10 and obj_w
+    // are the defocus and weight of each point (one point unless 4)
+    int ctf_mode = 1;
+    std::vector<float> obj_c10;
+    std::vector<double> obj_w;
     bool pn_coh_contrib = false, pn_single_conf = false;
     int pn_nconf = 1, fp_iconf_0 = 1, pn_seed = 300183;
     bool pn_x = true, pn_y = true, pn_z = false;
@@ -151,6 +157,12 @@ struct Model {
     bool is_EWFS() const { return simulation_type == 51; }
     bool is_EWRS() const { return simulation_type == 52; }
     bool is_EW() const { return is_EWFS() || is_EWRS(); }
+    bool is_ED() const { return simulation_type == 31; }
+    bool is_HRTEM() const { return simulation_type == 32; }
+    // one plane wave per configuration through the slice loop (EWFS, EWRS, ED, HRTEM)
+    bool is_plane_sim() const { return is_EW() || is_ED() || is_HRTEM(); }
+    // outputs on the Fourier grid (is_grid_FS, src/input_multislice.cuh:367-372)
+    bool is_grid_FS() const { return is_EWFS() || is_ED(); }
     bool is_frozen_phonon() const { return pn_model == 3; }
     bool is_EW_SC() const { return is_EW() && is_frozen_phonon() && pn_single_conf; }
     bool is_plane_wave() const { return iw_type == 1; }
@@ -175,6 +187,7 @@ Model build_prop_model(const mt_input_multislice* in);
 void snap_incident_angle(Model& m);
 void gauss_hermite(int n, std::vector<double>& x, std::vector<double>& w);
 void temporal_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& w);
+void hrtem_ctf_points(Model& m);
 
 // Per-element spline-table header needed on the host (R_max drives statistics and footprints).
 struct AtomTypeHead {

@@ -79,6 +79,7 @@ struct ColArgs {
     GridDev g;
     const float2* Px;          // [nx] propagator factor along x (includes 1/N)
     const float2* Py;          // [ny]
+    const float2* P2;          // optional [nx][ny] factor applied after Px * Py (HRTEM transfer function)
     // probe generation
     const float2* beam;        // per probe (x, y) = exp_factor_R(beam position)
     ProbeDev probe;
@@ -100,6 +101,15 @@ int col_tiles(int nx, int ny);  // detector partials per probe per detector (ny 
 // Sum detector partials over tiles and add w * sum into image[(idet*n_scan) + scan_index].
 void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det, const int* scan_index,
                        double w, double* image, int n_scan, cudaStream_t s);
+
+// HRTEM transfer functions over the Fourier grid ([ix][iy], FFT order): exp_i_chi of `lens` (apply_CTF,
+// src/cgpu_fcns.cuh:1995-2006), or the partially coherent one with temporal and spatial envelopes
+// (apply_PCTF, :2010-2040).
+struct PctfArgs {
+    float g2_min, g2_max, c_c_10, c_c_30, c_10, c_30, lambda, lambda2, si_theta_c, ti_iehwgd;
+};
+void launch_ctf_table(const ProbeDev& lens, const GridDev& g, float2* out, cudaStream_t s);
+void launch_pctf_table(const PctfArgs& p, const GridDev& g, float2* out, cudaStream_t s);
 
 // STEM coherent images (Wave_Function::set_m2psi_coh, src/wave_function.cuh:189-209): for each
 // thickness and scan position, the detector sums of |psi_coh|^2 (weight 1) into

@@ -285,6 +285,11 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
             const float2 py = a.Py[iy];
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], cmul(s_px[reg_pos<NX, G::RL>(i, t)], py));
+            if (a.P2) {
+                const float2* p2 = a.P2 + iy;
+#pragma unroll
+                for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(p2 + (size_t)reg_pos<NX, G::RL>(i, t) * a.g.ny));
+            }
         }
         if constexpr (DET) {
             double acc[kMaxDet];
@@ -659,6 +664,11 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             const float2 py = a.Py[iy];
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], cmul(s_px[reg_pos<NX, G::RL>(i, t)], py));
+            if (a.P2) {
+                const float2* p2 = a.P2 + iy;
+#pragma unroll
+                for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(p2 + (size_t)reg_pos<NX, G::RL>(i, t) * a.g.ny));
+            }
         }
         if constexpr (DET) {
             double acc[kMaxDet];

@@ -163,3 +163,58 @@ def stem_coh_srtio3():
     p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=3, seed=10)
     p.pn_coh_contrib = 1
     return p
+
+
+def ed_si001():
+    """Electron diffraction (simulation_type 31) of Si(001) on a 256^2 grid: |psi_hat|^2 of the exit
+    wave averaged over two phonon configurations, with a cropped output window."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.simulation_type = 31
+    p.pn_nconf = 2
+    p.pn_seed = 3
+    p.output_area_ix_0, p.output_area_ix_e = 65, 192
+    p.output_area_iy_0, p.output_area_iy_e = 65, 192
+    return p
+
+
+def _hrtem(illumination):
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.simulation_type = 32
+    p.pn_nconf = 2
+    p.pn_seed = 4
+    p.illumination_model = illumination
+    p.obj_lens_c_10 = 60.0
+    p.obj_lens_c_30 = 0.002
+    p.obj_lens_c_12 = 20.0
+    p.obj_lens_phi_12 = 30.0
+    p.obj_lens_outer_aper_ang = 22.0
+    return p
+
+
+def hrtem_coherent_si001():
+    """HRTEM image of Si(001) (simulation_type 32), coherent transfer function: defocus 60 A,
+    C3 0.002 mm, 2-fold astigmatism 20 A at 30 deg, 22 mrad aperture; two phonon configurations."""
+    return _hrtem(1)
+
+
+def hrtem_pctf_si001():
+    """hrtem_coherent_si001 with the partially coherent transfer function (temporal and spatial
+    envelopes: ti_sigma 32 A, si_sigma 0.0072 1/A)."""
+    p = _hrtem(2)
+    p.temporal_spatial_incoh = 1
+    p.obj_lens_ti_sigma = 32.0
+    p.cond_lens_si_sigma = 0.0072
+    return p
+
+
+def hrtem_fullint_si001():
+    """hrtem_coherent_si001 integrated numerically over the objective's defocus spread (illumination
+    4, temporal only): 7 Gauss-Hermite points, ti_sigma 32 A."""
+    p = _hrtem(4)
+    p.temporal_spatial_incoh = 2
+    p.obj_lens_ti_sigma = 32.0
+    p.obj_lens_ti_npts = 7
+    p.cond_lens_si_sigma = 0.0
+    return p
