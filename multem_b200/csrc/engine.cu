@@ -77,8 +77,6 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     if (!line_size_supported(nx) || !line_size_supported(ny))
         fail(MT_ERR_UNSUPPORTED, "nx and ny must be one of 64, 128, 256, 384, 512, 1024, 2048");
-    if (m_.is_plane_sim() && !m_.is_plane_wave())
-        fail(MT_ERR_UNSUPPORTED, "EW, ED and HRTEM simulations need a plane incident wave");
 
     gdev_ = grid_dev(m_.grid);
 
@@ -116,22 +114,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
             d_image_coh_.alloc((size_t)n_thk * n_det * m_.n_scan());
         }
         d_scan_idx_.upload(idx.data(), idx.size(), stream_);
-        // probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
-        // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
-        // aperture's pixel count (aperture test in the kernel's float arithmetic; no tilt offset
-        // in the simulation's probes).
-        const LensF& L = m_.cond_lens;
-        double count = 0;
-        for (int ix = 0; ix < nx; ix++) {
-            float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx;
-            for (int iy = 0; iy < ny; iy++) {
-                float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy;
-                float g2 = gx * gx + gy * gy;
-                if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
-            }
-        }
-        if (count <= 0) fail(MT_ERR_INVALID_ARG, "condenser aperture contains no Fourier pixel");
-        probe_norm_ = (float)std::sqrt(1.0 / (double)(float)count);
+        probe_norm_ = aperture_norm();
         niter_ = m_.n_scan() * m_.number_conf() * (int)m_.ti_x.size();
     } else {
         batch_ = 1;
@@ -140,9 +123,20 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
         niter_ = m_.number_conf();
+        if (m_.is_convergent_wave()) {
+            // convergent beams at iw_x/iw_y, summed (Incident_Wave::operator(), src/incident_wave.cuh:72-90)
+            const int nb = (int)m_.iw_x.size();
+            if (nb <= 0 || m_.iw_y.size() != m_.iw_x.size()) fail(MT_ERR_INVALID_ARG, "convergent wave needs iw_x/iw_y");
+            std::vector<float2> beam(nb);
+            for (int i = 0; i < nb; i++)
+                beam[i] = make_float2(m_.grid.exp_factor_Rx(m_.iw_x[i]), m_.grid.exp_factor_Ry(m_.iw_y[i]));
+            d_beam_.upload(beam.data(), beam.size(), stream_);
+            if (nb > 1) d_beams_psi_.alloc((size_t)nb * nxy);
+            probe_norm_ = aperture_norm();
+        }
     }
     d_psi_.alloc((size_t)batch_ * nxy);
-    if (m_.is_HRTEM()) build_ctf_tables();
+    if (m_.is_imaging()) build_ctf_tables();
     if (m_.tilted()) {
         build_tilt_ramp();
         // STEM outputs at intermediate thicknesses apply the ramp to a copy of the batch
@@ -171,6 +165,7 @@ Engine::~Engine() {
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         d_detmat_.release_idle();
         d_ctf_.release_idle();
+        d_beams_psi_.release_idle();
         d_coh_.release_idle();
         d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -703,6 +698,26 @@ int Engine::tune_passes(int nprobe, ConfData& cd) {
     return chosen.emplace(key, bits).first->second;
 }
 
+// Probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
+// (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
+// aperture's pixel count (aperture test in the kernel's float arithmetic; no tilt offset in the
+// simulations' probes).
+float Engine::aperture_norm() const {
+    const LensF& L = m_.cond_lens;
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    double count = 0;
+    for (int ix = 0; ix < nx; ix++) {
+        float gx = (float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx;
+        for (int iy = 0; iy < ny; iy++) {
+            float gy = (float)((iy < m_.grid.nyh) ? iy : iy - ny) * m_.grid.dgy;
+            float g2 = gx * gx + gy * gy;
+            if ((L.g2_min <= g2) && (g2 < L.g2_max)) count += 1.0;
+        }
+    }
+    if (count <= 0) fail(MT_ERR_INVALID_ARG, "condenser aperture contains no Fourier pixel");
+    return (float)std::sqrt(1.0 / (double)(float)count);
+}
+
 ColArgs Engine::det_args() const {
     ColArgs ca{};
     ca.ny = m_.grid.ny;
@@ -811,11 +826,24 @@ void Engine::run_ew(ConfData& cd) {
     ca.g = gdev_;
     ca.n_det = 0;
     if (tune_) pipe_ = tune_passes(1, cd);
+    const bool conv = m_.is_convergent_wave();
+    if (conv) {
+        // the beams' probes, generated in Fourier space and brought to the hybrid layout, summed
+        const int nb = (int)m_.iw_x.size();
+        ColArgs cp = ca;
+        cp.nprobe = nb;
+        cp.in = nullptr;
+        cp.out = (nb > 1) ? d_beams_psi_.p : d_psi_.p;
+        cp.beam = d_beam_.p;
+        cp.probe = probe_params(cd.probe_c_c_10[0], cd.probe_nz_c10[0], false);
+        cols(COL_INVERSE | COL_STORE, cp);
+        if (nb > 1) launch_sum_waves(d_beams_psi_.p, nb, nxy, d_psi_.p, stream_);
+    }
     for (int k = 0; k <= cd.last_slice; k++) {
         ra.in = d_psi_.p;
         ra.out = d_psi_.p;
         ra.trans = d_trans_.p + (size_t)k * nxy;
-        rows(k == 0 ? ROW_FIRST_ONE : ROW_STEP, ra);
+        rows((k == 0 && !conv) ? ROW_FIRST_ONE : ROW_STEP, ra);
         ca.in = d_psi_.p;
         ca.out = d_psi_.p;
         ca.Px = cd.prop.p + (size_t)k * pl;
@@ -840,7 +868,7 @@ void Engine::run_ew(ConfData& cd) {
         cb.out = d_tmp_.p;
         cb.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
         cb.Py = cb.Px + nx;
-        if (m_.is_HRTEM()) {
+        if (m_.is_imaging()) {
             // image formation: transfer function per defocus point, inverse transform, |psi|^2
             // weighted (Microscope_Effects::operator(), src/microscope_effects.cuh:56-85)
             for (size_t j = 0; j < m_.obj_c10.size(); j++) {
@@ -873,9 +901,9 @@ void Engine::run_ew(ConfData& cd) {
         } else {
             cols(COL_LOAD | COL_PROP | COL_STORE, cb);
         }
-        // ED keeps only |psi_hat|^2 (add_scale_crop_shift_m2psi_tot_from_psi, wave_function.cuh:172-184)
+        // ED and CBED keep only |psi_hat|^2 (add_scale_crop_shift_m2psi_tot_from_psi, wave_function.cuh:172-184)
         launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
-                             m_.is_ED() ? nullptr : d_ew_psi_.p + (size_t)ithk * onxy * 2,
+                             m_.is_EW() ? d_ew_psi_.p + (size_t)ithk * onxy * 2 : nullptr,
                              sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
     }
     iter_ += 1;

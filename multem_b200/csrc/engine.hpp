@@ -159,6 +159,7 @@ class Engine {
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)
     DevBuf<float2> d_ctf_;           // HRTEM transfer functions, one [nx][ny] table per defocus point
+    DevBuf<float2> d_beams_psi_;     // convergent incident wave of several beams: one wave per beam
     DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
     DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
     ColArgs det_args() const;        // detector description for the column pass
@@ -176,6 +177,7 @@ class Engine {
     void prop_tables(float dz, float2* px, float2* py, bool output) const;
     ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
     void build_ctf_tables();
+    float aperture_norm() const;
     void check_cancel();
     ConfData* find_conf(int iconf);
 

@@ -649,10 +649,10 @@ Model build_model(const mt_input_multislice* in) {
     if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
     Model m;
     m.simulation_type = in->simulation_type;
-    if (!(m.is_STEM() || m.is_plane_sim()))
+    if (!(m.is_STEM() || m.is_wave_sim()))
         fail(MT_ERR_UNSUPPORTED, "simulation_type " + std::to_string(in->simulation_type) +
-                                     " is outside the plain multislice path (supported: 11 STEM, 31 ED, 32 HRTEM, "
-                                     "51 EWFS, 52 EWRS)");
+                                     " is outside the plain multislice path (supported: 11 STEM, 21 CBED, 22 CBEI, "
+                                     "31 ED, 32 HRTEM, 51 EWFS, 52 EWRS)");
     m.interaction_model = in->interaction_model;
     if (m.interaction_model != 1) fail(MT_ERR_UNSUPPORTED, "only interaction_model 1 (multislice) is implemented");
     m.potential_type = in->potential_type;
@@ -724,7 +724,7 @@ Model build_model(const mt_input_multislice* in) {
 
     // validate_incident_wave_type (src/input_multislice.cuh:438-448)
     int iw = in->iw_type;
-    if (iw == 4) iw = m.is_STEM() ? 2 : 1;
+    if (iw == 4) iw = (m.is_STEM() || m.is_CBED() || m.is_CBEI()) ? 2 : 1;
     m.iw_type = iw;
     if (m.is_STEM() && iw != 2) fail(MT_ERR_UNSUPPORTED, "STEM needs a convergent incident wave");
     if (m.is_EW() && iw == 3) {
@@ -733,6 +733,8 @@ Model build_model(const mt_input_multislice* in) {
         m.iw_psi.resize(2 * n);
         for (size_t i = 0; i < 2 * n; i++) m.iw_psi[i] = (float)in->iw_psi[i];
     }
+    if (m.is_wave_sim() && iw == 3)
+        fail(MT_ERR_UNSUPPORTED, "user-defined incident waves (iw_type 3) are implemented for mt_propagate only");
     for (int i = 0; i < in->n_iw_xy; i++) {
         m.iw_x.push_back((float)in->iw_x[i]);
         m.iw_y.push_back((float)in->iw_y[i]);
@@ -843,8 +845,8 @@ Model build_model(const mt_input_multislice* in) {
     m.lambda = lambda_f(m.E_0);
     snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
-    if ((m.is_ED() || m.is_HRTEM()) && m.pn_coh_contrib)
-        fail(MT_ERR_UNSUPPORTED, "ED/HRTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
+    if (m.is_wave_sim() && !m.is_EW() && m.pn_coh_contrib)
+        fail(MT_ERR_UNSUPPORTED, "CBED/CBEI/ED/HRTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 
@@ -891,13 +893,16 @@ Model build_model(const mt_input_multislice* in) {
     // illumination (src/input_multislice.cuh:672-676, 747-776): exit waves are coherent; without
     // full integration, or with spatial incoherence only, the condenser has one defocus point
     if (m.is_EW()) m.illumination_model = 1;
+    if ((m.is_CBED() || m.is_CBEI()) && m.illumination_model != 4) m.illumination_model = 1;
+    if ((m.is_CBED() || m.is_CBEI()) && m.illumination_model == 4)
+        fail(MT_ERR_UNSUPPORTED, "CBED/CBEI with full integration (source and defocus quadratures) is not implemented");
     if (is_zero_f(m.cond_lens.si_sigma)) m.temporal_spatial_incoh = 2;
     const bool full_integration = (m.illumination_model == 4);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.cond_lens.ti_npts = 1;
     m.cond_lens.set_input_data(m.E_0, m.grid);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.obj_lens.ti_npts = 1;
     m.obj_lens.set_input_data(m.E_0, m.grid);
-    if (m.is_HRTEM()) hrtem_ctf_points(m);
+    if (m.is_imaging()) hrtem_ctf_points(m);
     // Multislice::STEM_ISTEM integrates the defocus spread only under full integration, and not
     // in its coherent-contribution branch, which comes first (src/tem_simulation.cuh:115-176)
     if (m.is_STEM() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
@@ -927,7 +932,7 @@ Model build_model(const mt_input_multislice* in) {
     // an area given by the caller (not the "whole grid" default ix_0 == ix_e) that had to be
     // reordered or clipped
     const bool area_given = in->output_area_ix_0 != in->output_area_ix_e || in->output_area_iy_0 != in->output_area_iy_e;
-    if (m.is_plane_sim() && area_given &&
+    if (m.is_wave_sim() && area_given &&
         (m.out_ix_0 != in->output_area_ix_0 - 1 || m.out_ix_e != in->output_area_ix_e - 1 ||
          m.out_iy_0 != in->output_area_iy_0 - 1 || m.out_iy_e != in->output_area_iy_e - 1))
         m.clamps.push_back("output_area -> ix [" + std::to_string(m.out_ix_0 + 1) + ", " + std::to_string(m.out_ix_e + 1) +

@@ -157,12 +157,17 @@ struct Model {
     bool is_EWFS() const { return simulation_type == 51; }
     bool is_EWRS() const { return simulation_type == 52; }
     bool is_EW() const { return is_EWFS() || is_EWRS(); }
+    bool is_CBED() const { return simulation_type == 21; }
+    bool is_CBEI() const { return simulation_type == 22; }
     bool is_ED() const { return simulation_type == 31; }
     bool is_HRTEM() const { return simulation_type == 32; }
-    // one plane wave per configuration through the slice loop (EWFS, EWRS, ED, HRTEM)
-    bool is_plane_sim() const { return is_EW() || is_ED() || is_HRTEM(); }
+    // one incident wave (plane, or convergent beams summed) per configuration through the slice
+    // loop: EWFS, EWRS, ED, HRTEM, CBED, CBEI
+    bool is_wave_sim() const { return is_EW() || is_ED() || is_HRTEM() || is_CBED() || is_CBEI(); }
+    // image formation through the objective lens (Microscope_Effects): HRTEM, CBEI
+    bool is_imaging() const { return is_HRTEM() || is_CBEI(); }
     // outputs on the Fourier grid (is_grid_FS, src/input_multislice.cuh:367-372)
-    bool is_grid_FS() const { return is_EWFS() || is_ED(); }
+    bool is_grid_FS() const { return is_EWFS() || is_ED() || is_CBED(); }
     bool is_frozen_phonon() const { return pn_model == 3; }
     bool is_EW_SC() const { return is_EW() && is_frozen_phonon() && pn_single_conf; }
     bool is_plane_wave() const { return iw_type == 1; }

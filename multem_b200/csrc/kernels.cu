@@ -318,6 +318,23 @@ void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det
 }
 
 // =============================================================================================
+__global__ void sum_waves_kernel(const float2* __restrict__ src, int n, size_t nxy, float2* __restrict__ dst) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nxy; i += (size_t)gridDim.x * blockDim.x) {
+        float2 acc = src[i];
+        for (int j = 1; j < n; j++) {
+            const float2 v = src[(size_t)j * nxy + i];
+            acc = make_float2(__fadd_rn(acc.x, v.x), __fadd_rn(acc.y, v.y));
+        }
+        dst[i] = acc;
+    }
+}
+
+void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s) {
+    sum_waves_kernel<<<(unsigned)std::min<size_t>((nxy + 255) / 256, 148 * 8), 256, 0, s>>>(src, n, nxy, dst);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
 // One CTA per (thickness, scan position): detector sums of |psi_coh|^2 over the grid, per-thread
 // partials in FP64 reduced in a fixed order.
 __global__ void coh_detect_kernel(const float2* __restrict__ coh, int n_scan, ColArgs a, double* __restrict__ image) {

@@ -111,6 +111,9 @@ struct PctfArgs {
 void launch_ctf_table(const ProbeDev& lens, const GridDev& g, float2* out, cudaStream_t s);
 void launch_pctf_table(const PctfArgs& p, const GridDev& g, float2* out, cudaStream_t s);
 
+// dst = sum over j < n of src[j * nxy + i] (the beams of a convergent incident wave, in order).
+void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s);
+
 // STEM coherent images (Wave_Function::set_m2psi_coh, src/wave_function.cuh:189-209): for each
 // thickness and scan position, the detector sums of |psi_coh|^2 (weight 1) into
 // image_coh[(ithk*n_det + idet)*n_scan + iscan]; coh is [n_thk][n_scan][nx][ny] in FFT order.

@@ -218,3 +218,39 @@ def hrtem_fullint_si001():
     p.obj_lens_ti_npts = 7
     p.cond_lens_si_sigma = 0.0
     return p
+
+
+def _conv_si001(sim_type, beams):
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.simulation_type = sim_type
+    p.pn_nconf = 2
+    p.pn_seed = 5
+    p.iw_type = 2
+    p.iw_x = [b[0] for b in beams]
+    p.iw_y = [b[1] for b in beams]
+    p.cond_lens_c_10 = 30.0
+    p.cond_lens_c_30 = 0.001
+    p.cond_lens_outer_aper_ang = 15.0
+    return p
+
+
+def cbed_si001():
+    """CBED (simulation_type 21) of Si(001) on a 256^2 grid: a 15 mrad probe (defocus 30 A) off the
+    cell centre, |psi_hat|^2 averaged over two phonon configurations."""
+    return _conv_si001(21, [(11.2, 10.5)])
+
+
+def cbei_si001():
+    """CBEI (simulation_type 22): the cbed_si001 wave imaged through the objective's coherent
+    transfer function (defocus 40 A, 30 mrad aperture)."""
+    p = _conv_si001(22, [(11.2, 10.5)])
+    p.obj_lens_c_10 = 40.0
+    p.obj_lens_outer_aper_ang = 30.0
+    return p
+
+
+def ewrs_two_beams_si001():
+    """Exit wave (EWRS) of Si(001) under a convergent incident wave of two beams (the probes are
+    summed, Incident_Wave::operator())."""
+    return _conv_si001(52, [(8.0, 9.0), (13.5, 12.0)])

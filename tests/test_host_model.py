@@ -65,7 +65,8 @@ def test_configurations_differ_and_repeat():
 
 
 @pytest.mark.parametrize("field,value,status", [
-    ("simulation_type", 21, 6), ("potential_type", 5, 6), ("potential_slicing", 3, 6), ("nx", 0, 1),
+    ("simulation_type", 41, 6), ("simulation_type", 61, 6), ("potential_type", 5, 6), ("potential_slicing", 3, 6),
+    ("nx", 0, 1),
 ])
 def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
     from multem_b200 import capi
@@ -74,6 +75,26 @@ def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
     with pytest.raises(capi.MtError) as e:
         api.output_dims(p)
     assert e.value.status == status
+
+
+@pytest.mark.parametrize("sim,fields", [
+    (32, {"illumination_model": 3}),  # the reference's transmission-cross-coefficient branch computes nothing
+    (32, {"illumination_model": 4, "temporal_spatial_incoh": 1, "cond_lens_si_sigma": 0.01}),  # its spatial quadrature is empty
+    (21, {"illumination_model": 4}),  # CBED full integration (source and defocus quadratures)
+    (32, {"pn_coh_contrib": 1}),  # m2psi_coh
+    (52, {"iw_type": 3, "iw_psi": np.ones((64, 64), complex)}),  # user wave in the slice loop
+])
+def test_image_formation_limits_are_refused(sim, fields):
+    """Imaging and incident-wave variants outside what the engine implements fail with
+    MT_ERR_UNSUPPORTED at the engine's host-side set-up, before any GPU work."""
+    from multem_b200 import capi
+    p = specimens.hrtem_si001(nx=64, ny=64, na=2, nb=2, nc=2)
+    p.simulation_type = sim
+    for k, v in fields.items():
+        setattr(p, k, v)
+    with pytest.raises(capi.MtError) as e:
+        api.Engine(p)
+    assert e.value.status == 6
 
 
 def test_input_report_lists_silent_changes():
