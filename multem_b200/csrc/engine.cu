@@ -150,6 +150,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     graphs_ = env_int("MTB_GRAPH", 1) != 0;
     tune_ = pipe_ < 0;
     if (tune_) pipe_ = 3;
+    if (m_.is_wave_sim() && m_.is_user_wave()) build_user_wave();
     reset();
 }
 
@@ -166,6 +167,7 @@ Engine::~Engine() {
         d_detmat_.release_idle();
         d_ctf_.release_idle();
         d_beams_psi_.release_idle();
+        d_user_wave_.release_idle();
         d_coh_.release_idle();
         d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -698,6 +700,59 @@ int Engine::tune_passes(int nprobe, ConfData& cd) {
     return chosen.emplace(key, bits).first->second;
 }
 
+// User-defined incident wave (Incident_Wave, src/incident_wave.cuh:48-52 and 92-110): the wave
+// iw_psi, fft2-shifted, moved by (iw_x[0] - lx/2, iw_y[0] - ly/2) through the Fourier phase
+// exp(i (Rx gx + Ry gy)), Rx = exp_factor_Rx(iw_x[0]) (applied here as separable x and y factors
+// with the loop's 1/N), in the layout the first row step reads. Built once per engine: the wave is
+// the same for every configuration.
+void Engine::build_user_wave() {
+    const GridF& g = m_.grid;
+    const int nx = g.nx, ny = g.ny;
+    const size_t nxy = (size_t)nx * ny;
+    std::vector<float2> h(nxy);
+    for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny; iy++) {
+            const size_t src = (size_t)ix * ny + iy;
+            const size_t dst = (size_t)((ix + g.nxh) % nx) * ny + (iy + g.nyh) % ny;
+            h[dst] = make_float2(m_.iw_psi[2 * src], m_.iw_psi[2 * src + 1]);
+        }
+    const float Rx = g.exp_factor_Rx(m_.iw_x[0]), Ry = g.exp_factor_Ry(m_.iw_y[0]);
+    const double mnorm = (double)(1.0f / (float)(nx * ny));
+    std::vector<float2> tab((size_t)nx + ny);
+    for (int ix = 0; ix < nx; ix++) {
+        const double th = (double)(Rx * ((float)((ix < g.nxh) ? ix : ix - nx) * g.dgx));
+        tab[ix] = make_float2((float)(mnorm * std::cos(th)), (float)(mnorm * std::sin(th)));
+    }
+    for (int iy = 0; iy < ny; iy++) {
+        const double th = (double)(Ry * ((float)((iy < g.nyh) ? iy : iy - ny) * g.dgy));
+        tab[nx + iy] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+    std::vector<float2> ones(nxy, make_float2(1.0f, 0.0f));
+    DevBuf<float2> d_one, d_tab;
+    d_user_wave_.upload(h.data(), nxy, stream_);
+    d_one.upload(ones.data(), nxy, stream_);
+    d_tab.upload(tab.data(), tab.size(), stream_);
+    RowArgs ra{};
+    ra.in = d_user_wave_.p;
+    ra.out = d_user_wave_.p;
+    ra.trans = d_one.p;
+    ra.nx = nx;
+    ra.nprobe = 1;
+    ra.scale = 1.0f;
+    rows(ROW_FIRST_REAL, ra);
+    ColArgs ca{};
+    ca.in = d_user_wave_.p;
+    ca.out = d_user_wave_.p;
+    ca.ny = ny;
+    ca.nprobe = 1;
+    ca.g = gdev_;
+    ca.Px = d_tab.p;
+    ca.Py = d_tab.p + nx;
+    ca.det_w = col_det_width(nx);
+    cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca);
+    synchronize();
+}
+
 // Probe normalisation: the reference scales each probe by sqrt(1/sum|psi_hat|^2)
 // (src/gpu_fcns.cuh:1612-1624); |exp(i chi)| = 1 inside the aperture, so the sum is the
 // aperture's pixel count (aperture test in the kernel's float arithmetic; no tilt offset in the
@@ -839,11 +894,12 @@ void Engine::run_ew(ConfData& cd) {
         cols(COL_INVERSE | COL_STORE, cp);
         if (nb > 1) launch_sum_waves(d_beams_psi_.p, nb, nxy, d_psi_.p, stream_);
     }
+    const bool user = m_.is_user_wave();
     for (int k = 0; k <= cd.last_slice; k++) {
-        ra.in = d_psi_.p;
+        ra.in = (k == 0 && user) ? d_user_wave_.p : d_psi_.p;
         ra.out = d_psi_.p;
         ra.trans = d_trans_.p + (size_t)k * nxy;
-        rows((k == 0 && !conv) ? ROW_FIRST_ONE : ROW_STEP, ra);
+        rows((k == 0 && !conv && !user) ? ROW_FIRST_ONE : ROW_STEP, ra);
         ca.in = d_psi_.p;
         ca.out = d_psi_.p;
         ca.Px = cd.prop.p + (size_t)k * pl;

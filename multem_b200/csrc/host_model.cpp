@@ -727,14 +727,14 @@ Model build_model(const mt_input_multislice* in) {
     if (iw == 4) iw = (m.is_STEM() || m.is_CBED() || m.is_CBEI()) ? 2 : 1;
     m.iw_type = iw;
     if (m.is_STEM() && iw != 2) fail(MT_ERR_UNSUPPORTED, "STEM needs a convergent incident wave");
-    if (m.is_EW() && iw == 3) {
+    if (m.is_wave_sim() && iw == 3) {
         if (!in->iw_psi) fail(MT_ERR_INVALID_ARG, "iw_type 3 needs iw_psi");
         size_t n = (size_t)in->nx * in->ny;
         m.iw_psi.resize(2 * n);
         for (size_t i = 0; i < 2 * n; i++) m.iw_psi[i] = (float)in->iw_psi[i];
     }
-    if (m.is_wave_sim() && iw == 3)
-        fail(MT_ERR_UNSUPPORTED, "user-defined incident waves (iw_type 3) are implemented for mt_propagate only");
+    if (m.is_wave_sim() && iw == 3 && in->n_iw_xy < 1)
+        fail(MT_ERR_INVALID_ARG, "a user-defined incident wave needs its position in iw_x/iw_y");
     for (int i = 0; i < in->n_iw_xy; i++) {
         m.iw_x.push_back((float)in->iw_x[i]);
         m.iw_y.push_back((float)in->iw_y[i]);

@@ -254,3 +254,29 @@ def ewrs_two_beams_si001():
     """Exit wave (EWRS) of Si(001) under a convergent incident wave of two beams (the probes are
     summed, Incident_Wave::operator())."""
     return _conv_si001(52, [(8.0, 9.0), (13.5, 12.0)])
+
+
+def ewrs_user_wave_si001():
+    """Exit wave (EWRS) of Si(001) on a 256^2 grid under a user-defined incident wave (iw_type 3): a
+    seeded smooth complex wave, placed off the cell centre by iw_x/iw_y; two phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.pn_nconf = 2
+    p.pn_seed = 6
+    p.iw_type = 3
+    rng = np.random.default_rng(31)
+    y, x = np.meshgrid(np.arange(p.ny) * p.spec_ly / p.ny, np.arange(p.nx) * p.spec_lx / p.nx, indexing="ij")
+    env = np.exp(-((x - 0.5 * p.spec_lx) ** 2 + (y - 0.5 * p.spec_ly) ** 2) / (2 * 5.0 ** 2))
+    p.iw_psi = env * np.exp(1j * 0.4 * rng.standard_normal((p.ny, p.nx)))
+    p.iw_x, p.iw_y = [0.5 * p.spec_lx + 1.7], [0.5 * p.spec_ly - 2.3]
+    return p
+
+
+def hrtem_user_wave_si001():
+    """ewrs_user_wave_si001 imaged through the objective's coherent transfer function (HRTEM)."""
+    p = ewrs_user_wave_si001()
+    p.simulation_type = 32
+    p.illumination_model = 1
+    p.obj_lens_c_10 = 40.0
+    p.obj_lens_outer_aper_ang = 25.0
+    return p

@@ -82,7 +82,6 @@ def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
     (32, {"illumination_model": 4, "temporal_spatial_incoh": 1, "cond_lens_si_sigma": 0.01}),  # its spatial quadrature is empty
     (21, {"illumination_model": 4}),  # CBED full integration (source and defocus quadratures)
     (32, {"pn_coh_contrib": 1}),  # m2psi_coh
-    (52, {"iw_type": 3, "iw_psi": np.ones((64, 64), complex)}),  # user wave in the slice loop
 ])
 def test_image_formation_limits_are_refused(sim, fields):
     """Imaging and incident-wave variants outside what the engine implements fail with
