@@ -706,8 +706,6 @@ Model build_model(const mt_input_multislice* in) {
         fail(MT_ERR_INVALID_ARG, "spec_amorp_z_0, spec_amorp_z_e and spec_amorp_dz must hold spec_amorp_n values");
     for (int i = 0; i < in->spec_amorp_n; i++)
         A.amorp.push_back({(float)in->spec_amorp_z_0[i], (float)in->spec_amorp_z_e[i], (float)in->spec_amorp_dz[i], 0, 0});
-    if (!is_zero_f((float)((float)in->spec_rot_theta * kDeg)))
-        fail(MT_ERR_UNSUPPORTED, "specimen rotation is not implemented");
     m.thick_type = in->thick_type;
     if (m.thick_type < 1 || m.thick_type > 3) fail(MT_ERR_INVALID_ARG, "thick_type must be 1, 2 or 3");
     if (m.thick_type != 1) {
@@ -849,6 +847,47 @@ Model build_model(const mt_input_multislice* in) {
         fail(MT_ERR_UNSUPPORTED, "CBED/CBEI/ED/HRTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
+
+    // specimen rotation (input_multislice.cuh:707-722): whole-specimen thickness, the atoms rotated
+    // by spec_rot_theta about the unit axis u0 through the geometric centre (mean position) or a
+    // user point (rotate_atoms, src/atomic_data_mt.hpp:61-74; get_rotation_matrix,
+    // src/cgpu_fcns.cuh:185-205; r3d::rotate, src/lin_alg_def.cuh:355-360), all in float
+    const float rot_theta = (float)((float)in->spec_rot_theta * kDeg);
+    if (!is_zero_f(rot_theta)) {
+        m.thick_type = 1;
+        float ux = (float)in->spec_rot_u0[0], uy = (float)in->spec_rot_u0[1], uz = (float)in->spec_rot_u0[2];
+        const float un = std::sqrt(ux * ux + uy * uy + uz * uz);
+        if (!(un > 0)) fail(MT_ERR_INVALID_ARG, "spec_rot_u0 must be a non-zero vector");
+        ux /= un;
+        uy /= un;
+        uz /= un;
+        float px = (float)in->spec_rot_center_p[0], py = (float)in->spec_rot_center_p[1], pz = (float)in->spec_rot_center_p[2];
+        if (in->spec_rot_center_type == 1) {
+            float sx = 0, sy = 0, sz = 0;
+            for (size_t i = 0; i < A.size(); i++) {
+                sx += A.x[i];
+                sy += A.y[i];
+                sz += A.z[i];
+            }
+            px = sx / (float)A.size();
+            py = sy / (float)A.size();
+            pz = sz / (float)A.size();
+        }
+        float alpha = 1.0f - std::cos(rot_theta);
+        alpha = is_zero_f(alpha) ? 0.0f : alpha;
+        float beta = std::sin(rot_theta);
+        beta = is_zero_f(beta) ? 0.0f : beta;
+        const float R[9] = {1.0f + alpha * (ux * ux - 1), uy * ux * alpha + uz * beta, uz * ux * alpha - uy * beta,
+                            ux * uy * alpha - uz * beta, 1.0f + alpha * (uy * uy - 1), uz * uy * alpha + ux * beta,
+                            ux * uz * alpha + uy * beta, uy * uz * alpha - ux * beta, 1.0f + alpha * (uz * uz - 1)};
+        for (size_t i = 0; i < A.size(); i++) {
+            const float x = A.x[i] - px, y = A.y[i] - py, z = A.z[i] - pz;
+            A.x[i] = (R[0] * x + R[3] * y + R[6] * z) + px;
+            A.y[i] = (R[1] * x + R[4] * y + R[7] * z) + py;
+            A.z[i] = (R[2] * x + R[5] * y + R[8] * z) + pz;
+        }
+        A.statistic(nullptr);
+    }
 
     // Slicing::match_thickness (src/slicing.hpp:53-71)
     if (m.thick_type == 1) {

@@ -280,3 +280,29 @@ def hrtem_user_wave_si001():
     p.obj_lens_c_10 = 40.0
     p.obj_lens_outer_aper_ang = 25.0
     return p
+
+
+def ew_rot_si001():
+    """Exit wave (EWRS) of Si(001), 256^2 grid, 4 x 4 x 4 cells rotated by 4 deg about (1, 0.5, 0)
+    through the geometric centre (spec_rot_*), dz_Proj slices of 1.36 A (with plane slicing the
+    rotated atoms fall into a single plane and the reference switches to its phase-object mode)."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.potential_slicing = 2
+    p.spec_dz = 1.36
+    p.spec_rot_theta = 4.0
+    p.spec_rot_u0 = (1.0, 0.5, 0.0)
+    p.spec_rot_center_type = 1
+    return p
+
+
+def stem_rot_srtio3():
+    """STEM ADF through SrTiO3(001) rotated by 10 deg about z through a user point (7, 8, 5), 256^2
+    grid, 3 x 3 probes, two phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=12)
+    p.spec_rot_theta = 10.0
+    p.spec_rot_u0 = (0.0, 0.0, 1.0)
+    p.spec_rot_center_type = 2
+    p.spec_rot_center_p = (7.0, 8.0, 5.0)
+    return p

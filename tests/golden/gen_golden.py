@@ -24,7 +24,8 @@ from multem_b200 import specimens  # noqa: E402
 from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case, stem_1024, stem_384,  # noqa: E402
                    stem_tilt_au001, ew_tilt_si001, ewfs_tilt_si001, stem_incoh_srtio3, stem_matrix_srtio3,
                    stem_coh_srtio3, ed_si001, hrtem_coherent_si001, hrtem_pctf_si001, hrtem_fullint_si001,
-                   cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001)
+                   cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001,
+                   ew_rot_si001, stem_rot_srtio3)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -58,7 +59,24 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("ed_si001", ed_si001), ("hrtem_coherent_si001", hrtem_coherent_si001),
              ("hrtem_pctf_si001", hrtem_pctf_si001), ("hrtem_fullint_si001", hrtem_fullint_si001),
              ("cbed_si001", cbed_si001), ("cbei_si001", cbei_si001), ("ewrs_two_beams_si001", ewrs_two_beams_si001),
-             ("ewrs_user_wave_si001", ewrs_user_wave_si001), ("hrtem_user_wave_si001", hrtem_user_wave_si001))
+             ("ewrs_user_wave_si001", ewrs_user_wave_si001), ("hrtem_user_wave_si001", hrtem_user_wave_si001),
+             ("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3))
+
+SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3))
+
+
+def specimen_fixtures(rec, names=None):
+    """Displaced atoms and slicing of configurations 1 and 2 from the reference (SPECIMENS)."""
+    for name, fn in SPECIMENS:
+        if names is not None and name not in names:
+            continue
+        p = fn()
+        for iconf in (1, 2):
+            if iconf > p.pn_nconf:
+                continue
+            sp = R.specimen(p, iconf)
+            for k in ("Z", "xyz", "z_0", "z_e", "iatom_0", "iatom_e", "ithk"):
+                rec[f"{name}_c{iconf}_{k}"] = sp[k]
 
 
 def full_runs(rec, names=None):
@@ -81,6 +99,7 @@ def add_only(names):
     old = np.load(path)
     rec = {k: old[k] for k in old.files}
     full_runs(rec, names)
+    specimen_fixtures(rec, names)
     np.savez_compressed(path, **rec)
     print("wrote", path, len(rec), "arrays")
 
@@ -138,6 +157,7 @@ def main():
                     rec[f"{name}_z{int(z)}_s{space}_p{prec}"] = r.astype(np.complex64) if prec == 1 else r
     # full runs on a radix-3 grid, a 1024^2 grid, an amorphous layer and a tilted beam
     full_runs(rec)
+    specimen_fixtures(rec)
     # full runs
     for name, fn in (("stem_small", stem_small), ("stem_thick", stem_thick), ("ew_small", ew_small),
                      ("ew_config1", ew_config1)):

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from multem_b200 import api, specimens
-from cases import amorph_au110
+from cases import amorph_au110, ew_rot_si001, stem_rot_srtio3
 
 
 def cases():
@@ -21,10 +21,13 @@ def cases():
         "ew_small": specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2),
         "ew_config1": specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=8),
         "amorph_au110": amorph_au110(),
+        "ew_rot_si001": ew_rot_si001(),
+        "stem_rot_srtio3": stem_rot_srtio3(),
     }
 
 
-@pytest.mark.parametrize("name", ["stem_small", "stem_thick", "ew_small", "ew_config1", "amorph_au110"])
+@pytest.mark.parametrize("name", ["stem_small", "stem_thick", "ew_small", "ew_config1", "amorph_au110", "ew_rot_si001",
+                                  "stem_rot_srtio3"])
 @pytest.mark.parametrize("iconf", [1, 2])
 def test_displaced_atoms_and_slices_bit_exact(golden, name, iconf):
     p = cases()[name]
