@@ -131,6 +131,10 @@ typedef struct mt_input_multislice {
 
     double E_0;                  /* keV */
     double theta, phi;           /* degrees */
+    /* precession (PED, simulation_type 41) and hollow-cone illumination (HCTEM, 42): beam tilt in
+     * degrees and number of azimuthal rotations (ilc_multem.cu:338-347) */
+    double ped_theta, hci_theta;
+    int ped_nrot, hci_nrot;
 
     int illumination_model;
     int temporal_spatial_incoh;

@@ -63,6 +63,7 @@ class MtInputMultislice(C.Structure):
         ("nx", c_int), ("ny", c_int), ("bwl", c_int),
         ("iw_type", c_int), ("iw_psi", P_double), ("iw_x", P_double), ("iw_y", P_double), ("n_iw_xy", c_int),
         ("E_0", c_double), ("theta", c_double), ("phi", c_double),
+        ("ped_theta", c_double), ("hci_theta", c_double), ("ped_nrot", c_int), ("hci_nrot", c_int),
         ("illumination_model", c_int), ("temporal_spatial_incoh", c_int),
         ("cond_lens", MtLens), ("obj_lens", MtLens),
         ("scanning_type", c_int), ("scanning_periodic", c_int), ("scanning_square_pxs", c_int),

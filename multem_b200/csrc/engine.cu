@@ -122,7 +122,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         if (m_.is_EW()) d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
-        niter_ = m_.number_conf();
+        niter_ = m_.number_conf() * m_.nrot;
         if (m_.is_convergent_wave()) {
             // convergent beams at iw_x/iw_y, summed (Incident_Wave::operator(), src/incident_wave.cuh:72-90)
             const int nb = (int)m_.iw_x.size();
@@ -234,25 +234,19 @@ void Engine::build_types() {
 // (phase_multiplication :77-94, exp_r_factor_2d src/cgpu_fcns.cuh:1869-1878, unscaled), with
 // Rx = Rx_shift(ix) - Rx_c and Rx_c = int(lx/2) (Grid_2d::Rx_c returns an int, src/types.cuh:2284).
 // Applied as a row step whose "transmission" is this table; the table carries the row pass's 1/ny
-// so the result is in the layout the output propagator tables expect. Stored [ix][iy].
+// so the result is in the layout the output propagator tables expect. Stored [ix][iy], one table
+// per beam rotation that needs one (launch_tilt_ramp).
 void Engine::build_tilt_ramp() {
     const GridF& g = m_.grid;
-    const int nx = g.nx, ny = g.ny;
-    const float gx = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gx_0()));
-    const float gy = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gy_0()));
+    const size_t nxy = (size_t)g.nx * g.ny;
+    d_ramp_.alloc(nxy * m_.nrot);
     const float rxc = (float)(int)(g.Rx_0 + 0.5f * g.lx), ryc = (float)(int)(g.Ry_0 + 0.5f * g.ly);
-    const double s = 1.0 / (double)ny;
-    std::vector<float2> ramp((size_t)nx * ny);
-    for (int ix = 0; ix < nx; ix++) {
-        const float rx = (float)((ix < g.nxh) ? ix + g.nxh : ix - g.nxh) * g.dRx + g.Rx_0 - rxc;
-        for (int iy = 0; iy < ny; iy++) {
-            const float ry = (float)((iy < g.nyh) ? iy + g.nyh : iy - g.nyh) * g.dRy + g.Ry_0 - ryc;
-            volatile float a = gx * rx, b = gy * ry;  // two roundings and a sum, no fused multiply-add
-            const double th = (double)(float)(a + b);
-            ramp[(size_t)ix * ny + iy] = make_float2((float)(std::cos(th) * s), (float)(std::sin(th) * s));
-        }
+    for (int r = 0; r < m_.nrot; r++) {
+        if (!m_.ramp_needed(r)) continue;
+        const float gx = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gx_0(r)));
+        const float gy = (float)(2.0 * 3.141592653589793238463 * (double)(-m_.gy_0(r)));
+        launch_tilt_ramp(gdev_, gx, gy, rxc, ryc, d_ramp_.p + r * nxy, stream_);
     }
-    d_ramp_.upload(ramp.data(), ramp.size(), stream_);
 }
 
 // HRTEM: the objective's transfer function per defocus point (Microscope_Effects, see
@@ -314,7 +308,7 @@ void Engine::build_ctf_tables() {
 // Fresnel propagator factors for distance dz, separable in x and y:
 // P(ix, iy) = exp(i*w*(gx^2 + gy^2))/N, w = -pi*lambda*dz (propagate, src/cgpu_fcns.cuh:1837-1845;
 // get_propagator_factor, src/input_multislice.cuh:909-912). Phases in double, stored as float.
-void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output) {
+void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output, int irot) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const double w = (double)m_.propagator_factor(dz);
     // Between passes the wave is kept as F_y(psi)/ny (the unnormalised row transforms of one step
@@ -322,7 +316,7 @@ void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output)
     // the output tables (back-propagation to the zero-defocus plane) carry 1/nx so that the
     // materialised wave is psi (or FFT2(psi)*P) itself.
     const double m = output ? 1.0 / (double)nx : (double)(1.0f / (float)(nx * ny));
-    const double gx0 = m_.gx_0(), gy0 = m_.gy_0();
+    const double gx0 = m_.gx_0(irot), gy0 = m_.gy_0(irot);
     for (int ix = 0; ix < nx; ix++) {
         double gx = (double)((float)((ix < m_.grid.nxh) ? ix : ix - nx) * m_.grid.dgx) - gx0;
         double th = w * gx * gx;
@@ -335,7 +329,9 @@ void prop_tables(const Model& m_, float dz, float2* px, float2* py, bool output)
     }
 }
 
-void Engine::prop_tables(float dz, float2* px, float2* py, bool output) const { mtb::prop_tables(m_, dz, px, py, output); }
+void Engine::prop_tables(float dz, float2* px, float2* py, bool output, int irot) const {
+    mtb::prop_tables(m_, dz, px, py, output, irot);
+}
 
 // gxu/gyu: the beam-tilt offset of exp_i_chi (src/cgpu_fcns.cuh:1950-1980). The simulations build
 // their probes with gxu = gyu = 0 (Wave_Function::set_incident_wave, src/wave_function.cuh:300-307);
@@ -398,10 +394,14 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     cd.thick_z_back_prop.resize(TH.size());
     for (size_t t = 0; t < TH.size(); t++) cd.thick_z_back_prop[t] = TH[t].z_back_prop;
     const size_t pl = (size_t)nx + ny;
-    std::vector<float2> prop((S.size() + TH.size()) * pl);
-    for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), &prop[k * pl], &prop[k * pl + nx], false);
-    for (size_t t = 0; t < TH.size(); t++)
-        prop_tables(TH[t].z_back_prop, &prop[(S.size() + t) * pl], &prop[(S.size() + t) * pl + nx], true);
+    const size_t rb = (S.size() + TH.size()) * pl;  // one block per beam rotation
+    std::vector<float2> prop(rb * m_.nrot);
+    for (int r = 0; r < m_.nrot; r++) {
+        float2* q = prop.data() + r * rb;
+        for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), q + k * pl, q + k * pl + nx, false, r);
+        for (size_t t = 0; t < TH.size(); t++)
+            prop_tables(TH[t].z_back_prop, q + (S.size() + t) * pl, q + (S.size() + t) * pl + nx, true, r);
+    }
     // incident-wave defocus relative to the first slice (Incident_Wave::operator(),
     // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0)), with c_10 moved
     // by each defocus-spread point (cond_lens.set_defocus(c_10_0 + qt.x), src/tem_simulation.cuh:155-157)
@@ -882,6 +882,13 @@ void Engine::run_ew(ConfData& cd) {
     ca.n_det = 0;
     if (tune_) pipe_ = tune_passes(1, cd);
     const bool conv = m_.is_convergent_wave();
+    const bool user = m_.is_user_wave();
+    const size_t rblock = (size_t)(cd.n_slice + (int)cd.thick_z_back_prop.size()) * pl;
+    // beam rotations of PED / HCTEM (Multislice::PED_HCTEM, src/tem_simulation.cuh:274-300); one
+    // pass otherwise
+    for (int r = 0; r < m_.nrot; r++) {
+    const float2* prop = cd.prop.p + (size_t)r * rblock;
+    const float2* ramp = m_.ramp_needed(r) ? d_ramp_.p + (size_t)r * nxy : nullptr;
     if (conv) {
         // the beams' probes, generated in Fourier space and brought to the hybrid layout, summed
         const int nb = (int)m_.iw_x.size();
@@ -894,7 +901,6 @@ void Engine::run_ew(ConfData& cd) {
         cols(COL_INVERSE | COL_STORE, cp);
         if (nb > 1) launch_sum_waves(d_beams_psi_.p, nb, nxy, d_psi_.p, stream_);
     }
-    const bool user = m_.is_user_wave();
     for (int k = 0; k <= cd.last_slice; k++) {
         ra.in = (k == 0 && user) ? d_user_wave_.p : d_psi_.p;
         ra.out = d_psi_.p;
@@ -902,7 +908,7 @@ void Engine::run_ew(ConfData& cd) {
         rows((k == 0 && !conv && !user) ? ROW_FIRST_ONE : ROW_STEP, ra);
         ca.in = d_psi_.p;
         ca.out = d_psi_.p;
-        ca.Px = cd.prop.p + (size_t)k * pl;
+        ca.Px = prop + (size_t)k * pl;
         ca.Py = ca.Px + nx;
         cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca);
         const int ithk = cd.slice_ithk[k];
@@ -910,19 +916,19 @@ void Engine::run_ew(ConfData& cd) {
         // wave at this thickness (Wave_Function::get_psi, src/wave_function.cuh:96-105)
         const float zbp = cd.thick_z_back_prop[ithk];
         float2* src = d_psi_.p;
-        if (d_ramp_.p) {
+        if (ramp) {
             // tilted beam: phase ramp before the output propagation
             RowArgs rr = ra;
             rr.in = d_psi_.p;
             rr.out = d_tmp_.p;
-            rr.trans = d_ramp_.p;
+            rr.trans = ramp;
             rows(ROW_STEP, rr);
             src = d_tmp_.p;
         }
         ColArgs cb = ca;
         cb.in = src;
         cb.out = d_tmp_.p;
-        cb.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
+        cb.Px = prop + (size_t)(cd.n_slice + ithk) * pl;
         cb.Py = cb.Px + nx;
         if (m_.is_imaging()) {
             // image formation: transfer function per defocus point, inverse transform, |psi|^2
@@ -963,6 +969,7 @@ void Engine::run_ew(ConfData& cd) {
                              sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
     }
     iter_ += 1;
+    }
     check_cancel();
 }
 

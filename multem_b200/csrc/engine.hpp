@@ -54,7 +54,7 @@ struct DevBuf {
 
 GridDev grid_dev(const GridF& g);
 // Fresnel propagator factors Px[nx], Py[ny] of distance dz (see engine.cu).
-void prop_tables(const Model& m, float dz, float2* px, float2* py, bool output);
+void prop_tables(const Model& m, float dz, float2* px, float2* py, bool output, int irot = 0);
 // mt_propagate: the user wave in->iw_psi propagated by z (space 1 real, 2 reciprocal).
 void propagate_wave(const mt_system_conf* conf, const mt_input_multislice* in, int space, double z, double* psi_out);
 
@@ -69,7 +69,7 @@ struct ConfData {
     std::vector<int> probe_nz_c10;
     DevBuf<float4> atoms;
     DevBuf<int2> ranges;
-    DevBuf<float2> prop;            // per slice: Px[nx] then Py[ny]
+    DevBuf<float2> prop;            // per rotation, per slice then per thickness: Px[nx] then Py[ny]
     void release_idle() {
         atoms.release_idle();
         ranges.release_idle();
@@ -156,7 +156,7 @@ class Engine {
     DevBuf<double> d_ew_psi_;        // [n_thk][out_nxy][2]
     DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
-    DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny (else empty)
+    DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny per rotation (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)
     DevBuf<float2> d_ctf_;           // HRTEM transfer functions, one [nx][ny] table per defocus point
     DevBuf<float2> d_beams_psi_;     // convergent incident wave of several beams: one wave per beam
@@ -175,7 +175,7 @@ class Engine {
     int tune_passes(int nprobe, ConfData& cd);
     void run_stem(ConfData& cd);
     void run_ew(ConfData& cd);
-    void prop_tables(float dz, float2* px, float2* py, bool output) const;
+    void prop_tables(float dz, float2* px, float2* py, bool output, int irot = 0) const;
     ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
     void build_ctf_tables();
     float aperture_norm() const;

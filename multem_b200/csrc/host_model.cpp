@@ -597,18 +597,31 @@ void hrtem_ctf_points(Model& m) {
 }
 
 // isZero(gx_0, gy_0) of Wave_Function::phase_multiplication (src/wave_function.cuh:79)
-bool Model::tilted() const { return !(is_zero_f(gx_0()) && is_zero_f(gy_0())); }
+bool Model::tilted() const {
+    for (int r = 0; r < nrot; r++)
+        if (ramp_needed(r)) return true;
+    return false;
+}
 
 float Model::gx_0() const { return (float)(std::sin(theta) * std::cos(phi) / lambda); }
 float Model::gy_0() const { return (float)(std::sin(theta) * std::sin(phi) / lambda); }
+float Model::rot_phi(int irot) const {
+    if (!(is_PED() || is_HCTEM())) return phi;
+    return (irot == 0) ? 0.0f : (float)((2.0 * 3.141592653589793238463 * (double)(float)irot) / (double)(float)nrot);
+}
+float Model::gx_0(int irot) const { return (float)(std::sin(theta) * std::cos(rot_phi(irot)) / lambda); }
+float Model::gy_0(int irot) const { return (float)(std::sin(theta) * std::sin(rot_phi(irot)) / lambda); }
+// Wave_Function::phase_multiplication is skipped for PED (dp_Shift) and for no tilt
+bool Model::ramp_needed(int irot) const { return !dp_shift && !(is_zero_f(gx_0(irot)) && is_zero_f(gy_0(irot))); }
 // Input_Multislice::Vr_factor (src/input_multislice.cuh:914-917)
 float Model::Vr_factor() const { return (float)mul_sign * vr_factor_f(E_0, theta); }
 // Input_Multislice::get_propagator_factor (src/input_multislice.cuh:909-912)
 float Model::propagator_factor(float z) const { return (float)(-mul_sign * kPi * lambda * z); }
 // Input_Multislice::get_phonon_rot_weight (src/input_multislice.cuh:897-901)
+// Input_Multislice::get_phonon_rot_weight (src/input_multislice.cuh:897-901)
 float Model::phonon_weight() const {
     int nconf = (!is_frozen_phonon() || pn_single_conf) ? 1 : pn_nconf;
-    return 1.0f / (float)nconf;
+    return 1.0f / (float)(nconf * nrot);
 }
 
 // read_input_multislice + validate_parameters (mex_files_multem/ilc_multem.cu:38-379,
@@ -652,7 +665,7 @@ Model build_model(const mt_input_multislice* in) {
     if (!(m.is_STEM() || m.is_wave_sim()))
         fail(MT_ERR_UNSUPPORTED, "simulation_type " + std::to_string(in->simulation_type) +
                                      " is outside the plain multislice path (supported: 11 STEM, 21 CBED, 22 CBEI, "
-                                     "31 ED, 32 HRTEM, 51 EWFS, 52 EWRS)");
+                                     "31 ED, 32 HRTEM, 41 PED, 42 HCTEM, 51 EWFS, 52 EWRS)");
     m.interaction_model = in->interaction_model;
     if (m.interaction_model != 1) fail(MT_ERR_UNSUPPORTED, "only interaction_model 1 (multislice) is implemented");
     m.potential_type = in->potential_type;
@@ -741,6 +754,12 @@ Model build_model(const mt_input_multislice* in) {
     m.E_0 = (float)in->E_0;
     m.theta = (float)((float)in->theta * kDeg);
     m.phi = (float)((float)in->phi * kDeg);
+    // ilc_multem.cu:338-347 and validate_parameters (src/input_multislice.cuh:655-660)
+    if (m.is_PED() || m.is_HCTEM()) {
+        m.theta = (float)((float)(m.is_PED() ? in->ped_theta : in->hci_theta) * kDeg);
+        m.nrot = std::max(1, (int)(float)(m.is_PED() ? in->ped_nrot : in->hci_nrot));
+        m.dp_shift = m.is_PED();
+    }
 
     m.cond_lens.from_input(in->cond_lens);
     m.cond_lens.set_input_data(m.E_0, m.grid);

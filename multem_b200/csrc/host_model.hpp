@@ -158,16 +158,20 @@ struct Model {
     bool is_EWRS() const { return simulation_type == 52; }
     bool is_EW() const { return is_EWFS() || is_EWRS(); }
     bool is_CBED() const { return simulation_type == 21; }
+    bool is_PED() const { return simulation_type == 41; }
+    bool is_HCTEM() const { return simulation_type == 42; }
     bool is_CBEI() const { return simulation_type == 22; }
     bool is_ED() const { return simulation_type == 31; }
     bool is_HRTEM() const { return simulation_type == 32; }
-    // one incident wave (plane, or convergent beams summed) per configuration through the slice
-    // loop: EWFS, EWRS, ED, HRTEM, CBED, CBEI
-    bool is_wave_sim() const { return is_EW() || is_ED() || is_HRTEM() || is_CBED() || is_CBEI(); }
-    // image formation through the objective lens (Microscope_Effects): HRTEM, CBEI
-    bool is_imaging() const { return is_HRTEM() || is_CBEI(); }
+    // one incident wave (plane, convergent beams summed, or user-defined) per configuration, and
+    // per beam rotation for PED / HCTEM, through the slice loop
+    bool is_wave_sim() const {
+        return is_EW() || is_ED() || is_HRTEM() || is_CBED() || is_CBEI() || is_PED() || is_HCTEM();
+    }
+    // image formation through the objective lens (Microscope_Effects): HRTEM, CBEI, HCTEM
+    bool is_imaging() const { return is_HRTEM() || is_CBEI() || is_HCTEM(); }
     // outputs on the Fourier grid (is_grid_FS, src/input_multislice.cuh:367-372)
-    bool is_grid_FS() const { return is_EWFS() || is_ED() || is_CBED(); }
+    bool is_grid_FS() const { return is_EWFS() || is_ED() || is_CBED() || is_PED(); }
     bool is_frozen_phonon() const { return pn_model == 3; }
     bool is_EW_SC() const { return is_EW() && is_frozen_phonon() && pn_single_conf; }
     bool is_plane_wave() const { return iw_type == 1; }
@@ -178,6 +182,14 @@ struct Model {
     float gx_0() const;
     float gy_0() const;
     bool tilted() const;
+    // beam rotations of PED / HCTEM (nrot > 1): azimuth of rotation irot (Input_Multislice::set_phi,
+    // src/input_multislice.cuh:903-906), and the tilt offsets there
+    int nrot = 1;
+    bool dp_shift = false;  // PED: the diffraction pattern is not shifted back (no output phase ramp)
+    float rot_phi(int irot) const;
+    float gx_0(int irot) const;
+    float gy_0(int irot) const;
+    bool ramp_needed(int irot) const;
     float Vr_factor() const;
     float propagator_factor(float z) const;
     float phonon_weight() const;

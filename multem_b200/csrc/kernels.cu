@@ -318,6 +318,24 @@ void launch_det_reduce(const double* partial, int nprobe, int n_tiles, int n_det
 }
 
 // =============================================================================================
+__global__ void tilt_ramp_kernel(GridDev g, float gx, float gy, float rxc, float ryc, float2* __restrict__ out) {
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
+    if (iy >= g.ny) return;
+    const float rx = __fsub_rn(__fadd_rn(__fmul_rn((float)((ix < g.nxh) ? ix + g.nxh : ix - g.nxh), g.dRx), g.Rx_0), rxc);
+    const float ry = __fsub_rn(__fadd_rn(__fmul_rn((float)((iy < g.nyh) ? iy + g.nyh : iy - g.nyh), g.dRy), g.Ry_0), ryc);
+    const double th = (double)__fadd_rn(__fmul_rn(gx, rx), __fmul_rn(gy, ry));
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    const double s = 1.0 / (double)g.ny;
+    out[(size_t)ix * g.ny + iy] = make_float2((float)(cs * s), (float)(sn * s));
+}
+
+void launch_tilt_ramp(const GridDev& g, float gx, float gy, float rxc, float ryc, float2* out, cudaStream_t s) {
+    tilt_ramp_kernel<<<dim3((unsigned)((g.ny + 127) / 128), (unsigned)g.nx), 128, 0, s>>>(g, gx, gy, rxc, ryc, out);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
 __global__ void sum_waves_kernel(const float2* __restrict__ src, int n, size_t nxy, float2* __restrict__ dst) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nxy; i += (size_t)gridDim.x * blockDim.x) {
         float2 acc = src[i];

@@ -111,6 +111,10 @@ struct PctfArgs {
 void launch_ctf_table(const ProbeDev& lens, const GridDev& g, float2* out, cudaStream_t s);
 void launch_pctf_table(const PctfArgs& p, const GridDev& g, float2* out, cudaStream_t s);
 
+// Output phase ramp of a tilted beam, / ny, [ix][iy]: exp(i (gx Rx + gy Ry)) with Rx = Rx_shift(ix) -
+// rxc (two rounded products and a rounded sum in float, the phase's sine and cosine in double).
+void launch_tilt_ramp(const GridDev& g, float gx, float gy, float rxc, float ryc, float2* out, cudaStream_t s);
+
 // dst = sum over j < n of src[j * nxy + i] (the beams of a convergent incident wave, in order).
 void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s);
 

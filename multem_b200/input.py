@@ -87,6 +87,8 @@ class Parameters:
         self.E_0 = 300.0
         self.theta = 0.0
         self.phi = 0.0
+        self.ped_theta, self.ped_nrot = 3.0, 360
+        self.hci_theta, self.hci_nrot = 3.0, 360
         self.illumination_model = 3
         self.temporal_spatial_incoh = 1
         for k, v in _lens_defaults("cond_lens").items():
@@ -130,11 +132,12 @@ class Parameters:
                   "spec_cryst_na", "spec_cryst_nb", "spec_cryst_nc", "spec_rot_center_type", "thick_type",
                   "potential_slicing", "nx", "ny", "bwl", "iw_type", "illumination_model",
                   "temporal_spatial_incoh", "scanning_type", "scanning_periodic", "scanning_square_pxs",
-                  "scanning_ns", "output_area_ix_0", "output_area_iy_0", "output_area_ix_e", "output_area_iy_e"]:
+                  "scanning_ns", "output_area_ix_0", "output_area_iy_0", "output_area_ix_e", "output_area_iy_e",
+                  "ped_nrot", "hci_nrot"]:
             setattr(s, k, int(getattr(self, k)))
         for k in ["spec_lx", "spec_ly", "spec_lz", "spec_dz", "spec_cryst_a", "spec_cryst_b", "spec_cryst_c",
                   "spec_cryst_x0", "spec_cryst_y0", "spec_rot_theta", "E_0", "theta", "phi", "scanning_x0",
-                  "scanning_y0", "scanning_xe", "scanning_ye"]:
+                  "scanning_y0", "scanning_xe", "scanning_ye", "ped_theta", "hci_theta"]:
             setattr(s, k, float(getattr(self, k)))
         atoms = np.atleast_2d(np.asarray(self.spec_atoms, dtype=np.float64))
         if atoms.size == 0:

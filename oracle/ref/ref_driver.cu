@@ -151,6 +151,13 @@ void fill_input(const mt_input_multislice* in, mt::Input_Multislice<T>& im, int 
     im.E_0 = in->E_0;
     im.theta = in->theta * mt::c_deg_2_rad;
     im.phi = in->phi * mt::c_deg_2_rad;
+    if (im.is_PED()) {  // ilc_multem.cu:338-347
+        im.theta = in->ped_theta * mt::c_deg_2_rad;
+        im.nrot = in->ped_nrot;
+    } else if (im.is_HCTEM()) {
+        im.theta = in->hci_theta * mt::c_deg_2_rad;
+        im.nrot = in->hci_nrot;
+    }
 
     im.illumination_model = static_cast<mt::eIllumination_Model>(in->illumination_model);
     im.temporal_spatial_incoh = static_cast<mt::eTemporal_Spatial_Incoh>(in->temporal_spatial_incoh);

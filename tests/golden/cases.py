@@ -306,3 +306,32 @@ def stem_rot_srtio3():
     p.spec_rot_center_type = 2
     p.spec_rot_center_p = (7.0, 8.0, 5.0)
     return p
+
+
+def ped_si001():
+    """Precession electron diffraction (simulation_type 41) of Si(001), 256^2 grid: the beam tilted
+    by 2 deg and turned through 8 azimuths, diffraction patterns averaged over rotations and two
+    phonon configurations (the pattern is not shifted back: dp_Shift)."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.simulation_type = 41
+    p.pn_nconf = 2
+    p.pn_seed = 8
+    p.ped_theta, p.ped_nrot = 2.0, 8
+    return p
+
+
+def hctem_si001():
+    """Hollow-cone TEM (simulation_type 42) of Si(001), 256^2 grid: 1.5 deg cone, 6 azimuths, images
+    through the objective's coherent transfer function (defocus 50 A, 25 mrad), two phonon
+    configurations."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.simulation_type = 42
+    p.pn_nconf = 2
+    p.pn_seed = 9
+    p.hci_theta, p.hci_nrot = 1.5, 6
+    p.illumination_model = 1
+    p.obj_lens_c_10 = 50.0
+    p.obj_lens_outer_aper_ang = 25.0
+    return p
