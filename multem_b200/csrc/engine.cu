@@ -87,16 +87,22 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
 
     const size_t nxy = (size_t)nx * ny;
     const int n_thk = (int)m_.thick.size();
-    if (m_.is_STEM()) {
+    if (m_.is_scanning()) {
         // 64 Mi complex values (512 MiB) per batch, a multiple of the row pipeline's 8 groups
         int bdef = std::max(1, (int)((size_t)1 << 26) / (int)nxy);
         if (bdef >= 8) bdef -= bdef % 8;
         int bmax = env_int("MTB_BATCH", bdef);
         batch_ = std::max(1, std::min(bmax, m_.n_scan()));
         const int n_det = (int)m_.det_g_inner.size();
-        d_image_.alloc((size_t)n_thk * n_det * m_.n_scan());
-        const int tiles = col_tiles(nx, ny);
-        d_partial_.alloc((size_t)n_thk * batch_ * tiles * n_det);
+        if (m_.is_STEM()) {
+            d_image_.alloc((size_t)n_thk * n_det * m_.n_scan());
+            d_partial_.alloc((size_t)n_thk * batch_ * col_tiles(nx, ny) * n_det);
+        } else {
+            // ISTEM: one image per thickness, the images of every probe summed
+            const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
+            d_ew_m2_.alloc((size_t)n_thk * onxy);
+            d_tmp_.alloc((size_t)batch_ * nxy);
+        }
         std::vector<float2> beam(m_.n_scan());
         std::vector<int> idx(m_.n_scan());
         for (int i = 0; i < m_.n_scan(); i++) {
@@ -140,7 +146,8 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     if (m_.tilted()) {
         build_tilt_ramp();
         // STEM outputs at intermediate thicknesses apply the ramp to a copy of the batch
-        if (m_.is_STEM() && n_thk > 1) d_tmp_.alloc((size_t)batch_ * nxy);
+        if (m_.is_scanning() && n_thk > 1) d_tmp_.alloc((size_t)batch_ * nxy);
+        if (m_.is_ISTEM() && n_thk > 1) d_tmp2_.alloc((size_t)batch_ * nxy);
     }
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
     d_err_.alloc(1);
@@ -168,6 +175,7 @@ Engine::~Engine() {
         d_ctf_.release_idle();
         d_beams_psi_.release_idle();
         d_user_wave_.release_idle();
+        d_tmp2_.release_idle();
         d_coh_.release_idle();
         d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -525,7 +533,7 @@ void Engine::run_confs(int c0, int c1) {
     long long l0 = launches_issued();
     // graphs where launch overhead matters: passes of at most 4 Mi points per launch (above that
     // one launch runs for tens of microseconds and a recapture would cost more than it saves)
-    const size_t per_launch = (size_t)m_.grid.nx * m_.grid.ny * (m_.is_STEM() ? std::min(batch_, m_.n_scan()) : 1);
+    const size_t per_launch = (size_t)m_.grid.nx * m_.grid.ny * (m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1);
     if (graphs_ && !timing_ && per_launch <= ((size_t)1 << 22)) {
         // configuration c is prepared in slot c % 2 (prepare_conf waits for the stream, so the
         // slot's previous user, c - 2, has finished) and runs as that slot's graph
@@ -581,7 +589,7 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
 // launch sequence and arguments (same slot buffers, slice count, thickness map and probe defocus).
 // The line-pass autotuner runs before the capture (it times launches and waits for them).
 void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
-    if (tune_) pipe_ = tune_passes(m_.is_STEM() ? std::min(batch_, m_.n_scan()) : 1, cd);
+    if (tune_) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, cd);
     std::vector<char> sig = graph_signature(cd);
     if (!g.exec || sig != g.sig) {
         if (g.exec) {
@@ -634,7 +642,7 @@ void Engine::run_conf(ConfData& cd) {
     sa.trans = d_trans_.p;
     sa.V = nullptr;
     launch_splat(sa, 0, cd.last_slice + 1, stream_);
-    if (m_.is_STEM()) run_stem(cd); else run_ew(cd);
+    if (m_.is_scanning()) run_stem(cd); else run_ew(cd);
 }
 
 // Autotuner of the line passes: for each (nx, ny, probes per launch) the process times, once, the
@@ -789,6 +797,7 @@ ColArgs Engine::det_args() const {
     return ca;
 }
 
+
 void Engine::run_stem(ConfData& cd) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const size_t nxy = (size_t)nx * ny;
@@ -801,6 +810,7 @@ void Engine::run_stem(ConfData& cd) {
     ca.det_w = col_det_width(nx);
     ca.coh_w = (float)m_.phonon_weight();
     const bool tilt = d_ramp_.p != nullptr;
+    const bool istem = m_.is_ISTEM();
     RowArgs ra{};
     ra.nx = nx;
     ra.scale = 1.0f;
@@ -829,8 +839,8 @@ void Engine::run_stem(ConfData& cd) {
             rows(ROW_STEP, ra);
             const int ithk = cd.slice_ithk[k];
             int flags = COL_LOAD | COL_PROP;
-            if (ithk >= 0 && !tilt) flags |= COL_DETECT;
-            if (k < cd.last_slice || tilt) flags |= COL_INVERSE | COL_STORE;
+            if (ithk >= 0 && !tilt && !istem) flags |= COL_DETECT;
+            if (k < cd.last_slice || tilt || istem) flags |= COL_INVERSE | COL_STORE;
             ca.in = d_psi_.p;
             ca.out = d_psi_.p;
             ca.Px = cd.prop.p + (size_t)k * pl;
@@ -838,6 +848,39 @@ void Engine::run_stem(ConfData& cd) {
             ca.det_partial = d_partial_.p + (size_t)(ithk >= 0 ? ithk : 0) * batch_ * tiles * n_det;
             ca.coh = (d_coh_.p && ithk >= 0) ? d_coh_.p + ((size_t)ithk * n_scan + p0) * nxy : nullptr;
             cols(flags, ca);
+            if (istem && ithk >= 0) {
+                // ISTEM: each probe's wave through the objective lens (get_psi, then
+                // Microscope_Effects), |psi|^2 of the batch summed into the thickness's image
+                // (set_m2psi_tot_psi_coh, src/wave_function.cuh:166-170)
+                const float2* src = d_psi_.p;
+                if (tilt) {
+                    // the ramped batch goes where the next slices do not need it
+                    RowArgs rr = ra;
+                    rr.out = (k < cd.last_slice) ? d_tmp2_.p : d_psi_.p;
+                    rr.trans = d_ramp_.p;
+                    rows(ROW_STEP, rr);
+                    src = rr.out;
+                }
+                for (size_t j = 0; j < m_.obj_c10.size(); j++) {
+                    ColArgs cj = ca;
+                    cj.in = src;
+                    cj.out = d_tmp_.p;
+                    cj.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
+                    cj.Py = cj.Px + nx;
+                    cj.P2 = d_ctf_.p + j * nxy;
+                    cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cj);
+                    RowArgs rb = ra;
+                    rb.in = d_tmp_.p;
+                    rb.out = d_tmp_.p;
+                    rows(ROW_INVERSE, rb);
+                    launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e,
+                                         (double)(float)(w * m_.obj_w[j]), 0, nullptr,
+                                         d_ew_m2_.p + (size_t)ithk * ((size_t)(m_.out_ix_e - m_.out_ix_0) *
+                                                                      (m_.out_iy_e - m_.out_iy_0)),
+                                         stream_, nb);
+                }
+                continue;
+            }
             if (tilt && ithk >= 0) {
                 // get_psi: phase ramp, then the detectors on the transform (the output
                 // propagator's phase does not change |psi_hat|^2)
@@ -853,7 +896,7 @@ void Engine::run_stem(ConfData& cd) {
                 cols(COL_LOAD | COL_PROP | COL_DETECT, cc);
             }
         }
-        for (int t = 0; t < n_thk; t++)
+        for (int t = 0; t < n_thk && !istem; t++)
             launch_det_reduce(d_partial_.p + (size_t)t * batch_ * tiles * n_det, nb, tiles, n_det, d_scan_idx_.p + p0, w,
                               d_image_.p + (size_t)t * n_det * n_scan, n_scan, stream_);
         iter_ += nb;

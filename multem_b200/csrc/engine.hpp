@@ -161,6 +161,7 @@ class Engine {
     DevBuf<float2> d_ctf_;           // HRTEM transfer functions, one [nx][ny] table per defocus point
     DevBuf<float2> d_beams_psi_;     // convergent incident wave of several beams: one wave per beam
     DevBuf<float2> d_user_wave_;     // user-defined incident wave, in the row pass's input layout
+    DevBuf<float2> d_tmp2_;          // tilted ISTEM with several thicknesses: the ramped batch
     DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
     DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
     ColArgs det_args() const;        // detector description for the column pass

@@ -662,9 +662,9 @@ Model build_model(const mt_input_multislice* in) {
     if (!in) fail(MT_ERR_INVALID_ARG, "input is NULL");
     Model m;
     m.simulation_type = in->simulation_type;
-    if (!(m.is_STEM() || m.is_wave_sim()))
+    if (!(m.is_scanning() || m.is_wave_sim()))
         fail(MT_ERR_UNSUPPORTED, "simulation_type " + std::to_string(in->simulation_type) +
-                                     " is outside the plain multislice path (supported: 11 STEM, 21 CBED, 22 CBEI, "
+                                     " is outside the plain multislice path (supported: 11 STEM, 12 ISTEM, 21 CBED, 22 CBEI, "
                                      "31 ED, 32 HRTEM, 41 PED, 42 HCTEM, 51 EWFS, 52 EWRS)");
     m.interaction_model = in->interaction_model;
     if (m.interaction_model != 1) fail(MT_ERR_UNSUPPORTED, "only interaction_model 1 (multislice) is implemented");
@@ -735,9 +735,9 @@ Model build_model(const mt_input_multislice* in) {
 
     // validate_incident_wave_type (src/input_multislice.cuh:438-448)
     int iw = in->iw_type;
-    if (iw == 4) iw = (m.is_STEM() || m.is_CBED() || m.is_CBEI()) ? 2 : 1;
+    if (iw == 4) iw = (m.is_scanning() || m.is_CBED() || m.is_CBEI()) ? 2 : 1;
     m.iw_type = iw;
-    if (m.is_STEM() && iw != 2) fail(MT_ERR_UNSUPPORTED, "STEM needs a convergent incident wave");
+    if (m.is_scanning() && iw != 2) fail(MT_ERR_UNSUPPORTED, "STEM and ISTEM need a convergent incident wave");
     if (m.is_wave_sim() && iw == 3) {
         if (!in->iw_psi) fail(MT_ERR_INVALID_ARG, "iw_type 3 needs iw_psi");
         size_t n = (size_t)in->nx * in->ny;
@@ -770,7 +770,7 @@ Model build_model(const mt_input_multislice* in) {
     m.obj_lens.from_input(obj);
     m.obj_lens.set_input_data(m.E_0, m.grid);
 
-    if (m.is_STEM()) {
+    if (m.is_scanning()) {
         // Scanning::set_grid (src/types.cuh:4294-4390), regular grid
         m.scan_type = in->scanning_type;
         m.scan_pbc = in->scanning_periodic != 0;
@@ -821,6 +821,8 @@ Model build_model(const mt_input_multislice* in) {
                 }
         }
         if (m.scan_nx <= 0 || m.scan_ny <= 0) fail(MT_ERR_INVALID_ARG, "empty scan");
+    }
+    if (m.is_STEM()) {
         if (in->detector_type != 1 && in->detector_type != 3)
             fail(MT_ERR_UNSUPPORTED, "only circular (type 1) and matrix (type 3) detectors are implemented");
         m.det_type = in->detector_type;
@@ -862,8 +864,8 @@ Model build_model(const mt_input_multislice* in) {
     m.lambda = lambda_f(m.E_0);
     snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
-    if (m.is_wave_sim() && !m.is_EW() && m.pn_coh_contrib)
-        fail(MT_ERR_UNSUPPORTED, "CBED/CBEI/ED/HRTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
+    if (((m.is_wave_sim() && !m.is_EW()) || m.is_ISTEM()) && m.pn_coh_contrib)
+        fail(MT_ERR_UNSUPPORTED, "ISTEM/CBED/CBEI/ED/HRTEM/PED/HCTEM with pn_coh_contrib = 1 (m2psi_coh) is not implemented");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 
@@ -963,7 +965,7 @@ Model build_model(const mt_input_multislice* in) {
     if (m.is_imaging()) hrtem_ctf_points(m);
     // Multislice::STEM_ISTEM integrates the defocus spread only under full integration, and not
     // in its coherent-contribution branch, which comes first (src/tem_simulation.cuh:115-176)
-    if (m.is_STEM() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
+    if (m.is_scanning() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
     m.cond_lens.zero_defocus_plane = A.size() ? m.cond_lens.get_zero_defocus_plane(A.z_min, A.z_max) : 0.0f;
     m.cond_lens.zero_defocus_type = 4;
     m.obj_lens.set_input_data(m.E_0, m.grid);
@@ -990,7 +992,7 @@ Model build_model(const mt_input_multislice* in) {
     // an area given by the caller (not the "whole grid" default ix_0 == ix_e) that had to be
     // reordered or clipped
     const bool area_given = in->output_area_ix_0 != in->output_area_ix_e || in->output_area_iy_0 != in->output_area_iy_e;
-    if (m.is_wave_sim() && area_given &&
+    if ((m.is_wave_sim() || m.is_ISTEM()) && area_given &&
         (m.out_ix_0 != in->output_area_ix_0 - 1 || m.out_ix_e != in->output_area_ix_e - 1 ||
          m.out_iy_0 != in->output_area_iy_0 - 1 || m.out_iy_e != in->output_area_iy_e - 1))
         m.clamps.push_back("output_area -> ix [" + std::to_string(m.out_ix_0 + 1) + ", " + std::to_string(m.out_ix_e + 1) +

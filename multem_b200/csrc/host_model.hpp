@@ -154,6 +154,8 @@ struct Model {
     AtomsF atoms_in;
 
     bool is_STEM() const { return simulation_type == 11; }
+    bool is_ISTEM() const { return simulation_type == 12; }
+    bool is_scanning() const { return is_STEM() || is_ISTEM(); }
     bool is_EWFS() const { return simulation_type == 51; }
     bool is_EWRS() const { return simulation_type == 52; }
     bool is_EW() const { return is_EWFS() || is_EWRS(); }
@@ -168,8 +170,8 @@ struct Model {
     bool is_wave_sim() const {
         return is_EW() || is_ED() || is_HRTEM() || is_CBED() || is_CBEI() || is_PED() || is_HCTEM();
     }
-    // image formation through the objective lens (Microscope_Effects): HRTEM, CBEI, HCTEM
-    bool is_imaging() const { return is_HRTEM() || is_CBEI() || is_HCTEM(); }
+    // image formation through the objective lens (Microscope_Effects): HRTEM, CBEI, HCTEM, ISTEM
+    bool is_imaging() const { return is_HRTEM() || is_CBEI() || is_HCTEM() || is_ISTEM(); }
     // outputs on the Fourier grid (is_grid_FS, src/input_multislice.cuh:367-372)
     bool is_grid_FS() const { return is_EWFS() || is_ED() || is_CBED() || is_PED(); }
     bool is_frozen_phonon() const { return pn_model == 3; }

@@ -404,7 +404,7 @@ void launch_coh_detect(const float2* coh, int n_thk, int n_scan, const ColArgs& 
 // add_scale_square_crop_shift_2d / assign_crop_shift_2d, src/cgpu_fcns.cuh:1681-1780).
 __global__ void ew_accumulate_kernel(const float2* __restrict__ psi, int nx, int ny, int ix0, int ix1, int iy0,
                                      int iy1, double w, int assign, double* __restrict__ psi_out,
-                                     double* __restrict__ m2_out) {
+                                     double* __restrict__ m2_out, int nwave) {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y;
     if (iy >= ny || ix >= nx) return;
@@ -423,15 +423,20 @@ __global__ void ew_accumulate_kernel(const float2* __restrict__ psi, int nx, int
         }
     }
     if (m2_out) {
-        const float n2 = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
-        m2_out[o] += w * (double)n2;
+        double acc = 0.0;
+        for (int j = 0; j < nwave; j++) {
+            const float2 u = (j == 0) ? v : psi[(size_t)j * nx * ny + (size_t)sx * ny + sy];
+            const float n2 = __fadd_rn(__fmul_rn(u.x, u.x), __fmul_rn(u.y, u.y));
+            acc += w * (double)n2;
+        }
+        m2_out[o] += acc;
     }
 }
 
 void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, int iy0, int iy1, double w,
-                          int assign, double* psi_out, double* m2_out, cudaStream_t s) {
+                          int assign, double* psi_out, double* m2_out, cudaStream_t s, int nwave) {
     dim3 grid((ny + 127) / 128, nx);
-    ew_accumulate_kernel<<<grid, 128, 0, s>>>(psi, nx, ny, ix0, ix1, iy0, iy1, w, assign, psi_out, m2_out);
+    ew_accumulate_kernel<<<grid, 128, 0, s>>>(psi, nx, ny, ix0, ix1, iy0, iy1, w, assign, psi_out, m2_out, nwave);
     g_launches++;
     MTB_CUDA(cudaGetLastError());
 }

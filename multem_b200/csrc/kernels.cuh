@@ -126,8 +126,9 @@ void launch_coh_detect(const float2* coh, int n_thk, int n_scan, const ColArgs& 
 
 // EW output: out[(ix-ix0)*oy + (iy-iy0)] accumulates psi (complex) and |psi|^2 over the output
 // area after an fft-shift by (nx/2, ny/2) (add_scale_crop_shift_2d, src/cgpu_fcns.cuh:1701-1739).
+// With nwave > 1 (ISTEM) the |psi|^2 of nwave consecutive waves are summed in order (m2 only).
 void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, int iy0, int iy1, double w,
-                          int assign, double* psi_out, double* m2_out, cudaStream_t s);
+                          int assign, double* psi_out, double* m2_out, cudaStream_t s, int nwave = 1);
 
 // Device-side counters of this library's launches (for reporting).
 long long launches_issued();

@@ -335,3 +335,16 @@ def hctem_si001():
     p.obj_lens_c_10 = 50.0
     p.obj_lens_outer_aper_ang = 25.0
     return p
+
+
+def istem_srtio3():
+    """ISTEM (simulation_type 12) of SrTiO3(001), 256^2 grid: 3 x 3 probes (21 mrad), each exit wave
+    imaged through the objective's coherent transfer function (defocus 30 A, 25 mrad), the images
+    of all probes and two phonon configurations summed."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=13)
+    p.simulation_type = 12
+    p.illumination_model = 1
+    p.obj_lens_c_10 = 30.0
+    p.obj_lens_outer_aper_ang = 25.0
+    return p
