@@ -667,7 +667,8 @@ Model build_model(const mt_input_multislice* in) {
                                      " is outside the plain multislice path (supported: 11 STEM, 12 ISTEM, 21 CBED, 22 CBEI, "
                                      "31 ED, 32 HRTEM, 41 PED, 42 HCTEM, 51 EWFS, 52 EWRS)");
     m.interaction_model = in->interaction_model;
-    if (m.interaction_model != 1) fail(MT_ERR_UNSUPPORTED, "only interaction_model 1 (multislice) is implemented");
+    if (m.interaction_model < 1 || m.interaction_model > 3)
+        fail(MT_ERR_UNSUPPORTED, "interaction_model must be 1 (multislice), 2 (phase object) or 3 (weak phase object)");
     m.potential_type = in->potential_type;
     if (m.potential_type != 6) fail(MT_ERR_UNSUPPORTED, "only potential_type 6 (Lobato 0-12) is implemented");
     m.mul_sign = in->reverse_multislice ? -1 : 1;
@@ -910,6 +911,9 @@ Model build_model(const mt_input_multislice* in) {
         A.statistic(nullptr);
     }
 
+    // "temporal fix for phase object" (src/input_multislice.cuh:724-728)
+    if (!m.is_multislice() && m.thick_type == 1) m.potential_slicing = 2;
+
     // Slicing::match_thickness (src/slicing.hpp:53-71)
     if (m.thick_type == 1) {
         m.thick.assign(1, A.z_max);
@@ -1030,11 +1034,19 @@ Specimen::Specimen(const Model& m, const std::vector<float>& R_max_of_Z) : m_(m)
     atoms_u_.sort_by_z();
     z_plane_ = z_planes(m.potential_slicing, atoms_u_);
     grid_dz_ = m.grid.dz;
-    // phase-object switch (src/spec.hpp:65-77)
-    if ((atoms_u_.s_z_int < 2.0f * grid_dz_) || ((z_plane_.size() == 1) && m.potential_slicing == 1)) {
+    // phase-object switch (src/spec.hpp:65-77): a phase object requested, or a specimen thinner
+    // than two slices, or a single plane under plane slicing, is transmitted without propagation,
+    // one slice per thickness (the weak phase object uses the same slicing, Slicing::get_thick /
+    // get_slicing branch on !is_multislice, src/slicing.hpp:326-356)
+    thick_type_ = m.thick_type;
+    if ((m.interaction_model == 2) || (atoms_u_.s_z_int < 2.0f * grid_dz_) ||
+        ((z_plane_.size() == 1) && m.potential_slicing == 1)) {
         phase_object_ = true;
-        fail(MT_ERR_UNSUPPORTED, "specimen thinner than two slices (phase-object mode) is not implemented");
+        grid_dz_ = atoms_u_.s_z_int;
+        atoms_u_.dz = grid_dz_;
+        if (thick_type_ == 3) thick_type_ = 2;
     }
+    phase_object_ = phase_object_ || !m.is_multislice();
     atoms_ = atoms_u_;
     atoms_.statistic(R_max_of_Z_.data());
     calculate();
@@ -1099,7 +1111,7 @@ void Specimen::calculate() {
         ThickF& t = thick_[ik];
         t.z = m_.thick[ik];
         int islice = 0;
-        if (m_.thick_type == 3) {
+        if (thick_type_ == 3) {
             for (size_t i = 0; i + 1 < z_slice_.size(); i++)
                 if (std::fabs(z_slice_[i + 1] - t.z) < 1e-4f) { islice = (int)i; break; }
         } else {
@@ -1110,12 +1122,31 @@ void Specimen::calculate() {
         t.iatom_e = last_atom_below(zr, z_slice_[islice + 1]);
         float za = zr[0], zb = zr[std::max(0, t.iatom_e)];
         t.z_zero_def_plane = m_.obj_lens.get_zero_defocus_plane(za, zb);
-        if (m_.thick_type == 3) {
+        if (thick_type_ == 3) {
             t.z_back_prop = 0;
         } else {
             t.z_back_prop = (float)(t.z_zero_def_plane - 0.5 * (z_slice_[islice] + z_slice_[islice + 1]));
             if (std::fabs(t.z_back_prop) < 1e-4f) t.z_back_prop = 0;
         }
+    }
+    if (phase_object_) {
+        // one slice per thickness, back-propagated from the thickness plane
+        for (size_t ik = 0; ik < thick_.size(); ik++) {
+            thick_[ik].islice = (int)ik;
+            thick_[ik].z_back_prop = thick_[ik].z_zero_def_plane - thick_[ik].z;
+        }
+        slice_.assign(thick_.size(), SliceF());
+        for (size_t i = 0; i < slice_.size(); i++) {
+            SliceF& s = slice_[i];
+            s.z_0 = (i == 0) ? atoms_.z_int_min : thick_[i - 1].z;
+            s.z_e = (thick_.size() == 1) ? atoms_.z_int_max : thick_[i].z;
+            s.z_int_0 = s.z_0;
+            s.z_int_e = s.z_e;
+            s.iatom_0 = (i == 0) ? 0 : thick_[i - 1].iatom_e + 1;
+            s.iatom_e = thick_[i].iatom_e;
+            s.ithk = (int)i;
+        }
+        return;
     }
 
     // get_slicing (src/slicing.hpp:339-403)
@@ -1134,6 +1165,7 @@ void Specimen::calculate() {
 
 // Spec::dz (src/spec.hpp:129-132)
 float Specimen::dz(int islice) const {
+    if (phase_object_) return 0.0f;  // transmission only (Wave_Function::psi_slice, src/wave_function.cuh:230-238)
     float d = (islice < (int)slice_.size()) ? slice_[islice].z_e - slice_[islice].z_0 : 0.0f;
     return d / std::cos(m_.theta);
 }

@@ -153,6 +153,7 @@ struct Model {
     // specimen as given (after the z-range filter of validate_parameters)
     AtomsF atoms_in;
 
+    bool is_multislice() const { return interaction_model == 1; }
     bool is_STEM() const { return simulation_type == 11; }
     bool is_ISTEM() const { return simulation_type == 12; }
     bool is_scanning() const { return is_STEM() || is_ISTEM(); }
@@ -238,6 +239,7 @@ class Specimen {
     std::vector<SliceF> slice_;
     std::vector<ThickF> thick_;
     bool phase_object_ = false;
+    int thick_type_ = 1;  // the model's, changed to 2 when a through-slice run becomes a phase object
     float grid_dz_ = 0;
 
     void calculate();

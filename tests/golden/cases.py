@@ -348,3 +348,53 @@ def istem_srtio3():
     p.obj_lens_c_10 = 30.0
     p.obj_lens_outer_aper_ang = 25.0
     return p
+
+
+def _au_monolayer():
+    from multem_b200 import specimens
+    a = 4.078
+    layer = (a, a, a, [(79, 0.0, 0.0, 0.0), (79, 0.5, 0.5, 0.0)])  # the z = 0 plane of fcc(001)
+    return specimens.crystal(layer, 6, 6, 1, sigma=0.085), 6 * a
+
+
+def ew_monolayer_au():
+    """Exit wave (EWRS) of a single Au(001) atomic plane (6 x 6 cells) on a 256^2 grid: one plane
+    under plane slicing, so the reference switches to its phase-object mode (transmission only);
+    two phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.spec_atoms, L = _au_monolayer()
+    p.spec_lx = p.spec_ly = L
+    p.spec_lz = 4.0
+    p.pn_nconf = 2
+    p.pn_seed = 14
+    return p
+
+
+def stem_monolayer_au():
+    """STEM ADF over the single Au(001) plane (phase-object mode), 256^2 grid, 3 x 3 probes."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=15)
+    p.spec_atoms, L = _au_monolayer()
+    p.spec_lx = p.spec_ly = L
+    p.spec_lz = 4.0
+    p.potential_slicing = 1
+    p.scanning_x0 = p.scanning_y0 = 2 * 4.078
+    p.scanning_xe = p.scanning_ye = 3 * 4.078
+    return p
+
+
+def ew_po_si001():
+    """Exit wave (EWRS) of Si(001) 4 x 4 x 4 cells in the phase-object approximation
+    (interaction_model 2): the whole specimen's projected potential, transmission only."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.interaction_model = 2
+    return p
+
+
+def ew_wpo_si001():
+    """ew_po_si001 in the weak-phase-object approximation (interaction_model 3: T = 1 + i sigma V)."""
+    p = ew_po_si001()
+    p.interaction_model = 3
+    return p

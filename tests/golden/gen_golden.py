@@ -25,7 +25,8 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    stem_tilt_au001, ew_tilt_si001, ewfs_tilt_si001, stem_incoh_srtio3, stem_matrix_srtio3,
                    stem_coh_srtio3, ed_si001, hrtem_coherent_si001, hrtem_pctf_si001, hrtem_fullint_si001,
                    cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001,
-                   ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3)
+                   ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3, ew_monolayer_au,
+                   stem_monolayer_au, ew_po_si001, ew_wpo_si001)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -61,9 +62,12 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("cbed_si001", cbed_si001), ("cbei_si001", cbei_si001), ("ewrs_two_beams_si001", ewrs_two_beams_si001),
              ("ewrs_user_wave_si001", ewrs_user_wave_si001), ("hrtem_user_wave_si001", hrtem_user_wave_si001),
              ("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3),
-             ("ped_si001", ped_si001), ("hctem_si001", hctem_si001), ("istem_srtio3", istem_srtio3))
+             ("ped_si001", ped_si001), ("hctem_si001", hctem_si001), ("istem_srtio3", istem_srtio3),
+             ("ew_monolayer_au", ew_monolayer_au), ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001),
+             ("ew_wpo_si001", ew_wpo_si001))
 
-SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3))
+SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
+             ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))
 
 
 def specimen_fixtures(rec, names=None):

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from multem_b200 import api, specimens
-from cases import amorph_au110, ew_rot_si001, stem_rot_srtio3
+from cases import amorph_au110, ew_monolayer_au, ew_po_si001, ew_rot_si001, ew_wpo_si001, stem_monolayer_au, stem_rot_srtio3
 
 
 def cases():
@@ -23,11 +23,16 @@ def cases():
         "amorph_au110": amorph_au110(),
         "ew_rot_si001": ew_rot_si001(),
         "stem_rot_srtio3": stem_rot_srtio3(),
+        "ew_monolayer_au": ew_monolayer_au(),
+        "stem_monolayer_au": stem_monolayer_au(),
+        "ew_po_si001": ew_po_si001(),
+        "ew_wpo_si001": ew_wpo_si001(),
     }
 
 
 @pytest.mark.parametrize("name", ["stem_small", "stem_thick", "ew_small", "ew_config1", "amorph_au110", "ew_rot_si001",
-                                  "stem_rot_srtio3"])
+                                  "stem_rot_srtio3", "ew_monolayer_au", "stem_monolayer_au", "ew_po_si001",
+                                  "ew_wpo_si001"])
 @pytest.mark.parametrize("iconf", [1, 2])
 def test_displaced_atoms_and_slices_bit_exact(golden, name, iconf):
     p = cases()[name]
