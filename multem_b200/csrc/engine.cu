@@ -142,6 +142,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         }
     }
     d_psi_.alloc((size_t)batch_ * nxy);
+    if (m_.grid.bwl) build_bwl();
     if (m_.is_imaging()) build_ctf_tables();
     if (m_.tilted()) {
         build_tilt_ramp();
@@ -176,6 +177,7 @@ Engine::~Engine() {
         d_beams_psi_.release_idle();
         d_user_wave_.release_idle();
         d_tmp2_.release_idle();
+        for (auto* b : {&d_bwl_, &d_one_, &d_p0_}) b->release_idle();
         d_coh_.release_idle();
         d_image_coh_.release_idle();
         for (auto* b : {&d_partial_, &d_image_, &d_ew_psi_, &d_ew_m2_}) b->release_idle();
@@ -257,6 +259,62 @@ void Engine::build_tilt_ramp() {
     }
 }
 
+// Band-width limit (bwl = 1): Grid_2d::bwl_factor_shift (src/types.cuh:2588-2598), the Fermi cut-off
+// 1/(1 + exp(alpha (g^2 - gl2_max))) at two thirds of g_max, in float as the reference. The
+// propagator multiplies by it (propagate, src/cgpu_fcns.cuh:1837-1845) and so do the transmission
+// functions (Transmission_Function::trans, src/transmission_function.cuh:72-82); here it is the
+// column passes' [nx][ny] factor (ColArgs::P2).
+void Engine::build_bwl() {
+    const GridF& g = m_.grid;
+    const int nx = g.nx, ny = g.ny;
+    std::vector<float2> f((size_t)nx * ny);
+    for (int ix = 0; ix < nx; ix++) {
+        const float gx = (float)((ix < g.nxh) ? ix : ix - nx) * g.dgx;
+        for (int iy = 0; iy < ny; iy++) {
+            const float gy = (float)((iy < g.nyh) ? iy : iy - ny) * g.dgy;
+            const float g2 = gx * gx + gy * gy;
+            const float e = std::exp(g.alpha * (g2 - g.gl2_max));
+            f[(size_t)ix * ny + iy] = make_float2((float)(1.0 / (1.0 + (double)e)), 0.0f);
+        }
+    }
+    d_bwl_.upload(f.data(), f.size(), stream_);
+    std::vector<float2> ones((size_t)nx * ny, make_float2(1.0f, 0.0f));
+    d_one_.upload(ones.data(), ones.size(), stream_);
+    std::vector<float2> p0((size_t)nx + ny);
+    mtb::prop_tables(m_, 0.0f, p0.data(), p0.data() + nx, false);
+    d_p0_.upload(p0.data(), p0.size(), stream_);
+    synchronize();
+}
+
+// bwl = 1: T <- IFFT(bwl_factor/N * FFT(T)) for the slices of a configuration, as three line passes
+// over all slices at once (a real-space row pass, the column pass with the cut-off, the inverse row
+// pass).
+void Engine::band_limit_trans(const ConfData& cd) {
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const int ns = cd.last_slice + 1;
+    RowArgs ra{};
+    ra.in = d_trans_.p;
+    ra.out = d_trans_.p;
+    ra.trans = d_one_.p;
+    ra.nx = nx;
+    ra.nprobe = ns;
+    ra.scale = 1.0f;
+    rows(ROW_FIRST_REAL, ra);
+    ColArgs ca{};
+    ca.in = d_trans_.p;
+    ca.out = d_trans_.p;
+    ca.ny = ny;
+    ca.nprobe = ns;
+    ca.g = gdev_;
+    ca.Px = d_p0_.p;
+    ca.Py = d_p0_.p + nx;
+    ca.P2 = d_bwl_.p;
+    ca.det_w = col_det_width(nx);
+    cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, ca);
+    RowArgs rb = ra;
+    rows(ROW_INVERSE, rb);
+}
+
 // HRTEM: the objective's transfer function per defocus point (Microscope_Effects, see
 // hrtem_ctf_points), as [nx][ny] tables in FFT order that the output column pass multiplies in
 // after the back-propagation factors (get_psi then apply_CTF / apply_PCTF).
@@ -264,6 +322,7 @@ void Engine::build_ctf_tables() {
     const size_t nxy = (size_t)m_.grid.nx * m_.grid.ny;
     const size_t np = m_.obj_c10.size();
     d_ctf_.alloc(np * nxy);
+    // the output propagation's band-width limit rides on the transfer function
     for (size_t j = 0; j < np; j++) {
         LensF L = m_.obj_lens;
         if (m_.ctf_mode == 2) {
@@ -310,6 +369,7 @@ void Engine::build_ctf_tables() {
             pr.c_c_56 = L.c_c_56; pr.phi_56 = L.phi_56;
             launch_ctf_table(pr, gdev_, d_ctf_.p + j * nxy, stream_);
         }
+        if (d_bwl_.p) launch_mul_tables(d_ctf_.p + j * nxy, d_bwl_.p, nxy, stream_);
     }
 }
 
@@ -642,6 +702,7 @@ void Engine::run_conf(ConfData& cd) {
     sa.trans = d_trans_.p;
     sa.V = nullptr;
     launch_splat(sa, 0, cd.last_slice + 1, stream_);
+    if (d_bwl_.p) band_limit_trans(cd);
     if (m_.is_scanning()) run_stem(cd); else run_ew(cd);
 }
 
@@ -809,8 +870,12 @@ void Engine::run_stem(ConfData& cd) {
     ColArgs ca = det_args();
     ca.det_w = col_det_width(nx);
     ca.coh_w = (float)m_.phonon_weight();
+    ca.P2 = d_bwl_.p;  // band-width limit of every propagation (NULL without bwl)
     const bool tilt = d_ramp_.p != nullptr;
     const bool istem = m_.is_ISTEM();
+    // the detectors get their own output pass when the output needs more than the last slice's
+    // column pass: a phase ramp (tilt) or a second band-width limit (bwl)
+    const bool sep_out = tilt || d_bwl_.p != nullptr;
     RowArgs ra{};
     ra.nx = nx;
     ra.scale = 1.0f;
@@ -839,8 +904,8 @@ void Engine::run_stem(ConfData& cd) {
             rows(ROW_STEP, ra);
             const int ithk = cd.slice_ithk[k];
             int flags = COL_LOAD | COL_PROP;
-            if (ithk >= 0 && !tilt && !istem) flags |= COL_DETECT;
-            if (k < cd.last_slice || tilt || istem) flags |= COL_INVERSE | COL_STORE;
+            if (ithk >= 0 && !sep_out && !istem) flags |= COL_DETECT;
+            if (k < cd.last_slice || sep_out || istem) flags |= COL_INVERSE | COL_STORE;
             ca.in = d_psi_.p;
             ca.out = d_psi_.p;
             ca.Px = cd.prop.p + (size_t)k * pl;
@@ -881,16 +946,21 @@ void Engine::run_stem(ConfData& cd) {
                 }
                 continue;
             }
-            if (tilt && ithk >= 0) {
-                // get_psi: phase ramp, then the detectors on the transform (the output
-                // propagator's phase does not change |psi_hat|^2)
-                RowArgs rr = ra;
-                rr.out = (k < cd.last_slice) ? d_tmp_.p : d_psi_.p;
-                rr.trans = d_ramp_.p;
-                rows(ROW_STEP, rr);
+            if (sep_out && ithk >= 0) {
+                // get_psi: phase ramp (tilted beam), then the detectors on the transform after
+                // the output propagation (its phase does not change |psi_hat|^2; its band-width
+                // limit does)
+                float2* src = d_psi_.p;
+                if (tilt) {
+                    RowArgs rr = ra;
+                    rr.out = (k < cd.last_slice) ? d_tmp_.p : d_psi_.p;
+                    rr.trans = d_ramp_.p;
+                    rows(ROW_STEP, rr);
+                    src = rr.out;
+                }
                 ColArgs cc = ca;
-                cc.in = rr.out;
-                cc.out = rr.out;
+                cc.in = src;
+                cc.out = src;
                 cc.Px = cd.prop.p + (size_t)(cd.n_slice + ithk) * pl;
                 cc.Py = cc.Px + nx;
                 cols(COL_LOAD | COL_PROP | COL_DETECT, cc);
@@ -923,6 +993,7 @@ void Engine::run_ew(ConfData& cd) {
     ca.nprobe = 1;
     ca.g = gdev_;
     ca.n_det = 0;
+    ca.P2 = d_bwl_.p;  // band-width limit of every propagation (NULL without bwl)
     if (tune_) pipe_ = tune_passes(1, cd);
     const bool conv = m_.is_convergent_wave();
     const bool user = m_.is_user_wave();
@@ -993,7 +1064,7 @@ void Engine::run_ew(ConfData& cd) {
         }
         if (m_.is_EWRS()) {
             RowArgs rb = ra;
-            if (zbp != 0.0f) {
+            if (zbp != 0.0f || d_bwl_.p) {
                 cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cb);
                 rb.in = d_tmp_.p;
                 rb.scale = 1.0f;

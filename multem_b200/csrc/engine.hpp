@@ -162,6 +162,9 @@ class Engine {
     DevBuf<float2> d_beams_psi_;     // convergent incident wave of several beams: one wave per beam
     DevBuf<float2> d_user_wave_;     // user-defined incident wave, in the row pass's input layout
     DevBuf<float2> d_tmp2_;          // tilted ISTEM with several thicknesses: the ramped batch
+    DevBuf<float2> d_bwl_;           // band-width limit factor [nx][ny] (bwl = 1), else empty
+    DevBuf<float2> d_one_;           // ones [nx][ny]: the row pass that transforms the transmission functions
+    DevBuf<float2> d_p0_;            // zero-distance propagator factors (1/N only), Px then Py
     DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
     DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
     ColArgs det_args() const;        // detector description for the column pass
@@ -181,6 +184,8 @@ class Engine {
     void build_ctf_tables();
     float aperture_norm() const;
     void build_user_wave();
+    void build_bwl();
+    void band_limit_trans(const ConfData& cd);
     void check_cancel();
     ConfData* find_conf(int iconf);
 

@@ -732,7 +732,6 @@ Model build_model(const mt_input_multislice* in) {
 
     if (in->nx <= 0 || in->ny <= 0) fail(MT_ERR_INVALID_ARG, "nx and ny must be positive");
     m.grid.set(in->nx, in->ny, lx, ly, dz, in->bwl != 0, true);
-    if (m.grid.bwl) fail(MT_ERR_UNSUPPORTED, "bwl = 1 (band-width limit) is not implemented");
 
     // validate_incident_wave_type (src/input_multislice.cuh:438-448)
     int iw = in->iw_type;

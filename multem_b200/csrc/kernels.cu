@@ -336,6 +336,17 @@ void launch_tilt_ramp(const GridDev& g, float gx, float gy, float rxc, float ryc
     MTB_CUDA(cudaGetLastError());
 }
 
+__global__ void mul_tables_kernel(float2* __restrict__ a, const float2* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        a[i] = cmul(a[i], b[i]);
+}
+
+void launch_mul_tables(float2* a, const float2* b, size_t n, cudaStream_t s) {
+    mul_tables_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, s>>>(a, b, n);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
 __global__ void sum_waves_kernel(const float2* __restrict__ src, int n, size_t nxy, float2* __restrict__ dst) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nxy; i += (size_t)gridDim.x * blockDim.x) {
         float2 acc = src[i];

@@ -115,6 +115,9 @@ void launch_pctf_table(const PctfArgs& p, const GridDev& g, float2* out, cudaStr
 // rxc (two rounded products and a rounded sum in float, the phase's sine and cosine in double).
 void launch_tilt_ramp(const GridDev& g, float gx, float gy, float rxc, float ryc, float2* out, cudaStream_t s);
 
+// a[i] *= b[i] (complex), n values.
+void launch_mul_tables(float2* a, const float2* b, size_t n, cudaStream_t s);
+
 // dst = sum over j < n of src[j * nxy + i] (the beams of a convergent incident wave, in order).
 void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s);
 

@@ -398,3 +398,32 @@ def ew_wpo_si001():
     p = ew_po_si001()
     p.interaction_model = 3
     return p
+
+
+def ew_bwl_si001():
+    """Exit wave (EWRS) of Si(001), 256^2 grid, with the band-width limit (bwl = 1: the transmission
+    functions and every propagation cut off smoothly at 2/3 of g_max); two phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.bwl = 1
+    p.pn_nconf = 2
+    p.pn_seed = 16
+    return p
+
+
+def stem_bwl_srtio3():
+    """STEM ADF through SrTiO3(001) with the band-width limit, 256^2 grid, 3 x 3 probes, two
+    thicknesses, two phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=17)
+    p.bwl = 1
+    p.thick_type = 2
+    p.thick = [8.0, 15.0]
+    return p
+
+
+def hrtem_bwl_si001():
+    """HRTEM (coherent transfer function) of Si(001) with the band-width limit."""
+    p = _hrtem(1)
+    p.bwl = 1
+    return p

@@ -26,7 +26,7 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    stem_coh_srtio3, ed_si001, hrtem_coherent_si001, hrtem_pctf_si001, hrtem_fullint_si001,
                    cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001,
                    ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3, ew_monolayer_au,
-                   stem_monolayer_au, ew_po_si001, ew_wpo_si001)
+                   stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -64,7 +64,8 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3),
              ("ped_si001", ped_si001), ("hctem_si001", hctem_si001), ("istem_srtio3", istem_srtio3),
              ("ew_monolayer_au", ew_monolayer_au), ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001),
-             ("ew_wpo_si001", ew_wpo_si001))
+             ("ew_wpo_si001", ew_wpo_si001), ("ew_bwl_si001", ew_bwl_si001), ("stem_bwl_srtio3", stem_bwl_srtio3),
+             ("hrtem_bwl_si001", hrtem_bwl_si001))
 
 SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
              ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))
