@@ -576,19 +576,29 @@ struct RowPipeShape {
 // transforms the items k = x, x+NG, ... of the CTA (item = blockIdx.x + k*gridDim.x) from its
 // own landing buffer, issues the copy of its next item as soon as it has read the buffer, and
 // exchanges through its own half-line buffers.
-template <int NX, int GT, int NG>
+// EARLY: the next tile is issued as soon as the group has read its slot, the exchanges use a separate
+// half-line buffer (HalfExchange). Otherwise (lengths without a half-line exchange, 1024) the slot
+// doubles as the full exchange buffer and the next tile is issued once the group's last exchange
+// read is done; the other groups keep the copy engine busy meanwhile.
+template <int NX, int GT, int NG, bool EARLY = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)>
 struct ColPipe {
     using G = LineGeom<NX>;
+    static constexpr bool EARLY_V = EARLY;
     static constexpr int W = GT / G::TPL;
     static constexpr int LSH = HalfLineSmem<NX>::value;
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
-    static constexpr size_t LAND = (size_t)W * NX;
-    static constexpr size_t HBUF = (size_t)W * LSH;
+    static constexpr size_t LAND0 = (size_t)W * NX;
+    static constexpr size_t LAND1 = EARLY ? LAND0 : ((size_t)W * G::LS > LAND0 ? (size_t)W * G::LS : LAND0);
+    static constexpr size_t LAND = (LAND1 + 15) / 16 * 16;  // slots on 128-byte boundaries (bulk-copy targets)
+    static constexpr size_t HBUF = EARLY ? (size_t)W * LSH : 0;
     static constexpr size_t SMEM = sizeof(float2) * (TW + NX + NG * LAND + NG * HBUF);
-    static constexpr int BOXR = NX < 256 ? NX : 256;
-    static constexpr bool OK = HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK && (GT % G::TPL == 0) &&
-                               (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) && (HBUF % 2 == 0) &&
-                               SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
+    // rows per bulk-copy box: the boxes must tile the NX rows exactly (a box reaching past NX would
+    // write past the slot and count bytes the barrier does not expect)
+    static constexpr int BOXR = (NX <= 256) ? NX : (NX % 256 == 0) ? 256 : (NX % 128 == 0) ? 128 : 0;
+    static constexpr bool OK = (!EARLY || (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)) &&
+                               (BOXR > 0) && (NX % (BOXR > 0 ? BOXR : 1) == 0) && ((size_t)NX * W <= LAND) &&
+                               (GT % G::TPL == 0) && (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) &&
+                               (HBUF % 2 == 0) && SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
 };
 
 template <int NX>
@@ -596,14 +606,15 @@ struct ColPipeShape {
     static constexpr int GT = 256, NG = 2;
 };
 
-template <int NX, int FLAGS, int LDY, int GT, int NG>
+template <int NX, int FLAGS, int LDY, int GT, int NG, bool EARLY>
 __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const __grid_constant__ CUtensorMap map) {
     using G = LineGeom<NX>;
-    using P = ColPipe<NX, GT, NG>;
+    using P = ColPipe<NX, GT, NG, EARLY>;
     constexpr int E = G::E, W = P::W, NWARP = GT / 32;
     constexpr bool PROP = FLAGS & COL_PROP, DET = FLAGS & COL_DETECT;
     constexpr bool INV = FLAGS & COL_INVERSE, STORE = FLAGS & COL_STORE;
     static_assert(FLAGS & COL_LOAD, "column pass without a load");
+    static_assert(P::BOXR > 0 && NX % P::BOXR == 0 && (size_t)NX * W <= P::LAND, "bulk-copy boxes must fit the slot");
     constexpr unsigned TILE_BYTES = NX * W * sizeof(float2);
     extern __shared__ __align__(1024) unsigned char pipe_smem[];
     __shared__ unsigned long long full[NG];
@@ -616,8 +627,8 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     float2* land0 = s_px + NX;  // NG landing buffers, [row][W] each
     const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
     const int c = gtid % W, t = gtid / W;
-    const float2* land = land0 + grp * P::LAND;
-    float2* buf = land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH;
+    float2* land = land0 + grp * P::LAND;
+    float2* buf = EARLY ? land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH : land + (size_t)c * G::LS;
     if constexpr (PROP) {
         for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
     }
@@ -658,8 +669,12 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
 #pragma unroll
         for (int i = 0; i < E; i++) x[i] = land[(size_t)reg_pos<NX, G::R1>(i, t) * W + c];
         gsync();  // the whole group has read its landing buffer
-        if (gtid == 0 && k + NG < K) issue(k + NG);
-        line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
+        if constexpr (EARLY) {
+            if (gtid == 0 && k + NG < K) issue(k + NG);
+            line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
+        } else {
+            line_fft<NX, false, -1>(x, buf, twP, t, gsync);
+        }
         if constexpr (PROP) {
             const float2 py = a.Py[iy];
 #pragma unroll
@@ -692,10 +707,22 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             gsync();
         }
         if constexpr (INV) {
-            line_fft_half<NX, true, +1>(x, buf, twR, t, gsync);
+            if constexpr (EARLY) {
+                line_fft_half<NX, true, +1>(x, buf, twR, t, gsync);
+            } else {
+                line_fft<NX, true, +1>(x, buf, twR, t, gsync);
+                gsync();  // every exchange read of the slot is done
+                if (gtid == 0 && k + NG < K) issue(k + NG);
+            }
 #pragma unroll
             for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::R1>(i, t) - t) * ldy] = x[i];
-        } else if constexpr (STORE) {
+            continue;
+        }
+        if constexpr (!EARLY) {
+            gsync();  // the forward transform's exchange reads of the slot are done
+            if (gtid == 0 && k + NG < K) issue(k + NG);
+        }
+        if constexpr (STORE) {
 #pragma unroll
             for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::RL>(i, t) - t) * ldy] = x[i];
         }
@@ -774,7 +801,7 @@ static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
     if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
         if (a.err) {
             constexpr size_t sm = CP::SMEM;
-            auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG>;
+            auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG, CP::EARLY_V>;
             static const int cap = max_ctas(kern, S::GT * S::NG, sm);
             const int items = (a.ny / CP::W) * a.nprobe;
             int grid = grid_ctas > 0 ? grid_ctas : cap;

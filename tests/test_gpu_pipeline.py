@@ -4,7 +4,10 @@ The engine runs its row and column passes either with kernels whose threads load
 straight from global memory, or with kernels that stage each item's lines in shared memory through
 the copy engine and keep the transmission rows resident; MTB_PIPE pins the choice (bit 0 rows,
 bit 1 columns), otherwise the engine's autotuner picks the faster per shape. All variants compute
-the same transforms with the same rounding, so their results must be bit-identical. Cases cover:
+the same transforms with the same rounding, so the waves are bit-identical; the FP64 detector sums
+are too where both variants use tiles of the same width, and agree to FP64 rounding (1e-13
+relative) where they do not (1024: 8-column tiles in the bulk-copy-fed pass, 16 in the other; the
+per-tile partials are then added in a different order). Cases cover:
 several line groups per CTA in the row pass (a change of transmission rows inside a CTA), probe
 counts that are and are not multiples of the row-pass unit, and the column pass's detector
 partials.
@@ -30,18 +33,23 @@ def _stem(p, pipe, monkeypatch):
 def test_stem_pipelined_matches_per_thread_kernels(nx, ns, monkeypatch):
     p = specimens.stem_srtio3(nx=nx, ny=nx, na=4, nb=4, nc=6, ns=ns, nconf=1, seed=3)
     ref = _stem(p, 0, monkeypatch)
+    exact = nx != 1024
     for pipe in (1, 2, 3):
         img = _stem(p, pipe, monkeypatch)
         assert img.shape == ref.shape
-        np.testing.assert_array_equal(img, ref, err_msg=f"MTB_PIPE={pipe}")
+        if exact:
+            np.testing.assert_array_equal(img, ref, err_msg=f"MTB_PIPE={pipe}")
+        else:
+            np.testing.assert_allclose(img, ref, rtol=1e-13, atol=0, err_msg=f"MTB_PIPE={pipe}")
     monkeypatch.delenv("MTB_PIPE")
     e = api.Engine(p)
     r = e.run()
     e.close()
-    np.testing.assert_array_equal(np.stack([np.stack(d["image_tot"]) for d in r["data"]]), ref)
+    np.testing.assert_allclose(np.stack([np.stack(d["image_tot"]) for d in r["data"]]), ref, rtol=0 if exact else 1e-13,
+                               atol=0)
 
 
-@pytest.mark.parametrize("nx", [128, 256, 512])
+@pytest.mark.parametrize("nx", [128, 256, 384, 512, 1024])
 def test_exit_wave_pipelined_matches_per_thread_kernels(nx, monkeypatch):
     p = specimens.hrtem_si001(nx=nx, ny=nx, na=4, nb=4, nc=6)
     out = {}
