@@ -57,7 +57,8 @@ enum ColFlags : int {
     COL_PROP = 2,      // multiply by Px[ix]*Py[iy]
     COL_DETECT = 4,    // ring sums of |psi_hat|^2 into partials
     COL_INVERSE = 8,   // inverse FFT_x before the store
-    COL_STORE = 16     // store the result
+    COL_STORE = 16,    // store the result
+    COL_P2 = 32        // with COL_PROP: also multiply by P2[ix][iy] (set from ColArgs::P2 by the launcher)
 };
 struct ProbeDev {
     float c_c_10, c_c_30, c_c_50;

@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
             const float2 py = a.Py[iy];
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], cmul(s_px[reg_pos<NX, G::RL>(i, t)], py));
-            if (a.P2) {
+            if constexpr (FLAGS & COL_P2) {
                 const float2* p2 = a.P2 + iy;
 #pragma unroll
                 for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(p2 + (size_t)reg_pos<NX, G::RL>(i, t) * a.g.ny));
@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             const float2 py = a.Py[iy];
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], cmul(s_px[reg_pos<NX, G::RL>(i, t)], py));
-            if (a.P2) {
+            if constexpr (FLAGS & COL_P2) {
                 const float2* p2 = a.P2 + iy;
 #pragma unroll
                 for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(p2 + (size_t)reg_pos<NX, G::RL>(i, t) * a.g.ny));
@@ -848,7 +848,13 @@ int cols_det_width() {
 
 template <int NX>
 void cols_dispatch_flags(int flags, const ColArgs& a, int grid_ctas, cudaStream_t s) {
+    // the [nx][ny] factor is a compile-time variant, so passes without it keep their registers
+    if (a.P2 && (flags & COL_PROP)) flags |= COL_P2;
     switch (flags) {
+        case COL_F_STEP | COL_P2: cols_launch<NX, COL_F_STEP | COL_P2>(a, grid_ctas, s); break;
+        case COL_F_STEP_DET | COL_P2: cols_launch<NX, COL_F_STEP_DET | COL_P2>(a, grid_ctas, s); break;
+        case COL_F_LAST_DET | COL_P2: cols_launch<NX, COL_F_LAST_DET | COL_P2>(a, grid_ctas, s); break;
+        case COL_F_FOURIER | COL_P2: cols_launch<NX, COL_F_FOURIER | COL_P2>(a, grid_ctas, s); break;
         case COL_F_PROBE: cols_launch<NX, COL_F_PROBE>(a, grid_ctas, s); break;
         case COL_F_STEP: cols_launch<NX, COL_F_STEP>(a, grid_ctas, s); break;
         case COL_F_STEP_DET: cols_launch<NX, COL_F_STEP_DET>(a, grid_ctas, s); break;
