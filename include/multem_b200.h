@@ -14,7 +14,7 @@
  * Conventions kept identical to the reference so a thin MATLAB/Python shim maps 1:1:
  *   - field names follow the MATLAB input class matlab_functions/+multem_input/parameters.m;
  *   - enum codes are the reference's (src/types.cuh:137-310), e.g. simulation_type 11 = STEM,
- *     52 = EWRS; potential_type 6 = Lobato; potential_slicing 1 = planes, 2 = dz_Proj;
+ *     52 = EWRS; potential_type 1-4, 6 (1 Doyle-Turner, 2/3 Peng, 4 Kirkland, 6 Lobato); potential_slicing 1 = planes, 2 = dz_Proj;
  *     pn_model 3 = frozen phonon; pn_dim 110 = x,y;
  *   - units are the MATLAB input's: lengths in Angstrom, E_0 in keV, theta/phi and lens azimuths in
  *     degrees, apertures and detector angles in mrad, c_30/c_50 in mm;
@@ -88,7 +88,8 @@ typedef struct mt_lens {
 typedef struct mt_input_multislice {
     int simulation_type;
     int interaction_model;       /* 1 multislice, 2 phase object, 3 weak phase object */
-    int potential_type;          /* 6 Lobato (0-12) */
+    int potential_type;          /* 1 Doyle-Turner (0-4), 2 Peng (0-4), 3 Peng (0-12), 4 Kirkland (0-12),
+                                    6 Lobato (0-12); 5 Weickenmeier-Kohl is refused */
     int operation_mode;
     int reverse_multislice;
 
@@ -299,13 +300,20 @@ mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice
  * projected-potential splat evaluates). Host buffers. */
 mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
                            double* heads, float* tab);
+/* mt_spline_tables for the parameterisation `potential_type` (MULTEM's ePotential_Type): 1 Doyle-Turner
+ * (0-4), 2 Peng (0-4), 3 Peng (0-12), 4 Kirkland (0-12) or 6 Lobato (0-12); the tables of
+ * Atomic_Data::get_atom_coef built with that type (src/atomic_data.hpp:1303-1400, 1547-1668).
+ * 5 (Weickenmeier-Kohl, no closed-form projected potential) returns MT_ERR_UNSUPPORTED.
+ * mt_spline_tables is this call with potential_type 6. */
+mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, int n, double dR_min,
+                              double Vrl, int nR, double* heads, float* tab);
 
 /* Allocation-free form of mt_spline_tables; it has no counterpart in the reference. It is for
  * callers that cannot call cudaMalloc: code running inside a CUDA stream capture, code whose GPU
  * memory is owned by a framework's pool allocator (a stray cudaMalloc would bypass the pool's budget
  * or fail), or real-time loops where an allocation is not allowed. The caller passes the output:
  * d_tab is a device buffer of n*5*nR floats on the current device, laid out as mt_spline_tables'
- * tab; heads (optional) is a host buffer of 4*n doubles. The only scratch is a fixed 26 KB device
+ * tab; heads (optional) is a host buffer of 4*n doubles. The only scratch is a fixed 32 KB device
  * array inside the library (held on every GPU that loads the library until the process exits):
  * n is limited to 128 elements and nR to 1024, larger requests return MT_ERR_INVALID_ARG. The work
  * is enqueued on `stream` (a cudaStream_t, NULL for the legacy default stream) and is complete when
@@ -315,6 +323,10 @@ mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, doub
  * the GPU (different streams or threads on one device) race on it. */
 mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
                                    float* d_tab, void* stream);
+/* mt_spline_tables_noalloc for `potential_type` (as mt_spline_tables_ex); mt_spline_tables_noalloc
+ * is this call with potential_type 6. */
+mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, int n, double dR_min, double Vrl, int nR,
+                                      double* heads, float* d_tab, void* stream);
 
 /* ---- specimen host logic, exposed for parity checks ---- */
 

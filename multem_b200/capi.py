@@ -128,6 +128,10 @@ SIGNATURES = {
                                  C.POINTER(C.c_float)]),
     "mt_spline_tables_noalloc": (c_int, [P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
                                          C.c_void_p]),
+    "mt_spline_tables_ex": (c_int, [C.POINTER(MtSystemConf), c_int, P_int, c_int, c_double, c_double, c_int,
+                                    P_double, C.POINTER(C.c_float)]),
+    "mt_spline_tables_noalloc_ex": (c_int, [c_int, P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
+                                            C.c_void_p]),
     # learned surrogate kernels (include/multem_b200_surrogate.h); tensors are device pointers
     "mt_sg_conv3x3_forward": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, c_int, _VP]),
     "mt_sg_conv3x3_backward_data": (c_int, [_VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),

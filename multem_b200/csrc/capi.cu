@@ -278,8 +278,15 @@ mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice
 
 mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
                            double* heads, float* tab) {
+    return mt_spline_tables_ex(conf, 6, Z, n, dR_min, Vrl, nR, heads, tab);
+}
+
+mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, int n, double dR_min,
+                              double Vrl, int nR, double* heads, float* tab) {
     return guarded([&] {
         if (!Z || n <= 0 || !tab || nR < 2) mtb::fail(MT_ERR_INVALID_ARG, "bad arguments");
+        if (!mtb::potential_type_supported(potential_type))
+            mtb::fail(MT_ERR_UNSUPPORTED, "potential_type must be 1-4 or 6");
         for (int i = 0; i < n; i++)
             if (Z[i] < 1 || Z[i] > 103) mtb::fail(MT_ERR_INVALID_ARG, "Z out of range 1..103");
         const int dev = conf ? conf->gpu_device : 0;
@@ -288,10 +295,10 @@ mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, doub
         MTB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         std::vector<int> zs(Z, Z + n);
         std::vector<mtb::TableHead> hd;
-        for (int z : zs) hd.push_back(mtb::element_head(z, (float)dR_min, (float)Vrl));
+        for (int z : zs) hd.push_back(mtb::element_head(z, potential_type, (float)dR_min, (float)Vrl));
         mtb::DevBuf<float> d_tab;
         d_tab.alloc((size_t)n * 5 * nR);
-        mtb::build_tables(zs, hd, nR, d_tab.p, s);
+        mtb::build_tables(zs, potential_type, hd, nR, d_tab.p, s);
         MTB_CUDA(cudaMemcpyAsync(tab, d_tab.p, sizeof(float) * (size_t)n * 5 * nR, cudaMemcpyDeviceToHost, s));
         MTB_CUDA(cudaStreamSynchronize(s));
         MTB_CUDA(cudaStreamDestroy(s));
@@ -307,15 +314,22 @@ mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, doub
 
 mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
                                    float* d_tab, void* stream) {
+    return mt_spline_tables_noalloc_ex(6, Z, n, dR_min, Vrl, nR, heads, d_tab, stream);
+}
+
+mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, int n, double dR_min, double Vrl, int nR,
+                                      double* heads, float* d_tab, void* stream) {
     return guarded([&] {
+        if (!mtb::potential_type_supported(potential_type))
+            mtb::fail(MT_ERR_UNSUPPORTED, "potential_type must be 1-4 or 6");
         if (!Z || !d_tab) mtb::fail(MT_ERR_INVALID_ARG, "Z and d_tab must not be NULL");
         if (n < 1) mtb::fail(MT_ERR_INVALID_ARG, "n must be positive");
         for (int i = 0; i < n; i++)
             if (Z[i] < 1 || Z[i] > 103) mtb::fail(MT_ERR_INVALID_ARG, "Z out of range 1..103");
         std::vector<int> zs(Z, Z + n);
         std::vector<mtb::TableHead> hd;
-        for (int z : zs) hd.push_back(mtb::element_head(z, (float)dR_min, (float)Vrl));
-        mtb::build_tables_noalloc(zs, hd, nR, d_tab, static_cast<cudaStream_t>(stream));
+        for (int z : zs) hd.push_back(mtb::element_head(z, potential_type, (float)dR_min, (float)Vrl));
+        mtb::build_tables_noalloc(zs, potential_type, hd, nR, d_tab, static_cast<cudaStream_t>(stream));
         if (heads)
             for (int i = 0; i < n; i++) {
                 heads[4 * i] = hd[i].R_min;
@@ -335,7 +349,8 @@ struct HostSpec {
         std::vector<float> rmax(103, 0.0f);
         for (int Zr : m.atoms_in.Z) {
             int Z = Zr % 1000;
-            if (rmax[Z - 1] == 0.0f) rmax[Z - 1] = (float)mtb::element_head(Z, m.grid.dR_min(), m.Vrl).R_max;
+            if (rmax[Z - 1] == 0.0f)
+                rmax[Z - 1] = (float)mtb::element_head(Z, m.potential_type, m.grid.dR_min(), m.Vrl).R_max;
         }
         spec.reset(new mtb::Specimen(m, rmax));
     }

@@ -231,8 +231,8 @@ void Engine::build_types() {
     if ((int)Z_of_type_.size() > kMaxTypes) fail(MT_ERR_UNSUPPORTED, "more than 16 elements in one specimen");
     d_tab_.alloc((size_t)Z_of_type_.size() * 5 * m_.nR);
     heads_.clear();
-    for (int Z : Z_of_type_) heads_.push_back(element_head(Z, m_.grid.dR_min(), m_.Vrl));
-    build_tables(Z_of_type_, heads_, m_.nR, d_tab_.p, stream_);
+    for (int Z : Z_of_type_) heads_.push_back(element_head(Z, m_.potential_type, m_.grid.dR_min(), m_.Vrl));
+    build_tables(Z_of_type_, m_.potential_type, heads_, m_.nR, d_tab_.p, stream_);
     R_max_f_.resize(Z_of_type_.size());
     for (size_t t = 0; t < Z_of_type_.size(); t++) R_max_f_[t] = (float)heads_[t].R_max;
     d_Rmax_.upload(R_max_f_.data(), R_max_f_.size(), stream_);

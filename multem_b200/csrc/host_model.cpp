@@ -13,6 +13,7 @@
 #include <string>
 
 #include "common.hpp"
+#include "tables.hpp"
 
 namespace mtb {
 
@@ -670,7 +671,11 @@ Model build_model(const mt_input_multislice* in) {
     if (m.interaction_model < 1 || m.interaction_model > 3)
         fail(MT_ERR_UNSUPPORTED, "interaction_model must be 1 (multislice), 2 (phase object) or 3 (weak phase object)");
     m.potential_type = in->potential_type;
-    if (m.potential_type != 6) fail(MT_ERR_UNSUPPORTED, "only potential_type 6 (Lobato 0-12) is implemented");
+    if (m.potential_type == 5)
+        fail(MT_ERR_UNSUPPORTED, "potential_type 5 (Weickenmeier-Kohl) has no closed-form projected potential; "
+                                 "use 1-4 or 6");
+    if (!potential_type_supported(m.potential_type))
+        fail(MT_ERR_INVALID_ARG, "potential_type must be 1-6, got " + std::to_string(m.potential_type));
     m.mul_sign = in->reverse_multislice ? -1 : 1;
     m.pn_model = in->pn_model;
     m.pn_coh_contrib = in->pn_coh_contrib != 0;

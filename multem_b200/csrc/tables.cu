@@ -1,20 +1,35 @@
-// FP64 build of the Lobato radial projected-potential spline tables on the GPU.
+// FP64 build of the radial projected-potential spline tables on the GPU.
 //
-// Follows Atomic_Data::get_atom_coef (src/atomic_data.hpp:1547-1668) for neutral atoms with the
-// Lobato (0-12) parameterisation (set_Lobato_neutral_coef, src/atomic_data.hpp:1441-1486):
-//   VR.cl = 2*Potf*pi^2*cl/cnl^1.5, VR.cnl = 2*pi/sqrt(cnl)        (projected potential)
-//   Vr.cl =   Potf*pi^2*cl/cnl^1.5, Vr.cnl = 2*pi/sqrt(cnl)        (3-D potential)
+// Follows Atomic_Data::get_atom_coef (src/atomic_data.hpp:1547-1668) for neutral atoms of the five
+// parameterisations with a closed-form projected potential (potential_type 1-4 and 6):
+//   6 Lobato (0-12), set_Lobato_neutral_coef (src/atomic_data.hpp:1441-1486):
+//     VR.cl = 2*Potf*pi^2*cl/cnl^1.5, VR.cnl = 2*pi/sqrt(cnl)        (projected potential)
+//     Vr.cl =   Potf*pi^2*cl/cnl^1.5, Vr.cnl = 2*pi/sqrt(cnl)        (3-D potential)
+//     VR(R) = sum_5 cl*(2*K0(cnl*R)/cnl + R*K1(cnl*R)), dVR/dR = -sum_5 cl*(cnl*R*K0 + 2*K1)
+//     (VR_dVR_Lobato_neutral_0_12, src/cgpu_fcns.cuh:1256-1268)
+//   1 Doyle-Turner (0-4, 4 Gaussians), 2 Peng (0-4, 5 Gaussians), 3 Peng (0-12, 5 Gaussians),
+//     set_Doyle_Peng_neutral_coef (src/atomic_data.hpp:1303-1348), with b = cnl/4:
+//     Vr.cl = Potf*cl*(pi/b)^1.5, VR.cl = Potf*pi*cl/b, Vr.cnl = VR.cnl = pi^2/b
+//     Vr(r) = sum cl*exp(-cnl*r^2), VR(R) = sum cl*exp(-cnl*R^2)   (add_Gauss_Fn,
+//     src/cgpu_fcns.cuh:491-520; Vr_/VR_Doyle/Peng_neutral_*, src/cgpu_fcns.cuh:1023-1063, 1162-1201)
+//   4 Kirkland (0-12, 3 Yukawa + 3 Gaussians), set_Kirkland_neutral_coef (src/atomic_data.hpp:1351-1400):
+//     Yukawa terms j < 3: Vr.cl = Potf*pi*cl, VR.cl = Potf*2*pi*cl, Vr.cnl = VR.cnl = 2*pi*sqrt(cnl)
+//     Gaussian terms j = 3..5: as above with b = cnl
+//     Vr(r) = sum_3 cl*exp(-cnl*r)/r + Gaussians (add_Yukawa_Fn, src/cgpu_fcns.cuh:557-570)
+//     VR(R) = sum_3 cl*K0(cnl*R) + Gaussians, dVR = -sum_3 cl*cnl*K1(cnl*R) + Gaussian derivatives
+//     (VR_dVR_Kirkland_neutral_0_12, src/cgpu_fcns.cuh:1203-1230)
+// Common to all types:
 //   R_min = max(dR_min, rn_c), rn_c = 1.2e-5*A^(1/3)
 //   R_max = root of Vr(r) = Vrl by bisection on [rn_c, 25] (Atom_Cal::AtomicRadius_Cutoff,
-//           src/atomic_fcns_mt.hpp:269-295; Root_Finder, src/cgpu_fcns.cuh:262-286),
-//           R_max = max(R_max, 2*R_min), or 1.75*ra when it is zero
+//           src/atomic_fcns_mt.hpp:269-295; Root_Finder, src/cgpu_fcns.cuh:262-286), or 0 when
+//           Vr.cl[0] is zero; R_max = max(R_max, 2*R_min), or 1.75*ra when it is zero
 //   R_tap = R_min + 0.85*(R_max - R_min), tap_cf = (pi/2)/(R_max^2 - R_tap^2)
 //   nR log-spaced knots R_i = R_min*exp(i*ln(R_max/R_min)/(nR-1)), spline variable R^2
-//   VR(R) = sum_5 cl*(2*K0(cnl*R)/cnl + R*K1(cnl*R)), dVR/dR = -sum_5 cl*(cnl*R*K0 + 2*K1)
-//           (VR_dVR_Lobato_neutral_0_12, src/cgpu_fcns.cuh:1256-1268)
 //   c0 = VR, c1 = dVR/d(R^2) = 0.5*dVR/R, both cosine-tapered beyond R_tap^2 (apply_tapering,
 //   src/cgpu_fcns.cuh:1530-1540); c2, c3 from the Hermite conditions between knots
 //   (src/atomic_data.hpp:1652-1663).
+// Weickenmeier-Kohl (type 5) has no closed-form projected potential (the reference integrates Vr
+// numerically along z) and is refused by the input validation.
 // The modified Bessel functions K0, K1 use the polynomial approximations of Abramowitz & Stegun,
 // Handbook of Mathematical Functions, 9.8.1-9.8.8 (I0, I1 for x <= 3.75; K0, K1 for x <= 2 and
 // x > 2), the same published approximations the reference uses (src/math.cuh:465-630).
@@ -38,14 +53,20 @@ namespace {
 #include "atomic_params.inc"
 
 constexpr double kPotf = 47.877645145863056;
+constexpr double kPi = 3.141592653589793238463;
 constexpr double kPi2 = 9.869604401089358618834;
 constexpr double k2Pi = 6.283185307179586476925;
 constexpr double kHalfPi = 1.570796326794896619231;
 
 struct ElemCoef {
-    double VRcl[5], VRcnl[5], Vrcl[5], Vrcnl[5];
+    double VRcl[6], VRcnl[6], Vrcl[6], Vrcnl[6];  // unused terms: cl = 0, cnl = 1
     double rn_c, ra;
+    int type;  // potential_type
 };
+
+// Gaussian terms of each parameterisation: [g0, g1); Kirkland's Yukawa terms are [0, 3)
+__host__ __device__ inline int gauss_first(int type) { return type == 4 ? 3 : 0; }
+__host__ __device__ inline int gauss_end(int type) { return type == 1 ? 4 : (type == 4 ? 6 : 5); }
 
 __device__ double as_i0(double x) {  // A&S 9.8.1 / 9.8.2
     double ax = fabs(x), y;
@@ -115,11 +136,24 @@ __global__ void build_tables_kernel(const ElemCoef* __restrict__ coef, const Tab
         double R = R_min * exp(iR * dlnr);
         double r2 = pow(R, 2);
         double y = 0, dy = 0;
-        for (int i = 0; i < 5; i++) {
-            double k0 = as_k0(c.VRcnl[i] * R);
-            double k1 = as_k1(c.VRcnl[i] * R);
-            y += c.VRcl[i] * (2 * k0 / c.VRcnl[i] + R * k1);
-            dy += -c.VRcl[i] * (c.VRcnl[i] * R * k0 + 2 * k1);
+        if (c.type == 6) {
+            for (int i = 0; i < 5; i++) {
+                double k0 = as_k0(c.VRcnl[i] * R);
+                double k1 = as_k1(c.VRcnl[i] * R);
+                y += c.VRcl[i] * (2 * k0 / c.VRcnl[i] + R * k1);
+                dy += -c.VRcl[i] * (c.VRcnl[i] * R * k0 + 2 * k1);
+            }
+        } else {
+            if (c.type == 4)
+                for (int i = 0; i < 3; i++) {
+                    y += c.VRcl[i] * as_k0(c.VRcnl[i] * R);
+                    dy += -c.VRcl[i] * c.VRcnl[i] * as_k1(c.VRcnl[i] * R);
+                }
+            for (int i = gauss_first(c.type); i < gauss_end(c.type); i++) {
+                double yt = c.VRcl[i] * exp(-c.VRcnl[i] * (R * R));
+                y += yt;
+                dy += -2 * c.VRcnl[i] * R * yt;
+            }
         }
         dy = 0.5 * dy / R;
         if (x_tap < r2) {
@@ -151,44 +185,72 @@ __global__ void build_tables_kernel(const ElemCoef* __restrict__ coef, const Tab
     }
 }
 
-// set_Lobato_neutral_coef (src/atomic_data.hpp:1441-1486) and the rn_c of To_atom_type_CPU
-// (src/atomic_data.hpp:148-176)
-ElemCoef element_coef(int Z) {
+// Coefficients of element Z for potential_type `type` (set_*_neutral_coef,
+// src/atomic_data.hpp:1303-1486) and the rn_c of To_atom_type_CPU (src/atomic_data.hpp:148-176)
+ElemCoef element_coef(int Z, int type) {
     ElemCoef e{};
-    int iZ = Z - 1;
-    for (int j = 0; j < 5; j++) {
-        double cl = kLobatoCl[iZ][j];
-        double cnl = (std::fabs(cl) <= 1e-13) ? 0.0 : kLobatoCnl[iZ][j];
-        bool nz = !((std::fabs(cl) <= 1e-13) || (std::fabs(cnl) <= 1e-13));
-        if (nz) {
-            e.Vrcl[j] = kPotf * kPi2 * cl / std::pow(cnl, 1.5);
-            e.Vrcnl[j] = k2Pi / std::sqrt(cnl);
-            e.VRcl[j] = 2.0 * kPotf * kPi2 * cl / std::pow(cnl, 1.5);
-            e.VRcnl[j] = k2Pi / std::sqrt(cnl);
-        } else {
-            e.Vrcl[j] = 0.0;
-            e.Vrcnl[j] = 1.0;
-            e.VRcl[j] = 0.0;
-            e.VRcnl[j] = 1.0;
+    const int iZ = Z - 1;
+    for (int j = 0; j < 6; j++) {
+        e.Vrcl[j] = e.VRcl[j] = 0.0;
+        e.Vrcnl[j] = e.VRcnl[j] = 1.0;
+    }
+    auto zero = [](double v) { return std::fabs(v) <= 1e-13; };
+    if (type == 6) {
+        for (int j = 0; j < 5; j++) {
+            double cl = kLobatoCl[iZ][j];
+            double cnl = zero(cl) ? 0.0 : kLobatoCnl[iZ][j];
+            if (!zero(cl) && !zero(cnl)) {
+                e.Vrcl[j] = kPotf * kPi2 * cl / std::pow(cnl, 1.5);
+                e.Vrcnl[j] = k2Pi / std::sqrt(cnl);
+                e.VRcl[j] = 2.0 * kPotf * kPi2 * cl / std::pow(cnl, 1.5);
+                e.VRcnl[j] = k2Pi / std::sqrt(cnl);
+            }
+        }
+    } else {
+        const double* fcl = kFegCl[type - 1][iZ];
+        const double* fcnl = kFegCnl[type - 1][iZ];
+        for (int j = 0; j < gauss_end(type); j++) {
+            double cl = fcl[j];
+            double cnl = zero(cl) ? 0.0 : (type == 4 ? fcnl[j] : fcnl[j] / 4.0);
+            if (zero(cl) || zero(cnl)) continue;
+            if (j < gauss_first(type)) {  // Kirkland's Yukawa terms
+                e.Vrcl[j] = kPotf * kPi * cl;
+                e.VRcl[j] = kPotf * k2Pi * cl;
+                e.Vrcnl[j] = e.VRcnl[j] = k2Pi * std::sqrt(cnl);
+            } else {
+                e.Vrcl[j] = kPotf * cl * std::pow(kPi / cnl, 1.5);
+                e.VRcl[j] = kPotf * kPi * cl / cnl;
+                e.Vrcnl[j] = e.VRcnl[j] = kPi2 / cnl;
+            }
         }
     }
     e.rn_c = 1.2e-05 * std::pow((double)kMassNumber[iZ], 1.0 / 3.0);
     e.ra = kAtomicRadius[iZ];
+    e.type = type;
     return e;
 }
 
 }  // namespace
 
-// 3-D potential of the Lobato parameterisation (Vr_Lobato_neutral_0_12,
-// src/cgpu_fcns.cuh:1111-1120)
-static double lobato_vr_host(double x, const ElemCoef& c) {
+// 3-D potential Vr(r) of the element (Vr_Lobato_neutral_0_12, src/cgpu_fcns.cuh:1111-1120; the
+// Gaussian and Yukawa sums of Vr_Doyle/Peng/Kirkland_neutral_*, src/cgpu_fcns.cuh:1023-1070)
+static double vr_host(double x, const ElemCoef& c) {
     double ix = 1.0 / x, y = 0;
-    for (int i = 0; i < 5; i++) y += c.Vrcl[i] * std::exp(-c.Vrcnl[i] * x) * ix * (2.0 / c.Vrcnl[i] + x);
+    if (c.type == 6) {
+        for (int i = 0; i < 5; i++) y += c.Vrcl[i] * std::exp(-c.Vrcnl[i] * x) * ix * (2.0 / c.Vrcnl[i] + x);
+        return y;
+    }
+    if (c.type == 4)
+        for (int i = 0; i < 3; i++) y += c.Vrcl[i] * std::exp(-c.Vrcnl[i] * x) * ix;
+    for (int i = gauss_first(c.type); i < gauss_end(c.type); i++) y += c.Vrcl[i] * std::exp(-c.Vrcnl[i] * (x * x));
     return y;
 }
 
-TableHead element_head(int Z, float dR_min, float Vrl_f) {
-    const ElemCoef c = element_coef(Z);
+bool potential_type_supported(int type) { return (type >= 1 && type <= 4) || type == 6; }
+
+TableHead element_head(int Z, int type, float dR_min, float Vrl_f) {
+    if (!potential_type_supported(type)) fail(MT_ERR_UNSUPPORTED, "potential_type " + std::to_string(type) + " has no table build");
+    const ElemCoef c = element_coef(Z, type);
     const double Vrl = (double)Vrl_f;
     const double R_min = std::fmax(c.rn_c, (double)dR_min);
     double R_max = 0;
@@ -196,11 +258,11 @@ TableHead element_head(int Z, float dR_min, float Vrl_f) {
     if (nonzero) {
         // Root_Finder (src/cgpu_fcns.cuh:262-286): bisection on [rn_c, 25], |f| <= 1e-8 or 200 steps
         double x0 = c.rn_c, xe = 25.0, x = 0, fx;
-        double fxe = lobato_vr_host(xe, c) - Vrl;
+        double fxe = vr_host(xe, c) - Vrl;
         int it = 0;
         do {
             x = 0.5 * (x0 + xe);
-            fx = lobato_vr_host(x, c) - Vrl;
+            fx = vr_host(x, c) - Vrl;
             if (fx * fxe < 0) {
                 x0 = x;
             } else {
@@ -218,11 +280,11 @@ TableHead element_head(int Z, float dR_min, float Vrl_f) {
     return TableHead{R_min, R_max, R_tap, tap_cf};
 }
 
-void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
+void build_tables(const std::vector<int>& Zs, int type, const std::vector<TableHead>& heads, int nR, float* d_tab,
                   cudaStream_t stream) {
     const int n = (int)Zs.size();
     std::vector<ElemCoef> h(n);
-    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i]);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type);
     int dev = 0;
     auto* d_coef = static_cast<ElemCoef*>(dev_alloc(sizeof(ElemCoef) * n, &dev));
     auto* d_head = static_cast<TableHead*>(dev_alloc(sizeof(TableHead) * n, &dev));
@@ -240,7 +302,7 @@ void build_tables(const std::vector<int>& Zs, const std::vector<TableHead>& head
 //
 // The per-call scratch of build_tables (the element coefficients and table heads the kernel reads)
 // lives here in one file-scope device array instead of memory allocated from the device pool. The
-// array is kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead)) bytes (about 26 KB) and is
+// array is kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead)) bytes (about 32 KB) and is
 // held by every GPU that loads this library until the process exits. All calls share it: each
 // call overwrites the entries it uses before its kernel reads them (nothing has to start at zero),
 // and two calls whose copies and kernels overlap on the GPU (different streams, or different host
@@ -267,8 +329,8 @@ static unsigned char* noalloc_scratch_address(int dev) {
     return addr[dev];
 }
 
-void build_tables_noalloc(const std::vector<int>& Zs, const std::vector<TableHead>& heads, int nR, float* d_tab,
-                          cudaStream_t stream) {
+void build_tables_noalloc(const std::vector<int>& Zs, int type, const std::vector<TableHead>& heads, int nR,
+                          float* d_tab, cudaStream_t stream) {
     const int n = (int)Zs.size();
     if (n < 1 || n > kNoAllocMaxElements)
         fail(MT_ERR_INVALID_ARG, "allocation-free table build takes 1.." + std::to_string(kNoAllocMaxElements) +
@@ -280,7 +342,7 @@ void build_tables_noalloc(const std::vector<int>& Zs, const std::vector<TableHea
     ElemCoef* d_coef = reinterpret_cast<ElemCoef*>(base);
     TableHead* d_head = reinterpret_cast<TableHead*>(base + kNoAllocMaxElements * sizeof(ElemCoef));
     std::vector<ElemCoef> h(n);
-    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i]);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type);
     // pageable sources: each copy returns once its source has been staged, so the vectors may go
     MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
     MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));

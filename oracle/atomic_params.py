@@ -1,4 +1,5 @@
-"""Lobato (0-12) coefficients, mass numbers and atomic radii for Z = 1..103, read from the data file
+"""Lobato (0-12) coefficients, the Doyle-Turner / Peng / Kirkland coefficients (FEG_CL[t - 1], FEG_CNL[t - 1]
+for potential_type t = 1..4), mass numbers and atomic radii for Z = 1..103, read from the data file
 the engine compiles in (multem_b200/csrc/atomic_params.inc, extracted from the reference's
 src/atomic_data.hpp by multem_b200/csrc/gen_atomic_params.py). Test infrastructure only."""
 import re
@@ -19,7 +20,13 @@ def _parse():
         body = re.search(name + r"\[103\] = \{([^}]*)\}", s).group(1)
         return [cast(v) for v in body.split(",")]
 
-    return table("kLobatoCl"), table("kLobatoCnl"), vec("kMassNumber", int), vec("kAtomicRadius", float)
+    def feg(name):
+        body = re.search(name + r"\[4\]\[103\]\[6\] = \{(.*?)\n\};", s, re.S).group(1)
+        rows = [[float(v) for v in r.split(",")] for r in re.findall(r"\{([^{}]*)\}", body)]
+        return [rows[103 * t:103 * (t + 1)] for t in range(4)]
+
+    return (table("kLobatoCl"), table("kLobatoCnl"), vec("kMassNumber", int), vec("kAtomicRadius", float),
+            feg("kFegCl"), feg("kFegCnl"))
 
 
-LOBATO_CL, LOBATO_CNL, MASS_NUMBER, ATOMIC_RADIUS = _parse()
+LOBATO_CL, LOBATO_CNL, MASS_NUMBER, ATOMIC_RADIUS, FEG_CL, FEG_CNL = _parse()

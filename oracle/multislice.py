@@ -2,7 +2,7 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and only as the
 checker. It restates, in numpy, the reference's algorithm for:
-  * the Lobato spline tables       Atomic_Data::get_atom_coef       src/atomic_data.hpp:1547-1668
+  * the spline tables              Atomic_Data::get_atom_coef       src/atomic_data.hpp:1303-1486, 1547-1668
   * the projected-potential splat  eval_cubic_poly / get_bn         src/cpu_fcns.hpp:234-262,1670-1684
   * the transmission function      functor::transmission_function   src/cgpu_fcns.cuh:3072-3086
   * the Fresnel propagator         Propagator::operator()           src/propagator.cuh:34-69
@@ -78,7 +78,7 @@ def bessel_k1(x):
 
 
 # ---------------------------------------------------------------------------------------------
-# Lobato spline tables (src/atomic_data.hpp:1441-1486, 1547-1668)
+# Spline tables (src/atomic_data.hpp:1303-1486, 1547-1668)
 
 def lobato_coef(Z):
     cl = np.array(atomic_params.LOBATO_CL[Z - 1], dtype=np.float64)
@@ -96,9 +96,69 @@ def vr_lobato(x, cl, cnl):
     return sum(cl[i] * math.exp(-cnl[i] * x) / x * (2.0 / cnl[i] + x) for i in range(5))
 
 
-def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128):
+def _gauss_range(pt):
+    """Gaussian terms [g0, g1) of potential_type 1-4 (Kirkland's first three terms are Yukawa)."""
+    return (3, 6) if pt == 4 else (0, 4 if pt == 1 else 5)
+
+
+def feg_coef(Z, pt):
+    """Vr and VR coefficients of potential_type 1-4: set_Doyle_Peng_neutral_coef and
+    set_Kirkland_neutral_coef (src/atomic_data.hpp:1303-1400); unused terms are (0, 1)."""
+    Vr_cl, VR_cl = np.zeros(6), np.zeros(6)
+    cnl_out = np.ones(6)
+    g0, g1 = _gauss_range(pt)
+    for j in range(g1):
+        cl = atomic_params.FEG_CL[pt - 1][Z - 1][j]
+        cnl = 0.0 if abs(cl) <= 1e-13 else atomic_params.FEG_CNL[pt - 1][Z - 1][j] / (1.0 if pt == 4 else 4.0)
+        if abs(cl) <= 1e-13 or abs(cnl) <= 1e-13:
+            continue
+        if j < g0:  # Yukawa
+            Vr_cl[j], VR_cl[j], cnl_out[j] = C_POTF * C_PI * cl, C_POTF * C_2PI * cl, C_2PI * math.sqrt(cnl)
+        else:
+            Vr_cl[j] = C_POTF * cl * (C_PI / cnl) ** 1.5
+            VR_cl[j] = C_POTF * C_PI * cl / cnl
+            cnl_out[j] = C_PI2 / cnl
+    return Vr_cl, cnl_out, VR_cl, cnl_out.copy()
+
+
+def vr_feg(x, cl, cnl, pt):
+    """Vr of potential_type 1-4 (Vr_Doyle/Peng/Kirkland_neutral_*, src/cgpu_fcns.cuh:1023-1070)."""
+    g0, g1 = _gauss_range(pt)
+    y = sum(cl[i] * math.exp(-cnl[i] * x) / x for i in range(g0))
+    return y + sum(cl[i] * math.exp(-cnl[i] * (x * x)) for i in range(g0, g1))
+
+
+def vr_dvr_projected(R, VR_cl, VR_cnl, pt):
+    """VR(R) and dVR/dR (VR_dVR_*_neutral_*, src/cgpu_fcns.cuh:1162-1268)."""
+    y = np.zeros_like(R)
+    dy = np.zeros_like(R)
+    if pt == 6:
+        for i in range(5):
+            k0 = bessel_k0(VR_cnl[i] * R)
+            k1 = bessel_k1(VR_cnl[i] * R)
+            y += VR_cl[i] * (2 * k0 / VR_cnl[i] + R * k1)
+            dy += -VR_cl[i] * (VR_cnl[i] * R * k0 + 2 * k1)
+        return y, dy
+    g0, g1 = _gauss_range(pt)
+    for i in range(g0):
+        y += VR_cl[i] * bessel_k0(VR_cnl[i] * R)
+        dy += -VR_cl[i] * VR_cnl[i] * bessel_k1(VR_cnl[i] * R)
+    for i in range(g0, g1):
+        yt = VR_cl[i] * np.exp(-VR_cnl[i] * (R * R))
+        y += yt
+        dy += -2 * VR_cnl[i] * R * yt
+    return y, dy
+
+
+def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128, potential_type=6):
     """Spline table of element Z: dict with R_min, R_max, R_tap, tap_cf (float64) and R2, c0..c3."""
-    Vr_cl, Vr_cnl, VR_cl, VR_cnl = lobato_coef(Z)
+    pt = potential_type
+    if pt == 6:
+        Vr_cl, Vr_cnl, VR_cl, VR_cnl = lobato_coef(Z)
+        vr = lambda x: vr_lobato(x, Vr_cl, Vr_cnl)  # noqa: E731
+    else:
+        Vr_cl, Vr_cnl, VR_cl, VR_cnl = feg_coef(Z, pt)
+        vr = lambda x: vr_feg(x, Vr_cl, Vr_cnl, pt)  # noqa: E731
     A = atomic_params.MASS_NUMBER[Z - 1]
     rn_c = 1.2e-05 * A ** (1.0 / 3.0)
     Vrl = float(Vrl)
@@ -106,11 +166,11 @@ def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128):
     R_max = 0.0
     if abs(Vrl) > 1e-13 and abs(Vr_cl[0]) > 1e-13:
         x0, xe = rn_c, 25.0
-        fxe = vr_lobato(xe, Vr_cl, Vr_cnl) - Vrl
+        fxe = vr(xe) - Vrl
         it = 0
         while True:
             x = 0.5 * (x0 + xe)
-            fx = vr_lobato(x, Vr_cl, Vr_cnl) - Vrl
+            fx = vr(x) - Vrl
             if fx * fxe < 0:
                 x0 = x
             else:
@@ -127,13 +187,7 @@ def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128):
     dlnr = math.log(R_max / R_min) / (nR - 1)
     R = R_min * np.exp(np.arange(nR) * dlnr)
     R2 = R ** 2
-    y = np.zeros(nR)
-    dy = np.zeros(nR)
-    for i in range(5):
-        k0 = bessel_k0(VR_cnl[i] * R)
-        k1 = bessel_k1(VR_cnl[i] * R)
-        y += VR_cl[i] * (2 * k0 / VR_cnl[i] + R * k1)
-        dy += -VR_cl[i] * (VR_cnl[i] * R * k0 + 2 * k1)
+    y, dy = vr_dvr_projected(R, VR_cl, VR_cnl, pt)
     dy = 0.5 * dy / R
     x_tap = R_tap ** 2
     t = x_tap < R2

@@ -427,3 +427,48 @@ def hrtem_bwl_si001():
     p = _hrtem(1)
     p.bwl = 1
     return p
+
+
+def _ew_potential(pt, seed):
+    from multem_b200 import specimens
+    p = specimens.hrtem_si001(nx=256, ny=256, na=4, nb=4, nc=4)
+    p.potential_type = pt
+    p.pn_nconf = 2
+    p.pn_seed = seed
+    return p
+
+
+def ew_doyle_si001():
+    """Exit wave (EWRS) of Si(001), 256^2 grid, two phonon configurations, with the Doyle-Turner
+    (0-4) parameterisation (potential_type 1)."""
+    return _ew_potential(1, 21)
+
+
+def ew_peng4_si001():
+    """As ew_doyle_si001 with the Peng (0-4) parameterisation (potential_type 2)."""
+    return _ew_potential(2, 22)
+
+
+def ew_kirkland_si001():
+    """As ew_doyle_si001 with the Kirkland (0-12) parameterisation (potential_type 4)."""
+    return _ew_potential(4, 24)
+
+
+def _stem_potential(pt, seed):
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nx=256, ny=256, na=4, nb=4, nc=4, ns=3, nconf=2, seed=seed)
+    p.potential_type = pt
+    p.thick_type = 2
+    p.thick = [8.0, 15.0]
+    return p
+
+
+def stem_peng12_srtio3():
+    """STEM ADF through SrTiO3(001), 256^2 grid, 3 x 3 probes, two thicknesses, two phonon
+    configurations, with the Peng (0-12) parameterisation (potential_type 3)."""
+    return _stem_potential(3, 23)
+
+
+def stem_kirkland_srtio3():
+    """As stem_peng12_srtio3 with the Kirkland (0-12) parameterisation (potential_type 4)."""
+    return _stem_potential(4, 25)

@@ -26,7 +26,8 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    stem_coh_srtio3, ed_si001, hrtem_coherent_si001, hrtem_pctf_si001, hrtem_fullint_si001,
                    cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001,
                    ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3, ew_monolayer_au,
-                   stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001)
+                   stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001,
+                   ew_doyle_si001, ew_peng4_si001, ew_kirkland_si001, stem_peng12_srtio3, stem_kirkland_srtio3)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -65,7 +66,9 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("ped_si001", ped_si001), ("hctem_si001", hctem_si001), ("istem_srtio3", istem_srtio3),
              ("ew_monolayer_au", ew_monolayer_au), ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001),
              ("ew_wpo_si001", ew_wpo_si001), ("ew_bwl_si001", ew_bwl_si001), ("stem_bwl_srtio3", stem_bwl_srtio3),
-             ("hrtem_bwl_si001", hrtem_bwl_si001))
+             ("hrtem_bwl_si001", hrtem_bwl_si001), ("ew_doyle_si001", ew_doyle_si001), ("ew_peng4_si001", ew_peng4_si001),
+             ("ew_kirkland_si001", ew_kirkland_si001), ("stem_peng12_srtio3", stem_peng12_srtio3),
+             ("stem_kirkland_srtio3", stem_kirkland_srtio3))
 
 SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
              ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))
@@ -99,13 +102,29 @@ def full_runs(rec, names=None):
                     rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
 
 
+def potential_table_fixtures(rec):
+    """Spline tables of potential_type 1-4 (Doyle-Turner, Peng 0-4, Peng 0-12, Kirkland) for O, Ti, Sr
+    at the small STEM grid's sampling and for Si at the small exit-wave grid's."""
+    for pt in (1, 2, 3, 4):
+        for fn, Zs in ((stem_small, (8, 22, 38)), (ew_small, (14,))):
+            p = fn()
+            p.potential_type = pt
+            for Z in Zs:
+                t = R.atom_type(p, Z, 1)
+                rec[f"tab_pt{pt}_Z{Z}_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
+                rec[f"tab_pt{pt}_Z{Z}_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
+
+
 def add_only(names):
-    """Adds the full runs of `names` to the existing fixture file (other arrays kept)."""
+    """Adds the full runs of `names` to the existing fixture file (other arrays kept); the name
+    potential_tables adds potential_table_fixtures."""
     path = OUT / "reference_fixtures.npz"
     old = np.load(path)
     rec = {k: old[k] for k in old.files}
     full_runs(rec, names)
     specimen_fixtures(rec, names)
+    if "potential_tables" in names:
+        potential_table_fixtures(rec)
     np.savez_compressed(path, **rec)
     print("wrote", path, len(rec), "arrays")
 
@@ -140,6 +159,7 @@ def main():
         t = R.atom_type(q, 14, prec)
         rec[f"tab_Z14_p{prec}_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
         rec[f"tab_Z14_p{prec}_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
+    potential_table_fixtures(rec)
     # projected potential and transmission of one slice
     for prec in (1, 2):
         rec[f"stem_small_V_c1_s3_p{prec}"] = R.projected_potential(p, 1, 3, prec).astype(np.float64)

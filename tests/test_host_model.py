@@ -73,8 +73,8 @@ def test_configurations_differ_and_repeat():
 
 
 @pytest.mark.parametrize("field,value,status", [
-    ("simulation_type", 62, 6), ("simulation_type", 61, 6), ("potential_type", 5, 6), ("potential_slicing", 3, 6),
-    ("nx", 0, 1),
+    ("simulation_type", 62, 6), ("simulation_type", 61, 6), ("potential_type", 5, 6), ("potential_type", 7, 1),
+    ("potential_slicing", 3, 6), ("nx", 0, 1),
 ])
 def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
     from multem_b200 import capi

@@ -31,6 +31,24 @@ def test_spline_tables_si(golden):
         np.testing.assert_array_equal(np.float32(t[k]), golden["tab_Z14_p1_tab"][i].astype(np.float32))
 
 
+@pytest.mark.parametrize("pt", [1, 2, 3, 4])
+def test_spline_tables_other_parameterisations(golden, pt):
+    """Doyle-Turner, Peng (0-4, 0-12) and Kirkland tables: bit-exact in float except at the last knot,
+    where the cosine taper leaves rounding noise around zero (|c0| ~ 1e-17)."""
+    cases = ((small_stem(), (8, 22, 38)), (specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2), (14,)))
+    for p, Zs in cases:
+        grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)
+        for Z in Zs:
+            t = O.atom_table(Z, grid.dRx, potential_type=pt)
+            assert np.float32(t["R_max"]) == np.float32(golden[f"tab_pt{pt}_Z{Z}_head"][1])
+            ref = golden[f"tab_pt{pt}_Z{Z}_tab"].astype(np.float32)
+            for i, k in enumerate(("R2", "c0", "c1", "c2", "c3")):
+                got = np.float32(t[k])
+                tiny = np.abs(ref[i]) < 1e-12 * np.abs(ref[i]).max()
+                np.testing.assert_array_equal(got[~tiny], ref[i][~tiny])
+                assert np.all(np.abs(got[tiny]) < 1e-12 * np.abs(ref[i]).max())
+
+
 def test_projected_potential_float_bit_exact(golden):
     p = small_stem()
     grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)

@@ -2,9 +2,9 @@
 
 It serves callers that cannot call cudaMalloc (inside a stream capture, under a framework's GPU
 memory pool, in allocation-free real-time loops): they pass their own device output buffer, and the
-library's only scratch is a fixed device array. This test calls it through the C ABI twice in a row,
-on different element lists, and checks each result against the allocating mt_spline_tables with the
-tolerance the table-parity test uses. The file is named to be collected last.
+library's only scratch is a fixed device array. This test calls it (and mt_spline_tables_noalloc_ex
+for other parameterisations) through the C ABI several times in a row, on different element lists,
+and checks each result against the allocating entry with the tolerance the table-parity test uses. The file is named to be collected last.
 """
 import ctypes as C
 
@@ -18,14 +18,14 @@ pytestmark = pytest.mark.gpu
 RTOL = 2e-6
 
 
-def _noalloc(lib, Z, dR, nR, torch):
+def _noalloc(lib, Z, dR, nR, torch, pt=6):
     z = np.ascontiguousarray(np.asarray(Z, dtype=np.int32))
     d_tab = torch.full((z.size * 5 * nR,), float("nan"), dtype=torch.float32, device="cuda")
     heads = np.zeros((z.size, 4))
     stream = torch.cuda.current_stream()
-    rc = lib.mt_spline_tables_noalloc(z.ctypes.data_as(capi.P_int), z.size, float(dR), 0.015, nR,
-                                      heads.ctypes.data_as(capi.P_double), C.c_void_p(d_tab.data_ptr()),
-                                      C.c_void_p(stream.cuda_stream))
+    args = (z.ctypes.data_as(capi.P_int), z.size, float(dR), 0.015, nR, heads.ctypes.data_as(capi.P_double),
+            C.c_void_p(d_tab.data_ptr()), C.c_void_p(stream.cuda_stream))
+    rc = lib.mt_spline_tables_noalloc(*args) if pt == 6 else lib.mt_spline_tables_noalloc_ex(pt, *args)
     capi.check(rc)
     stream.synchronize()
     return heads, d_tab.cpu().numpy().reshape(z.size, 5, nR)
@@ -35,9 +35,9 @@ def test_noalloc_tables_match_allocating_entry_on_two_calls():
     torch = pytest.importorskip("torch")
     lib = capi.load()
     dR = np.float32(np.float32(15.62) / np.float32(128))
-    for Z in ([8, 22, 38], [14, 79, 6, 1, 78]):
-        heads_ref, tab_ref = api.spline_tables(Z, float(dR))
-        heads, tab = _noalloc(lib, Z, dR, 128, torch)
+    for Z, pt in (([8, 22, 38], 6), ([14, 79, 6, 1, 78], 6), ([14, 79, 6, 1, 78], 4), ([8, 22, 38], 3)):
+        heads_ref, tab_ref = api.spline_tables(Z, float(dR), potential_type=pt)
+        heads, tab = _noalloc(lib, Z, dR, 128, torch, pt)
         np.testing.assert_array_equal(heads, heads_ref)
         assert np.all(np.isfinite(tab))
         for i in range(len(Z)):
