@@ -99,6 +99,12 @@ typedef struct mt_input_multislice {
     int pn_nconf;
     int pn_dim;                  /* 110, 111, ... */
     int pn_seed;
+    /* phonon generator (no counterpart in the reference): 0 = the reference's own draws on the host
+     * (mt19937_64 + std::normal_distribution, the configurations MULTEM simulates; default),
+     * 1 = counter-based draws on the GPU (Philox4x32-10 + Box-Muller from pn_seed, configuration and
+     * atom index: the same displacement statistics, different configurations, no host work per
+     * configuration) */
+    int pn_rng;
 
     const double* spec_atoms;    /* column-major spec_atoms_rows x spec_atoms_cols */
     int spec_atoms_rows;
@@ -337,8 +343,18 @@ mt_status mt_specimen_info(const mt_input_multislice* in, int iconf, int* n_atom
  * Z[n], xyz[3n] as (x, y, z) triples, in the working precision of the engine (float) widened to
  * double. */
 mt_status mt_specimen_atoms(const mt_input_multislice* in, int iconf, int* Z, double* xyz, int n);
+/* The atoms of configuration `iconf` as the engine simulates them, in mt_specimen_atoms' layout:
+ * with pn_rng 0 the same as mt_specimen_atoms (no GPU); with pn_rng 1 the undisplaced atoms moved
+ * in x and y by the device generator (a GPU call on conf->gpu_device). No counterpart in the
+ * reference. */
+mt_status mt_phonon_atoms(const mt_system_conf* conf, const mt_input_multislice* in, int iconf, int* Z,
+                          double* xyz, int n);
+/* Philox4x32-10 on the device, the generator of pn_rng 1: out[4i..4i+3] from counter ctr[4i..4i+3]
+ * and key key[2i..2i+1], for checks against the published known-answer vectors. */
+mt_status mt_philox4x32_10(const unsigned* ctr, const unsigned* key, int n, unsigned* out);
 /* Slices of configuration `iconf` (Slicing::calculate, src/slicing.hpp:93-100):
- * z_0, z_e, iatom_0, iatom_e, ithk per slice. */
+ * z_0, z_e, iatom_0, iatom_e, ithk per slice. With pn_rng 1, the slicing of the undisplaced atoms,
+ * which every device-generated configuration uses. */
 mt_status mt_specimen_slices(const mt_input_multislice* in, int iconf, double* z_0, double* z_e,
                              int* iatom_0, int* iatom_e, int* ithk, int n);
 

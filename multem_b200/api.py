@@ -276,6 +276,32 @@ def specimen_atoms(params: Parameters, iconf: int):
     return Z, xyz.reshape(-1, 3)
 
 
+def phonon_atoms(params: Parameters, iconf: int, system_conf=None):
+    """Atoms of configuration iconf as the engine simulates them: the host draws of the reference
+    (pn_rng 0, no GPU) or the device generator's (pn_rng 1)."""
+    lib = capi.load()
+    s, keep = params.to_c()
+    na, ns, nt = C.c_int(), C.c_int(), C.c_int()
+    capi.check(lib.mt_specimen_info(C.byref(s), iconf, C.byref(na), C.byref(ns), C.byref(nt)))
+    Z = np.zeros(na.value, np.int32)
+    xyz = np.zeros(3 * na.value)
+    conf = _conf(system_conf)
+    capi.check(lib.mt_phonon_atoms(C.byref(conf), C.byref(s), iconf, Z.ctypes.data_as(capi.P_int), _dp(xyz),
+                                   na.value))
+    return Z, xyz.reshape(-1, 3)
+
+
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 on the device: ctr [n, 4] and key [n, 2] uint32 -> [n, 4] uint32."""
+    lib = capi.load()
+    c = np.ascontiguousarray(np.asarray(ctr, dtype=np.uint32).reshape(-1, 4))
+    k = np.ascontiguousarray(np.asarray(key, dtype=np.uint32).reshape(-1, 2))
+    out = np.zeros_like(c)
+    P = C.POINTER(C.c_uint)
+    capi.check(lib.mt_philox4x32_10(c.ctypes.data_as(P), k.ctypes.data_as(P), c.shape[0], out.ctypes.data_as(P)))
+    return out
+
+
 def specimen_slices(params: Parameters, iconf: int):
     lib = capi.load()
     s, keep = params.to_c()

@@ -48,7 +48,7 @@ class MtInputMultislice(C.Structure):
         ("simulation_type", c_int), ("interaction_model", c_int), ("potential_type", c_int),
         ("operation_mode", c_int), ("reverse_multislice", c_int),
         ("pn_model", c_int), ("pn_coh_contrib", c_int), ("pn_single_conf", c_int), ("pn_nconf", c_int),
-        ("pn_dim", c_int), ("pn_seed", c_int),
+        ("pn_dim", c_int), ("pn_seed", c_int), ("pn_rng", c_int),
         ("spec_atoms", P_double), ("spec_atoms_rows", c_int), ("spec_atoms_cols", c_int),
         ("spec_lx", c_double), ("spec_ly", c_double), ("spec_lz", c_double), ("spec_dz", c_double),
         ("spec_cryst_na", c_int), ("spec_cryst_nb", c_int), ("spec_cryst_nc", c_int),
@@ -128,6 +128,9 @@ SIGNATURES = {
                                  C.POINTER(C.c_float)]),
     "mt_spline_tables_noalloc": (c_int, [P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
                                          C.c_void_p]),
+    "mt_phonon_atoms": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), c_int, P_int, P_double,
+                                c_int]),
+    "mt_philox4x32_10": (c_int, [C.POINTER(C.c_uint), C.POINTER(C.c_uint), c_int, C.POINTER(C.c_uint)]),
     "mt_spline_tables_ex": (c_int, [C.POINTER(MtSystemConf), c_int, P_int, c_int, c_double, c_double, c_int,
                                     P_double, C.POINTER(C.c_float)]),
     "mt_spline_tables_noalloc_ex": (c_int, [c_int, P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,

@@ -382,11 +382,74 @@ mt_status mt_specimen_atoms(const mt_input_multislice* in, int iconf, int* Z, do
     });
 }
 
+mt_status mt_phonon_atoms(const mt_system_conf* conf, const mt_input_multislice* in, int iconf, int* Z, double* xyz,
+                          int n) {
+    return guarded([&] {
+        HostSpec h(in);
+        if (!(h.m.pn_rng == 1 && h.m.is_frozen_phonon())) {
+            h.spec->move_atoms(iconf);
+        } else {
+            h.spec->still_atoms();
+        }
+        const auto& A = h.spec->atoms();
+        if (n < (int)A.size()) mtb::fail(MT_ERR_INVALID_ARG, "buffer too small");
+        std::vector<float> x(A.x), y(A.y);
+        if (h.m.pn_rng == 1 && h.m.is_frozen_phonon() && A.size()) {
+            if (iconf < 1 || iconf > h.m.pn_nconf) mtb::fail(MT_ERR_INVALID_ARG, "iconf out of range 1..pn_nconf");
+            MTB_CUDA(cudaSetDevice(conf ? conf->gpu_device : 0));
+            cudaStream_t s;
+            MTB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            std::vector<float4> base(A.size());
+            for (size_t i = 0; i < A.size(); i++) base[i] = make_float4(A.x[i], A.y[i], A.occ[i], 0.0f);
+            mtb::DevBuf<float4> d_base, d_out;
+            mtb::DevBuf<float> d_sigma;
+            d_base.upload(base.data(), base.size(), s);
+            d_sigma.upload(A.sigma.data(), A.size(), s);
+            d_out.alloc(A.size());
+            mtb::launch_phonon_displace(d_base.p, d_sigma.p, (int)A.size(), (uint32_t)h.m.pn_seed, iconf, h.m.pn_x,
+                                        h.m.pn_y, d_out.p, s);
+            MTB_CUDA(cudaMemcpyAsync(base.data(), d_out.p, sizeof(float4) * A.size(), cudaMemcpyDeviceToHost, s));
+            MTB_CUDA(cudaStreamSynchronize(s));
+            MTB_CUDA(cudaStreamDestroy(s));
+            for (size_t i = 0; i < A.size(); i++) {
+                x[i] = base[i].x;
+                y[i] = base[i].y;
+            }
+        }
+        for (size_t i = 0; i < A.size(); i++) {
+            Z[i] = A.Z[i];
+            xyz[3 * i] = x[i];
+            xyz[3 * i + 1] = y[i];
+            xyz[3 * i + 2] = A.z[i];
+        }
+    });
+}
+
+mt_status mt_philox4x32_10(const unsigned* ctr, const unsigned* key, int n, unsigned* out) {
+    return guarded([&] {
+        if (n < 1 || !ctr || !key || !out) mtb::fail(MT_ERR_INVALID_ARG, "bad arguments");
+        cudaStream_t s;
+        MTB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        mtb::DevBuf<uint4> d_ctr, d_out;
+        mtb::DevBuf<uint2> d_key;
+        d_ctr.upload(reinterpret_cast<const uint4*>(ctr), n, s);
+        d_key.upload(reinterpret_cast<const uint2*>(key), n, s);
+        d_out.alloc(n);
+        mtb::launch_philox(d_ctr.p, d_key.p, n, d_out.p, s);
+        MTB_CUDA(cudaMemcpyAsync(out, d_out.p, sizeof(uint4) * n, cudaMemcpyDeviceToHost, s));
+        MTB_CUDA(cudaStreamSynchronize(s));
+        MTB_CUDA(cudaStreamDestroy(s));
+    });
+}
+
 mt_status mt_specimen_slices(const mt_input_multislice* in, int iconf, double* z_0, double* z_e, int* iatom_0,
                              int* iatom_e, int* ithk, int n) {
     return guarded([&] {
         HostSpec h(in);
-        h.spec->move_atoms(iconf);
+        if (h.m.pn_rng == 1 && h.m.is_frozen_phonon())
+            h.spec->still_atoms();  // the slicing every device-generated configuration uses
+        else
+            h.spec->move_atoms(iconf);
         const auto& S = h.spec->slices();
         if (n < (int)S.size()) mtb::fail(MT_ERR_INVALID_ARG, "buffer too small");
         for (size_t i = 0; i < S.size(); i++) {

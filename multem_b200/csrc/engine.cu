@@ -436,18 +436,30 @@ ProbeDev Engine::probe_params(float c_c_10, int nz_c10, bool tilt_offset) const 
 
 // Host part of one configuration: Spec::move_atoms, slicing, tables; uploads on the stream.
 void Engine::prepare_conf(ConfData& cd, int iconf) {
-    spec_->move_atoms(iconf);
+    // pn_rng 1: the undisplaced atoms and their slicing once, the displacements on the device
+    const bool device_rng = m_.pn_rng == 1 && m_.is_frozen_phonon();
+    if (!device_rng)
+        spec_->move_atoms(iconf);
+    else if (!d_atoms_u_.p)
+        spec_->still_atoms();
     const auto& A = spec_->atoms();
     const auto& S = spec_->slices();
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     cd.iconf = iconf;
     cd.n_slice = (int)S.size();
-    std::vector<float4> at(A.size());
-    for (size_t i = 0; i < A.size(); i++) {
-        int t = type_of_Z_[(A.Z[i] % 1000) - 1];
-        float tf;
-        std::memcpy(&tf, &t, sizeof(float));
-        at[i] = make_float4(A.x[i], A.y[i], A.occ[i], tf);
+    std::vector<float4> at;
+    if (!device_rng || !d_atoms_u_.p) {
+        at.resize(A.size());
+        for (size_t i = 0; i < A.size(); i++) {
+            int t = type_of_Z_[(A.Z[i] % 1000) - 1];
+            float tf;
+            std::memcpy(&tf, &t, sizeof(float));
+            at[i] = make_float4(A.x[i], A.y[i], A.occ[i], tf);
+        }
+    }
+    if (device_rng && !d_atoms_u_.p) {
+        d_atoms_u_.upload(at.data(), at.size(), stream_);
+        d_sigma_.upload(A.sigma.data(), A.size(), stream_);
     }
     std::vector<int2> rg(S.size());
     cd.slice_ithk.resize(S.size());
@@ -484,7 +496,13 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
         cd.probe_c_c_10.push_back(L.c_c_10);
         cd.probe_nz_c10.push_back(!is_zero_f(f_s));
     }
-    cd.atoms.upload(at.data(), at.size(), stream_);
+    if (device_rng) {
+        cd.atoms.alloc(A.size());
+        launch_phonon_displace(d_atoms_u_.p, d_sigma_.p, (int)A.size(), (uint32_t)m_.pn_seed, iconf, m_.pn_x, m_.pn_y,
+                               cd.atoms.p, stream_);
+    } else {
+        cd.atoms.upload(at.data(), at.size(), stream_);
+    }
     cd.ranges.upload(rg.data(), rg.size(), stream_);
     cd.prop.upload(prop.data(), prop.size(), stream_);
     synchronize();  // host vectors go out of scope

@@ -167,6 +167,8 @@ class Engine {
     DevBuf<float2> d_p0_;            // zero-distance propagator factors (1/N only), Px then Py
     DevBuf<float2> d_coh_;           // STEM with pn_coh_contrib: psi_coh [n_thk][n_scan][nx][ny]
     DevBuf<double> d_image_coh_;     // [n_thk][n_det][n_scan]
+    DevBuf<float4> d_atoms_u_;       // pn_rng 1: undisplaced atoms (x, y, occ, type), z-sorted
+    DevBuf<float> d_sigma_;          // pn_rng 1: per-atom displacement sigma
     ColArgs det_args() const;        // detector description for the column pass
     std::vector<ConfData> confs_;
     GridDev gdev_{};

@@ -692,6 +692,8 @@ Model build_model(const mt_input_multislice* in) {
         default: break;
     }
     m.pn_seed = in->pn_seed;
+    m.pn_rng = in->pn_rng;
+    if (m.pn_rng != 0 && m.pn_rng != 1) fail(MT_ERR_INVALID_ARG, "pn_rng must be 0 (host) or 1 (device)");
 
     const float lx = (float)in->spec_lx, ly = (float)in->spec_ly, lz = (float)in->spec_lz, dz = (float)in->spec_dz;
     if (in->spec_atoms_rows < 0 || (in->spec_atoms_rows > 0 && (!in->spec_atoms || in->spec_atoms_cols < 4)))
@@ -1100,6 +1102,12 @@ void Specimen::move_atoms(int iconf) {
         atoms_.charge[i] = atoms_u_.charge[i];
     }
     if (m_.pn_z) atoms_.sort_by_z();
+    atoms_.statistic(R_max_of_Z_.data());
+    calculate();
+}
+
+void Specimen::still_atoms() {
+    atoms_ = atoms_u_;
     atoms_.statistic(R_max_of_Z_.data());
     calculate();
 }

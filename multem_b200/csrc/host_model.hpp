@@ -117,6 +117,7 @@ struct Model {
     std::vector<double> obj_w;
     bool pn_coh_contrib = false, pn_single_conf = false;
     int pn_nconf = 1, fp_iconf_0 = 1, pn_seed = 300183;
+    int pn_rng = 0;  // 0 host draws of the reference, 1 counter-based draws on the device
     bool pn_x = true, pn_y = true, pn_z = false;
     int thick_type = 1;
     int potential_slicing = 1;
@@ -222,6 +223,10 @@ class Specimen {
 
     // Spec::move_atoms(fp_iconf): displace, (re)sort, statistics, slicing.
     void move_atoms(int iconf);
+    // The undisplaced atoms with their statistics and slicing: the device phonon generator
+    // displaces x and y only, so this slicing holds for every configuration.
+    void still_atoms();
+    const AtomsF& atoms_undisplaced() const { return atoms_u_; }
 
     const AtomsF& atoms() const { return atoms_; }
     const std::vector<SliceF>& slices() const { return slice_; }

@@ -138,4 +138,12 @@ void launch_ew_accumulate(const float2* psi, int nx, int ny, int ix0, int ix1, i
 long long launches_issued();
 void add_launches(long long n);
 
+// ---- frozen-phonon displacements on the device (phonon.cu) ----
+// out[i] = base[i] with x, y moved by sigma[i] times two standard normals drawn from
+// Philox4x32-10(key (seed, 0), counter (i, iconf, 0, 0)) through Box-Muller; z is never displaced.
+void launch_phonon_displace(const float4* base, const float* sigma, int n, uint32_t seed, int iconf, bool pn_x,
+                            bool pn_y, float4* out, cudaStream_t s);
+// Philox4x32-10 of n (counter, key) pairs, for checking the generator against published vectors.
+void launch_philox(const uint4* ctr, const uint2* key, int n, uint4* out, cudaStream_t s);
+
 }  // namespace mtb

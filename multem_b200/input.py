@@ -55,6 +55,7 @@ class Parameters:
         self.pn_nconf = 1
         self.pn_dim = 110
         self.pn_seed = 300183
+        self.pn_rng = 0          # 0 the reference's host draws, 1 counter-based draws on the GPU
         self.spec_atoms = np.zeros((0, 8))
         self.spec_dz = 0.25
         self.spec_lx = 10.0
@@ -128,7 +129,7 @@ class Parameters:
 
         s = capi.MtInputMultislice()
         for k in ["simulation_type", "interaction_model", "potential_type", "operation_mode", "reverse_multislice",
-                  "pn_model", "pn_coh_contrib", "pn_single_conf", "pn_nconf", "pn_dim", "pn_seed",
+                  "pn_model", "pn_coh_contrib", "pn_single_conf", "pn_nconf", "pn_dim", "pn_seed", "pn_rng",
                   "spec_cryst_na", "spec_cryst_nb", "spec_cryst_nc", "spec_rot_center_type", "thick_type",
                   "potential_slicing", "nx", "ny", "bwl", "iw_type", "illumination_model",
                   "temporal_spatial_incoh", "scanning_type", "scanning_periodic", "scanning_square_pxs",

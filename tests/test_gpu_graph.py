@@ -31,10 +31,12 @@ def _cases():
     ew = specimens.hrtem_si001(nx=128, ny=128, na=4, nb=4, nc=4)
     ew.pn_nconf = 4
     ew.pn_seed = 7
-    return {"stem": stem, "stem_thicknesses": thick, "stem_tilt": tilt, "ew": ew}
+    stem_dev = specimens.stem_srtio3(nx=128, ny=128, na=4, nb=4, nc=6, ns=5, nconf=5, seed=2)
+    stem_dev.pn_rng = 1  # configurations drawn on the device, into the slot the graph reads
+    return {"stem": stem, "stem_thicknesses": thick, "stem_tilt": tilt, "ew": ew, "stem_device_rng": stem_dev}
 
 
-@pytest.mark.parametrize("name", ["stem", "stem_thicknesses", "stem_tilt", "ew"])
+@pytest.mark.parametrize("name", ["stem", "stem_thicknesses", "stem_tilt", "ew", "stem_device_rng"])
 def test_graph_replay_is_bit_identical(name, monkeypatch):
     p = _cases()[name]
     direct, n0 = _run(p, 0, monkeypatch)
