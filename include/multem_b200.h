@@ -310,9 +310,12 @@ mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, doub
  * (0-4), 2 Peng (0-4), 3 Peng (0-12), 4 Kirkland (0-12) or 6 Lobato (0-12); the tables of
  * Atomic_Data::get_atom_coef built with that type (src/atomic_data.hpp:1303-1400, 1547-1668).
  * 5 (Weickenmeier-Kohl, no closed-form projected potential) returns MT_ERR_UNSUPPORTED.
- * mt_spline_tables is this call with potential_type 6. */
-mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, int n, double dR_min,
-                              double Vrl, int nR, double* heads, float* tab);
+ * charge (optional, NULL = neutral): the ionic charge of each entry; a charge with an entry in
+ * Peng's ionic table (0-4) gets its ionic table (set_Peng_ions_coef, src/atomic_data.hpp:1489-1543,
+ * whatever potential_type), any other charge the neutral one, as the reference.
+ * mt_spline_tables is this call with potential_type 6 and no charges. */
+mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, const int* charge, int n,
+                              double dR_min, double Vrl, int nR, double* heads, float* tab);
 
 /* Allocation-free form of mt_spline_tables; it has no counterpart in the reference. It is for
  * callers that cannot call cudaMalloc: code running inside a CUDA stream capture, code whose GPU
@@ -331,8 +334,8 @@ mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vr
                                    float* d_tab, void* stream);
 /* mt_spline_tables_noalloc for `potential_type` (as mt_spline_tables_ex); mt_spline_tables_noalloc
  * is this call with potential_type 6. */
-mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, int n, double dR_min, double Vrl, int nR,
-                                      double* heads, float* d_tab, void* stream);
+mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, const int* charge, int n, double dR_min,
+                                      double Vrl, int nR, double* heads, float* d_tab, void* stream);
 
 /* ---- specimen host logic, exposed for parity checks ---- */
 

@@ -250,15 +250,18 @@ def ilc_propagate(system_conf, params: Parameters) -> dict:
     return {"dx": params.spec_lx / params.nx, "dy": params.spec_ly / params.ny, "psi": psi}
 
 
-def spline_tables(Z, dR_min: float, Vrl: float = 0.015, nR: int = 128, system_conf=None, potential_type: int = 6):
+def spline_tables(Z, dR_min: float, Vrl: float = 0.015, nR: int = 128, system_conf=None, potential_type: int = 6,
+                  charge=None):
     """FP64 GPU build of the spline tables of `potential_type` (6 Lobato; 1-4 Doyle-Turner, Peng 0-4,
-    Peng 0-12, Kirkland): returns (heads[n, 4], tab[n, 5, nR] float32)."""
+    Peng 0-12, Kirkland), optionally for ionic charges: returns (heads[n, 4], tab[n, 5, nR] float32)."""
     lib = capi.load()
     z = np.ascontiguousarray(np.asarray(Z, dtype=np.int32))
+    q = None if charge is None else np.ascontiguousarray(np.asarray(charge, dtype=np.int32))
     heads = np.zeros((z.size, 4))
     tab = np.zeros((z.size, 5, nR), dtype=np.float32)
     conf = _conf(system_conf)
-    capi.check(lib.mt_spline_tables_ex(C.byref(conf), int(potential_type), z.ctypes.data_as(capi.P_int), z.size,
+    capi.check(lib.mt_spline_tables_ex(C.byref(conf), int(potential_type), z.ctypes.data_as(capi.P_int),
+                                       q.ctypes.data_as(capi.P_int) if q is not None else capi.P_int(), z.size,
                                        float(dR_min), float(Vrl), nR, _dp(heads),
                                        tab.ctypes.data_as(C.POINTER(C.c_float))))
     return heads, tab

@@ -131,10 +131,10 @@ SIGNATURES = {
     "mt_phonon_atoms": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), c_int, P_int, P_double,
                                 c_int]),
     "mt_philox4x32_10": (c_int, [C.POINTER(C.c_uint), C.POINTER(C.c_uint), c_int, C.POINTER(C.c_uint)]),
-    "mt_spline_tables_ex": (c_int, [C.POINTER(MtSystemConf), c_int, P_int, c_int, c_double, c_double, c_int,
+    "mt_spline_tables_ex": (c_int, [C.POINTER(MtSystemConf), c_int, P_int, P_int, c_int, c_double, c_double, c_int,
                                     P_double, C.POINTER(C.c_float)]),
-    "mt_spline_tables_noalloc_ex": (c_int, [c_int, P_int, c_int, c_double, c_double, c_int, P_double, C.c_void_p,
-                                            C.c_void_p]),
+    "mt_spline_tables_noalloc_ex": (c_int, [c_int, P_int, P_int, c_int, c_double, c_double, c_int, P_double,
+                                            C.c_void_p, C.c_void_p]),
     # learned surrogate kernels (include/multem_b200_surrogate.h); tensors are device pointers
     "mt_sg_conv3x3_forward": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, c_int, _VP]),
     "mt_sg_conv3x3_backward_data": (c_int, [_VP, _VP, _VP, _VP, c_int, c_int, c_int, c_int, c_int, _VP]),

@@ -278,11 +278,11 @@ mt_status mt_incident_wave(const mt_system_conf* conf, const mt_input_multislice
 
 mt_status mt_spline_tables(const mt_system_conf* conf, const int* Z, int n, double dR_min, double Vrl, int nR,
                            double* heads, float* tab) {
-    return mt_spline_tables_ex(conf, 6, Z, n, dR_min, Vrl, nR, heads, tab);
+    return mt_spline_tables_ex(conf, 6, Z, nullptr, n, dR_min, Vrl, nR, heads, tab);
 }
 
-mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, int n, double dR_min,
-                              double Vrl, int nR, double* heads, float* tab) {
+mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, const int* Z, const int* charge, int n,
+                              double dR_min, double Vrl, int nR, double* heads, float* tab) {
     return guarded([&] {
         if (!Z || n <= 0 || !tab || nR < 2) mtb::fail(MT_ERR_INVALID_ARG, "bad arguments");
         if (!mtb::potential_type_supported(potential_type))
@@ -298,7 +298,9 @@ mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, co
         for (int z : zs) hd.push_back(mtb::element_head(z, potential_type, (float)dR_min, (float)Vrl));
         mtb::DevBuf<float> d_tab;
         d_tab.alloc((size_t)n * 5 * nR);
-        mtb::build_tables(zs, potential_type, hd, nR, d_tab.p, s);
+        std::vector<int> qs;
+        if (charge) qs.assign(charge, charge + n);
+        mtb::build_tables(zs, potential_type, hd, nR, d_tab.p, s, qs);
         MTB_CUDA(cudaMemcpyAsync(tab, d_tab.p, sizeof(float) * (size_t)n * 5 * nR, cudaMemcpyDeviceToHost, s));
         MTB_CUDA(cudaStreamSynchronize(s));
         MTB_CUDA(cudaStreamDestroy(s));
@@ -314,11 +316,11 @@ mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, co
 
 mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
                                    float* d_tab, void* stream) {
-    return mt_spline_tables_noalloc_ex(6, Z, n, dR_min, Vrl, nR, heads, d_tab, stream);
+    return mt_spline_tables_noalloc_ex(6, Z, nullptr, n, dR_min, Vrl, nR, heads, d_tab, stream);
 }
 
-mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, int n, double dR_min, double Vrl, int nR,
-                                      double* heads, float* d_tab, void* stream) {
+mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, const int* charge, int n, double dR_min,
+                                      double Vrl, int nR, double* heads, float* d_tab, void* stream) {
     return guarded([&] {
         if (!mtb::potential_type_supported(potential_type))
             mtb::fail(MT_ERR_UNSUPPORTED, "potential_type must be 1-4 or 6");
@@ -329,7 +331,9 @@ mt_status mt_spline_tables_noalloc_ex(int potential_type, const int* Z, int n, d
         std::vector<int> zs(Z, Z + n);
         std::vector<mtb::TableHead> hd;
         for (int z : zs) hd.push_back(mtb::element_head(z, potential_type, (float)dR_min, (float)Vrl));
-        mtb::build_tables_noalloc(zs, potential_type, hd, nR, d_tab, static_cast<cudaStream_t>(stream));
+        std::vector<int> qs;
+        if (charge) qs.assign(charge, charge + n);
+        mtb::build_tables_noalloc(zs, potential_type, hd, nR, d_tab, static_cast<cudaStream_t>(stream), qs);
         if (heads)
             for (int i = 0; i < n; i++) {
                 heads[4 * i] = hd[i].R_min;

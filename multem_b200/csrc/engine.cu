@@ -218,21 +218,33 @@ void Engine::reset() {
 
 // Element spline tables for the elements present (Spec::set_input_data builds all 103,
 // src/spec.hpp:49-55; only the present ones are ever read).
+// One table per (element, charge) in the specimen; an ion without its own coefficients shares its
+// element's neutral table. Atoms carry the table index (atom_type(Z, charge)).
+int Engine::atom_type(int Z, int charge) const {
+    const int q = effective_charge(Z, charge);
+    return type_of_Zq_[(size_t)(Z - 1) * kChargeSlots + (q + kChargeSlots / 2)];
+}
+
 void Engine::build_types() {
-    type_of_Z_.assign(103, -1);
+    type_of_Zq_.assign((size_t)103 * kChargeSlots, -1);
     Z_of_type_.clear();
-    for (int Zr : m_.atoms_in.Z) {
-        int Z = Zr % 1000;
-        if (type_of_Z_[Z - 1] < 0) {
-            type_of_Z_[Z - 1] = (int)Z_of_type_.size();
+    charge_of_type_.clear();
+    const auto& A = m_.atoms_in;
+    for (size_t i = 0; i < A.Z.size(); i++) {
+        const int Z = A.Z[i] % 1000;
+        const int q = effective_charge(Z, A.charge[i]);
+        int& t = type_of_Zq_[(size_t)(Z - 1) * kChargeSlots + (q + kChargeSlots / 2)];
+        if (t < 0) {
+            t = (int)Z_of_type_.size();
             Z_of_type_.push_back(Z);
+            charge_of_type_.push_back(q);
         }
     }
-    if ((int)Z_of_type_.size() > kMaxTypes) fail(MT_ERR_UNSUPPORTED, "more than 16 elements in one specimen");
+    if ((int)Z_of_type_.size() > kMaxTypes) fail(MT_ERR_UNSUPPORTED, "more than 16 (element, charge) types in one specimen");
     d_tab_.alloc((size_t)Z_of_type_.size() * 5 * m_.nR);
     heads_.clear();
     for (int Z : Z_of_type_) heads_.push_back(element_head(Z, m_.potential_type, m_.grid.dR_min(), m_.Vrl));
-    build_tables(Z_of_type_, m_.potential_type, heads_, m_.nR, d_tab_.p, stream_);
+    build_tables(Z_of_type_, m_.potential_type, heads_, m_.nR, d_tab_.p, stream_, charge_of_type_);
     R_max_f_.resize(Z_of_type_.size());
     for (size_t t = 0; t < Z_of_type_.size(); t++) R_max_f_[t] = (float)heads_[t].R_max;
     d_Rmax_.upload(R_max_f_.data(), R_max_f_.size(), stream_);
@@ -451,7 +463,7 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     if (!device_rng || !d_atoms_u_.p) {
         at.resize(A.size());
         for (size_t i = 0; i < A.size(); i++) {
-            int t = type_of_Z_[(A.Z[i] % 1000) - 1];
+            int t = atom_type(A.Z[i] % 1000, A.charge[i]);
             float tf;
             std::memcpy(&tf, &t, sizeof(float));
             at[i] = make_float4(A.x[i], A.y[i], A.occ[i], tf);

@@ -134,8 +134,11 @@ class Engine {
     long long launches_ = 0;
 
     // element tables
-    std::vector<int> type_of_Z_;     // Z-1 -> type index or -1
+    static constexpr int kChargeSlots = 15;  // charges -7..7, the reference's ionic range
+    std::vector<int> type_of_Zq_;    // (Z-1)*kChargeSlots + charge+7 -> table index or -1
     std::vector<int> Z_of_type_;
+    std::vector<int> charge_of_type_;
+    int atom_type(int Z, int charge) const;
     std::vector<float> R_max_f_;     // per type
     std::vector<TableHead> heads_;
     DevBuf<float> d_tab_;

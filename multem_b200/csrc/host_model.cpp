@@ -718,7 +718,6 @@ Model build_model(const mt_input_multislice* in) {
         A.charge[i] = (int)((nc > 7) ? a[7 * nr + i] : 0);
         int Zi = A.Z[i] % 1000;
         if (Zi < 1 || Zi > 103) fail(MT_ERR_INVALID_ARG, "atomic number out of range 1..103");
-        if (A.charge[i] != 0) fail(MT_ERR_UNSUPPORTED, "ionic charges are not implemented (charge column must be 0)");
     }
     if (nr == 0) fail(MT_ERR_INVALID_ARG, "specimen has no atoms");
     A.statistic(nullptr);

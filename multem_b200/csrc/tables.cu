@@ -28,6 +28,13 @@
 //   c0 = VR, c1 = dVR/d(R^2) = 0.5*dVR/R, both cosine-tapered beyond R_tap^2 (apply_tapering,
 //   src/cgpu_fcns.cuh:1530-1540); c2, c3 from the Hermite conditions between knots
 //   (src/atomic_data.hpp:1652-1663).
+//   Ions (atoms whose charge q has an entry in Peng's ionic table, whatever potential_type):
+//     set_Peng_ions_coef (src/atomic_data.hpp:1489-1543): five Gaussian terms as for type 2 from
+//     the ionic table, plus a screened Coulomb term for the net charge, cl = q/(2 pi^2 a0),
+//     cnl = (2 pi r0)^-2 with r0 = 2 A, turned into a Yukawa term as Kirkland's; VR adds
+//     cl*K0(cnl*R) (VR_dVR_Peng_ion_0_4, src/cgpu_fcns.cuh:1271-1284); R_max is the neutral
+//     atom's (src/atomic_data.hpp:1612). A charge without an entry uses the neutral coefficients
+//     (Atom_Type::charge_to_idx, src/types.cuh:4125-4137).
 // Weickenmeier-Kohl (type 5) has no closed-form projected potential (the reference integrates Vr
 // numerically along z) and is refused by the input validation.
 // The modified Bessel functions K0, K1 use the polynomial approximations of Abramowitz & Stegun,
@@ -61,12 +68,26 @@ constexpr double kHalfPi = 1.570796326794896619231;
 struct ElemCoef {
     double VRcl[6], VRcnl[6], Vrcl[6], Vrcnl[6];  // unused terms: cl = 0, cnl = 1
     double rn_c, ra;
-    int type;  // potential_type
+    int type;  // potential_type, or kIonType for a Peng ion
 };
+
+constexpr int kIonType = 7;
+constexpr double k2Pi2a0 = 10.445539456905012;  // 2 pi^2 a0 (Bohr radius in A)
 
 // Gaussian terms of each parameterisation: [g0, g1); Kirkland's Yukawa terms are [0, 3)
 __host__ __device__ inline int gauss_first(int type) { return type == 4 ? 3 : 0; }
 __host__ __device__ inline int gauss_end(int type) { return type == 1 ? 4 : (type == 4 ? 6 : 5); }
+
+// Index of charge q in the reference's per-element coefficient list (2q for q > 0, -2q - 1 below)
+int charge_index(int q) { return q >= 0 ? 2 * q : -2 * q - 1; }
+
+const PengIon* find_ion(int Z, int q) {
+    if (q == 0) return nullptr;
+    const int idx = charge_index(q);
+    for (const PengIon& e : kPengIon)
+        if (e.Z == Z && e.idx == idx) return &e;
+    return nullptr;
+}
 
 __device__ double as_i0(double x) {  // A&S 9.8.1 / 9.8.2
     double ax = fabs(x), y;
@@ -144,6 +165,10 @@ __global__ void build_tables_kernel(const ElemCoef* __restrict__ coef, const Tab
                 dy += -c.VRcl[i] * (c.VRcnl[i] * R * k0 + 2 * k1);
             }
         } else {
+            if (c.type == kIonType) {
+                y += c.VRcl[5] * as_k0(c.VRcnl[5] * R);
+                dy += -c.VRcl[5] * c.VRcnl[5] * as_k1(c.VRcnl[5] * R);
+            }
             if (c.type == 4)
                 for (int i = 0; i < 3; i++) {
                     y += c.VRcl[i] * as_k0(c.VRcnl[i] * R);
@@ -187,7 +212,7 @@ __global__ void build_tables_kernel(const ElemCoef* __restrict__ coef, const Tab
 
 // Coefficients of element Z for potential_type `type` (set_*_neutral_coef,
 // src/atomic_data.hpp:1303-1486) and the rn_c of To_atom_type_CPU (src/atomic_data.hpp:148-176)
-ElemCoef element_coef(int Z, int type) {
+ElemCoef element_coef(int Z, int type, int charge = 0) {
     ElemCoef e{};
     const int iZ = Z - 1;
     for (int j = 0; j < 6; j++) {
@@ -195,7 +220,22 @@ ElemCoef element_coef(int Z, int type) {
         e.Vrcnl[j] = e.VRcnl[j] = 1.0;
     }
     auto zero = [](double v) { return std::fabs(v) <= 1e-13; };
-    if (type == 6) {
+    const PengIon* ion = find_ion(Z, charge);
+    if (ion && !zero(ion->cl[0]) && !zero(ion->cnl[0])) {
+        for (int j = 0; j < 5; j++) {
+            double cl = ion->cl[j];
+            double cnl = zero(cl) ? 0.0 : ion->cnl[j] / 4.0;
+            if (zero(cl) || zero(cnl)) continue;
+            e.Vrcl[j] = kPotf * cl * std::pow(kPi / cnl, 1.5);
+            e.VRcl[j] = kPotf * kPi * cl / cnl;
+            e.Vrcnl[j] = e.VRcnl[j] = kPi2 / cnl;
+        }
+        const double cl = charge / k2Pi2a0, cnl = std::pow(k2Pi * 2.0, -2.0);
+        e.Vrcl[5] = kPotf * kPi * cl;
+        e.VRcl[5] = kPotf * k2Pi * cl;
+        e.Vrcnl[5] = e.VRcnl[5] = k2Pi * std::sqrt(cnl);
+        type = kIonType;
+    } else if (type == 6) {
         for (int j = 0; j < 5; j++) {
             double cl = kLobatoCl[iZ][j];
             double cnl = zero(cl) ? 0.0 : kLobatoCnl[iZ][j];
@@ -248,6 +288,11 @@ static double vr_host(double x, const ElemCoef& c) {
 
 bool potential_type_supported(int type) { return (type >= 1 && type <= 4) || type == 6; }
 
+int effective_charge(int Z, int charge) {
+    const PengIon* ion = find_ion(Z, charge);
+    return (ion && !(std::fabs(ion->cl[0]) <= 1e-13) && !(std::fabs(ion->cnl[0]) <= 1e-13)) ? charge : 0;
+}
+
 TableHead element_head(int Z, int type, float dR_min, float Vrl_f) {
     if (!potential_type_supported(type)) fail(MT_ERR_UNSUPPORTED, "potential_type " + std::to_string(type) + " has no table build");
     const ElemCoef c = element_coef(Z, type);
@@ -281,10 +326,10 @@ TableHead element_head(int Z, int type, float dR_min, float Vrl_f) {
 }
 
 void build_tables(const std::vector<int>& Zs, int type, const std::vector<TableHead>& heads, int nR, float* d_tab,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, const std::vector<int>& charges) {
     const int n = (int)Zs.size();
     std::vector<ElemCoef> h(n);
-    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type, charges.empty() ? 0 : charges[i]);
     int dev = 0;
     auto* d_coef = static_cast<ElemCoef*>(dev_alloc(sizeof(ElemCoef) * n, &dev));
     auto* d_head = static_cast<TableHead*>(dev_alloc(sizeof(TableHead) * n, &dev));
@@ -330,7 +375,7 @@ static unsigned char* noalloc_scratch_address(int dev) {
 }
 
 void build_tables_noalloc(const std::vector<int>& Zs, int type, const std::vector<TableHead>& heads, int nR,
-                          float* d_tab, cudaStream_t stream) {
+                          float* d_tab, cudaStream_t stream, const std::vector<int>& charges) {
     const int n = (int)Zs.size();
     if (n < 1 || n > kNoAllocMaxElements)
         fail(MT_ERR_INVALID_ARG, "allocation-free table build takes 1.." + std::to_string(kNoAllocMaxElements) +
@@ -342,7 +387,7 @@ void build_tables_noalloc(const std::vector<int>& Zs, int type, const std::vecto
     ElemCoef* d_coef = reinterpret_cast<ElemCoef*>(base);
     TableHead* d_head = reinterpret_cast<TableHead*>(base + kNoAllocMaxElements * sizeof(ElemCoef));
     std::vector<ElemCoef> h(n);
-    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type);
+    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type, charges.empty() ? 0 : charges[i]);
     // pageable sources: each copy returns once its source has been staged, so the vectors may go
     MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
     MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));

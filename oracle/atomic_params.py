@@ -1,5 +1,5 @@
 """Lobato (0-12) coefficients, the Doyle-Turner / Peng / Kirkland coefficients (FEG_CL[t - 1], FEG_CNL[t - 1]
-for potential_type t = 1..4), mass numbers and atomic radii for Z = 1..103, read from the data file
+for potential_type t = 1..4), Peng's ionic coefficients (PENG_ION[(Z, charge index)]), mass numbers and atomic radii for Z = 1..103, read from the data file
 the engine compiles in (multem_b200/csrc/atomic_params.inc, extracted from the reference's
 src/atomic_data.hpp by multem_b200/csrc/gen_atomic_params.py). Test infrastructure only."""
 import re
@@ -25,8 +25,16 @@ def _parse():
         rows = [[float(v) for v in r.split(",")] for r in re.findall(r"\{([^{}]*)\}", body)]
         return [rows[103 * t:103 * (t + 1)] for t in range(4)]
 
+    def ions():
+        body = re.search(r"kPengIon\[\d+\] = \{(.*?)\n\};", s, re.S).group(1)
+        out = {}
+        for m in re.finditer(r"\{(\d+), (\d+), \{([^}]*)\}, \{([^}]*)\}\}", body):
+            out[(int(m.group(1)), int(m.group(2)))] = ([float(v) for v in m.group(3).split(",")],
+                                                       [float(v) for v in m.group(4).split(",")])
+        return out
+
     return (table("kLobatoCl"), table("kLobatoCnl"), vec("kMassNumber", int), vec("kAtomicRadius", float),
-            feg("kFegCl"), feg("kFegCnl"))
+            feg("kFegCl"), feg("kFegCnl"), ions())
 
 
-LOBATO_CL, LOBATO_CNL, MASS_NUMBER, ATOMIC_RADIUS, FEG_CL, FEG_CNL = _parse()
+LOBATO_CL, LOBATO_CNL, MASS_NUMBER, ATOMIC_RADIUS, FEG_CL, FEG_CNL, PENG_ION = _parse()

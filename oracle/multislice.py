@@ -121,6 +121,32 @@ def feg_coef(Z, pt):
     return Vr_cl, cnl_out, VR_cl, cnl_out.copy()
 
 
+C_2PI2A0 = 10.445539456905012  # 2 pi^2 a0
+
+
+def ion_coef(Z, q):
+    """Vr/VR coefficients of element Z with ionic charge q from Peng's ionic table
+    (set_Peng_ions_coef, src/atomic_data.hpp:1489-1543), or None when the table has no entry (the
+    atom then uses the neutral coefficients, Atom_Type::charge_to_idx src/types.cuh:4125-4137)."""
+    if q == 0:
+        return None
+    e = atomic_params.PENG_ION.get((Z, 2 * q if q > 0 else -2 * q - 1))
+    if e is None or abs(e[0][0]) <= 1e-13 or abs(e[1][0]) <= 1e-13:
+        return None
+    Vr_cl, VR_cl, cnl_out = np.zeros(6), np.zeros(6), np.ones(6)
+    for j in range(5):
+        cl = e[0][j]
+        cnl = 0.0 if abs(cl) <= 1e-13 else e[1][j] / 4.0
+        if abs(cl) <= 1e-13 or abs(cnl) <= 1e-13:
+            continue
+        Vr_cl[j] = C_POTF * cl * (C_PI / cnl) ** 1.5
+        VR_cl[j] = C_POTF * C_PI * cl / cnl
+        cnl_out[j] = C_PI2 / cnl
+    cl, cnl = q / C_2PI2A0, (C_2PI * 2.0) ** -2
+    Vr_cl[5], VR_cl[5], cnl_out[5] = C_POTF * C_PI * cl, C_POTF * C_2PI * cl, C_2PI * math.sqrt(cnl)
+    return Vr_cl, cnl_out, VR_cl, cnl_out.copy()
+
+
 def vr_feg(x, cl, cnl, pt):
     """Vr of potential_type 1-4 (Vr_Doyle/Peng/Kirkland_neutral_*, src/cgpu_fcns.cuh:1023-1070)."""
     g0, g1 = _gauss_range(pt)
@@ -132,6 +158,14 @@ def vr_dvr_projected(R, VR_cl, VR_cnl, pt):
     """VR(R) and dVR/dR (VR_dVR_*_neutral_*, src/cgpu_fcns.cuh:1162-1268)."""
     y = np.zeros_like(R)
     dy = np.zeros_like(R)
+    if pt == "ion":
+        for i in range(5):
+            yt = VR_cl[i] * np.exp(-VR_cnl[i] * (R * R))
+            y += yt
+            dy += -2 * VR_cnl[i] * R * yt
+        y += VR_cl[5] * bessel_k0(VR_cnl[5] * R)
+        dy += -VR_cl[5] * VR_cnl[5] * bessel_k1(VR_cnl[5] * R)
+        return y, dy
     if pt == 6:
         for i in range(5):
             k0 = bessel_k0(VR_cnl[i] * R)
@@ -150,8 +184,14 @@ def vr_dvr_projected(R, VR_cl, VR_cnl, pt):
     return y, dy
 
 
-def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128, potential_type=6):
-    """Spline table of element Z: dict with R_min, R_max, R_tap, tap_cf (float64) and R2, c0..c3."""
+def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128, potential_type=6, charge=0):
+    """Spline table of element Z (ionic charge `charge`): dict with R_min, R_max, R_tap, tap_cf
+    (float64) and R2, c0..c3. An ion's R_min .. tap_cf are its neutral element's
+    (src/atomic_data.hpp:1612)."""
+    ion = ion_coef(Z, charge)
+    if ion is not None:
+        t = atom_table(Z, dR_min, Vrl, nR, potential_type)
+        return _table_body(t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"], nR, ion[2], ion[3], "ion")
     pt = potential_type
     if pt == 6:
         Vr_cl, Vr_cnl, VR_cl, VR_cnl = lobato_coef(Z)
@@ -184,6 +224,11 @@ def atom_table(Z, dR_min, Vrl=np.float32(0.015), nR=128, potential_type=6):
         R_max = 1.75 * atomic_params.ATOMIC_RADIUS[Z - 1]
     R_tap = R_min + 0.85 * (R_max - R_min)
     tap_cf = C_HALFPI / (R_max ** 2 - R_tap ** 2)
+    return _table_body(R_min, R_max, R_tap, tap_cf, nR, VR_cl, VR_cnl, pt)
+
+
+def _table_body(R_min, R_max, R_tap, tap_cf, nR, VR_cl, VR_cnl, pt):
+    """Knots, tapered VR / dVR and the cubic coefficients (src/atomic_data.hpp:1620-1663)."""
     dlnr = math.log(R_max / R_min) / (nR - 1)
     R = R_min * np.exp(np.arange(nR) * dlnr)
     R2 = R ** 2

@@ -419,13 +419,16 @@ int mtref_transmission_function(const mt_input_multislice* in, int precision, in
     });
 }
 
-// Spline table of element Z (Atomic_Data::get_atom_coef, src/atomic_data.hpp:1547-1668), as
-// stored in the working precision: R_min, R_max, R_tap, tap_cf, then R2[nR], c0..c3[nR].
-int mtref_atom_type(const mt_input_multislice* in, int precision, int Z, double* head, double* tab, int nR) {
+// Spline table of element Z with ionic charge `charge` (Atomic_Data::get_atom_coef,
+// src/atomic_data.hpp:1547-1668; the coefficient set Atom_Type::charge_to_idx selects), as stored in
+// the working precision: R_min, R_max, R_tap, tap_cf, then R2[nR], c0..c3[nR].
+int mtref_atom_type_q(const mt_input_multislice* in, int precision, int Z, int charge, double* head, double* tab,
+                      int nR) {
     return guarded([&] {
         auto body = [&](auto& w) {
             using TT = typename std::decay<decltype(w.im)>::type::value_type;
-            auto& c = static_cast<mt::Spec<TT>&>(w.wf).atom_type[Z - 1].coef[0];
+            auto& at = static_cast<mt::Spec<TT>&>(w.wf).atom_type[Z - 1];
+            auto& c = at.coef[at.charge_to_idx(charge)];
             head[0] = (double)c.R_min;
             head[1] = (double)c.R_max;
             head[2] = (double)c.R_tap;
@@ -443,6 +446,10 @@ int mtref_atom_type(const mt_input_multislice* in, int precision, int Z, double*
         WF<float> w(in, 1);
         return body(w);
     });
+}
+
+int mtref_atom_type(const mt_input_multislice* in, int precision, int Z, double* head, double* tab, int nR) {
+    return mtref_atom_type_q(in, precision, Z, 0, head, tab, nR);
 }
 
 // Incident wave (Incident_Wave::operator()(space, output), src/incident_wave.cuh:98-116), with the

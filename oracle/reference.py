@@ -43,6 +43,8 @@ def lib():
                                                   capi.P_double]
         L.mtref_atom_type.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, capi.P_double, capi.P_double,
                                       C.c_int]
+        L.mtref_atom_type_q.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, C.c_int, capi.P_double,
+                                        capi.P_double, C.c_int]
         L.mtref_incident_wave.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, capi.P_double]
         L.mtref_propagate.argtypes = [P(capi.MtInputMultislice), C.c_int, C.c_int, C.c_double, capi.P_double]
         _lib = L
@@ -157,11 +159,11 @@ def transmission_function(p, iconf, islice, precision=1, nthreads=1):
     return t.reshape(p.nx, p.ny).T
 
 
-def atom_type(p, Z, precision=1, nR=128):
+def atom_type(p, Z, precision=1, nR=128, charge=0):
     s, keep = p.to_c()
     head = np.zeros(4)
     tab = np.zeros(5 * nR)
-    _chk(lib().mtref_atom_type(C.byref(s), precision, Z, _dp(head), _dp(tab), nR))
+    _chk(lib().mtref_atom_type_q(C.byref(s), precision, Z, charge, _dp(head), _dp(tab), nR))
     t = tab.reshape(5, nR)
     return {"R_min": head[0], "R_max": head[1], "R_tap": head[2], "tap_cf": head[3], "R2": t[0], "c0": t[1],
             "c1": t[2], "c2": t[3], "c3": t[4]}

@@ -472,3 +472,27 @@ def stem_peng12_srtio3():
 def stem_kirkland_srtio3():
     """As stem_peng12_srtio3 with the Kirkland (0-12) parameterisation (potential_type 4)."""
     return _stem_potential(4, 25)
+
+
+def stem_ions_srtio3():
+    """STEM ADF through SrTiO3(001) with ionic charges (Sr 2+, Ti 4+, O 2-, Peng's ionic
+    coefficients), 256^2 grid, 3 x 3 probes, two thicknesses, two phonon configurations."""
+    import numpy as np
+    p = _stem_potential(6, 27)
+    a = np.array(p.spec_atoms, dtype=np.float64)
+    q = {38: 2, 22: 4, 8: -2}
+    a[:, 7] = [q[int(z)] for z in a[:, 0]]
+    p.spec_atoms = a
+    return p
+
+
+def ew_ions_si001():
+    """Exit wave (EWRS) of Si(001) with every second atom a Si 4+ ion and a charge that has no ionic
+    table (Si 2+, which the reference treats as neutral) on the others, 256^2 grid."""
+    import numpy as np
+    p = _ew_potential(6, 28)
+    a = np.array(p.spec_atoms, dtype=np.float64)
+    a[0::2, 7] = 4
+    a[1::2, 7] = 2
+    p.spec_atoms = a
+    return p

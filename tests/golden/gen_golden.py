@@ -27,7 +27,8 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    cbed_si001, cbei_si001, ewrs_two_beams_si001, ewrs_user_wave_si001, hrtem_user_wave_si001,
                    ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3, ew_monolayer_au,
                    stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001,
-                   ew_doyle_si001, ew_peng4_si001, ew_kirkland_si001, stem_peng12_srtio3, stem_kirkland_srtio3)
+                   ew_doyle_si001, ew_peng4_si001, ew_kirkland_si001, stem_peng12_srtio3, stem_kirkland_srtio3,
+                   stem_ions_srtio3, ew_ions_si001)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -68,7 +69,8 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("ew_wpo_si001", ew_wpo_si001), ("ew_bwl_si001", ew_bwl_si001), ("stem_bwl_srtio3", stem_bwl_srtio3),
              ("hrtem_bwl_si001", hrtem_bwl_si001), ("ew_doyle_si001", ew_doyle_si001), ("ew_peng4_si001", ew_peng4_si001),
              ("ew_kirkland_si001", ew_kirkland_si001), ("stem_peng12_srtio3", stem_peng12_srtio3),
-             ("stem_kirkland_srtio3", stem_kirkland_srtio3))
+             ("stem_kirkland_srtio3", stem_kirkland_srtio3), ("stem_ions_srtio3", stem_ions_srtio3),
+             ("ew_ions_si001", ew_ions_si001))
 
 SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
              ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))
@@ -113,6 +115,16 @@ def potential_table_fixtures(rec):
                 t = R.atom_type(p, Z, 1)
                 rec[f"tab_pt{pt}_Z{Z}_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
                 rec[f"tab_pt{pt}_Z{Z}_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
+    # ionic tables (Peng 0-4 ions; any potential_type): charges with and without an ionic entry
+    for pt, fn, Zq in ((6, stem_small, ((8, -2), (8, -1), (22, 4), (22, 2), (38, 2), (38, 1))),
+                       (4, ew_small, ((14, 4), (14, 1)))):
+        p = fn()
+        p.potential_type = pt
+        for Z, q in Zq:
+            t = R.atom_type(p, Z, 1, charge=q)
+            key = f"tab_ion_pt{pt}_Z{Z}_q{q}"
+            rec[key + "_head"] = np.array([t["R_min"], t["R_max"], t["R_tap"], t["tap_cf"]])
+            rec[key + "_tab"] = np.stack([t[k] for k in ("R2", "c0", "c1", "c2", "c3")])
 
 
 def add_only(names):

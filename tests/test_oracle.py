@@ -49,6 +49,22 @@ def test_spline_tables_other_parameterisations(golden, pt):
                 assert np.all(np.abs(got[tiny]) < 1e-12 * np.abs(ref[i]).max())
 
 
+ION_TABLES = [(6, 8, -2), (6, 8, -1), (6, 22, 4), (6, 22, 2), (6, 38, 2), (6, 38, 1), (4, 14, 4), (4, 14, 1)]
+
+
+@pytest.mark.parametrize("pt,Z,q", ION_TABLES)
+def test_ionic_spline_tables_bit_exact(golden, pt, Z, q):
+    """Peng's ionic tables (Sr 2+, Ti 2+/4+, O 1-/2-, Si 4+) and charges without an ionic entry
+    (Sr 1+, Si 1+: the neutral table), with Lobato and Kirkland neutral atoms, bit-identical."""
+    p = small_stem() if pt == 6 else specimens.hrtem_si001(nx=128, ny=128, na=2, nb=2, nc=2)
+    grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)
+    t = O.atom_table(Z, grid.dRx, potential_type=pt, charge=q)
+    key = f"tab_ion_pt{pt}_Z{Z}_q{q}"
+    assert np.float32(t["R_max"]) == np.float32(golden[key + "_head"][1])
+    for i, k in enumerate(("R2", "c0", "c1", "c2", "c3")):
+        np.testing.assert_array_equal(np.float32(t[k]), golden[key + "_tab"][i].astype(np.float32))
+
+
 def test_projected_potential_float_bit_exact(golden):
     p = small_stem()
     grid = O.Grid(p.nx, p.ny, p.spec_lx, p.spec_ly)

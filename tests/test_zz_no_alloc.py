@@ -25,7 +25,10 @@ def _noalloc(lib, Z, dR, nR, torch, pt=6):
     stream = torch.cuda.current_stream()
     args = (z.ctypes.data_as(capi.P_int), z.size, float(dR), 0.015, nR, heads.ctypes.data_as(capi.P_double),
             C.c_void_p(d_tab.data_ptr()), C.c_void_p(stream.cuda_stream))
-    rc = lib.mt_spline_tables_noalloc(*args) if pt == 6 else lib.mt_spline_tables_noalloc_ex(pt, *args)
+    if pt == 6:
+        rc = lib.mt_spline_tables_noalloc(*args)
+    else:  # (potential_type, Z, charge = NULL for neutral atoms, n, ...)
+        rc = lib.mt_spline_tables_noalloc_ex(pt, args[0], None, *args[1:])
     capi.check(rc)
     stream.synchronize()
     return heads, d_tab.cpu().numpy().reshape(z.size, 5, nR)
