@@ -128,14 +128,21 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         if (m_.is_EW()) d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
-        niter_ = m_.number_conf() * m_.nrot;
+        niter_ = m_.number_conf() * m_.nrot * (int)(m_.si_x.size() * m_.ti_x.size());
         if (m_.is_convergent_wave()) {
-            // convergent beams at iw_x/iw_y, summed (Incident_Wave::operator(), src/incident_wave.cuh:72-90)
+            // convergent beams at iw_x/iw_y, summed (Incident_Wave::operator(), src/incident_wave.cuh:72-90);
+            // one set of beams per source point (beam_x = iw_x + qs.x in the working precision,
+            // src/tem_simulation.cuh:233-237), one source point without full integration
             const int nb = (int)m_.iw_x.size();
             if (nb <= 0 || m_.iw_y.size() != m_.iw_x.size()) fail(MT_ERR_INVALID_ARG, "convergent wave needs iw_x/iw_y");
-            std::vector<float2> beam(nb);
-            for (int i = 0; i < nb; i++)
-                beam[i] = make_float2(m_.grid.exp_factor_Rx(m_.iw_x[i]), m_.grid.exp_factor_Ry(m_.iw_y[i]));
+            const size_t ns = m_.si_x.size();
+            std::vector<float2> beam(ns * nb);
+            for (size_t s = 0; s < ns; s++)
+                for (int i = 0; i < nb; i++) {
+                    const float bx = (float)((double)m_.iw_x[i] + m_.si_x[s]);
+                    const float by = (float)((double)m_.iw_y[i] + m_.si_y[s]);
+                    beam[s * nb + i] = make_float2(m_.grid.exp_factor_Rx(bx), m_.grid.exp_factor_Ry(by));
+                }
             d_beam_.upload(beam.data(), beam.size(), stream_);
             if (nb > 1) d_beams_psi_.alloc((size_t)nb * nxy);
             probe_norm_ = aperture_norm();
@@ -1030,7 +1037,16 @@ void Engine::run_ew(ConfData& cd) {
     const size_t rblock = (size_t)(cd.n_slice + (int)cd.thick_z_back_prop.size()) * pl;
     // beam rotations of PED / HCTEM (Multislice::PED_HCTEM, src/tem_simulation.cuh:274-300); one
     // pass otherwise
+    // CBED/CBEI under full integration: every (source point, defocus point) pair is a slice loop of
+    // its own, weighted by the product of the two quadrature weights (Multislice::CBED_CBEI,
+    // src/tem_simulation.cuh:226-251); one pass with the configuration's weight otherwise
+    const int n_si = (int)m_.si_x.size(), n_ti = (int)m_.ti_x.size();
+    const bool full = conv && (n_si * n_ti > 1);
+    const double w_pr = w;
     for (int r = 0; r < m_.nrot; r++) {
+    for (int ip = 0; ip < (full ? n_si * n_ti : 1); ip++) {
+    const int is = ip / n_ti, it = ip % n_ti;
+    const double w = full ? (double)(float)(w_pr * m_.si_w[is] * m_.ti_w[it]) : w_pr;
     const float2* prop = cd.prop.p + (size_t)r * rblock;
     const float2* ramp = m_.ramp_needed(r) ? d_ramp_.p + (size_t)r * nxy : nullptr;
     if (conv) {
@@ -1040,8 +1056,8 @@ void Engine::run_ew(ConfData& cd) {
         cp.nprobe = nb;
         cp.in = nullptr;
         cp.out = (nb > 1) ? d_beams_psi_.p : d_psi_.p;
-        cp.beam = d_beam_.p;
-        cp.probe = probe_params(cd.probe_c_c_10[0], cd.probe_nz_c10[0], false);
+        cp.beam = d_beam_.p + (size_t)is * nb;
+        cp.probe = probe_params(cd.probe_c_c_10[it], cd.probe_nz_c10[it], false);
         cols(COL_INVERSE | COL_STORE, cp);
         if (nb > 1) launch_sum_waves(d_beams_psi_.p, nb, nxy, d_psi_.p, stream_);
     }
@@ -1113,6 +1129,7 @@ void Engine::run_ew(ConfData& cd) {
                              sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
     }
     iter_ += 1;
+    }
     }
     check_cancel();
 }

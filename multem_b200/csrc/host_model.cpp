@@ -353,6 +353,10 @@ void LensF::from_input(const mt_lens& l) {
     inner_aper_ang = (float)((float)l.inner_aper_ang * kMrad);
     outer_aper_ang = (float)((float)l.outer_aper_ang * kMrad);
     si_sigma = (float)l.si_sigma;
+    si_a = (float)l.si_a;
+    si_beta = (float)l.si_beta;
+    si_rad_npts = l.si_rad_npts;
+    si_azm_npts = l.si_azm_npts;
     ti_a = (float)l.ti_a;
     ti_sigma = (float)l.ti_sigma;
     ti_beta = (float)l.ti_beta;
@@ -368,6 +372,11 @@ void LensF::set_input_data(float E_0, const GridF& grid) {
     ti_sigma = std::max(0.0f, ti_sigma);
     ti_beta = std::max(0.0f, ti_beta);
     ti_npts = std::max(1, ti_npts);
+    si_a = std::max(0.0f, std::min(1.0f, si_a));
+    si_sigma = std::max(0.0f, si_sigma);
+    si_beta = std::max(0.0f, si_beta);
+    si_rad_npts = std::max(1, si_rad_npts);
+    si_azm_npts = std::max(1, si_azm_npts);
     lambda = lambda_f(E_0);
     const double L = (double)lambda;
     auto cc = [&](float c, double f) -> float { return is_zero_f(c) ? 0.0f : (float)(f * (double)c); };
@@ -529,6 +538,85 @@ void gauss_hermite(int n, std::vector<double>& x, std::vector<double>& w) {
         x[i] = t;
         w[i] = 1.0 / sum;
     }
+}
+
+void gauss_laguerre1(int n, std::vector<double>& x, std::vector<double>& w) {
+    // Jacobi matrix of the monic Laguerre polynomials L_k^(1): diagonal 2k + 2, off-diagonal
+    // sqrt(k (k + 1)); nodes by Sturm-count bisection, weights by the Christoffel sum of the
+    // orthonormal polynomials (mu_0 = Gamma(2) = 1)
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    auto diag = [](int k) { return 2.0 * k + 2.0; };
+    auto off2 = [](int k) { return (double)k * (k + 1); };  // squared off-diagonal between k-1 and k
+    auto below = [&](double s) {
+        int c = 0;
+        double d = 1.0;
+        for (int k = 0; k < n; k++) {
+            d = (diag(k) - s) - (k > 0 ? off2(k) / d : 0.0);
+            if (d == 0.0) d = -1e-300;
+            if (d < 0.0) c++;
+        }
+        return c;
+    };
+    const double R = 4.0 * n + 4.0;  // every eigenvalue lies in (0, R) (Gershgorin)
+    for (int i = 0; i < n; i++) {
+        double lo = 0.0, hi = R;
+        for (int it = 0; it < 200 && hi - lo > 1e-15 * std::max(1.0, std::fabs(lo)); it++) {
+            const double mid = 0.5 * (lo + hi);
+            if (below(mid) > i) hi = mid; else lo = mid;
+        }
+        const double t = 0.5 * (lo + hi);
+        double p0 = 1.0, p1 = (n > 1) ? (t - diag(0)) / std::sqrt(off2(1)) : 0.0;
+        double sum = p0 * p0 + p1 * p1;
+        for (int k = 1; k + 1 < n; k++) {
+            const double p2 = ((t - diag(k)) * p1 - std::sqrt(off2(k)) * p0) / std::sqrt(off2(k + 1));
+            sum += p2 * p2;
+            p0 = p1;
+            p1 = p2;
+        }
+        x[i] = t;
+        w[i] = 1.0 / sum;
+    }
+}
+
+// Spatial part of cond_lens_temporal_spatial_quadratures (src/cpu_fcns.hpp:1573-1626): the source
+// spread is a 2-D Gaussian (share si_a, sigma si_sigma) plus an exponential (si_beta) component;
+// the radius is integrated with the generalized Laguerre rule of weight r exp(-b_q r) (quadrature
+// type 25 with alpha = 1: nodes t / b_q, weights / b_q^2), b_q = 1 / sigma_t,
+// sigma_t^2 = (2 si_a si_sigma^2 + 6 (1 - si_a) si_beta^2) / 6, each weight times the ratio of the
+// spread function to exp(-b_q r); the azimuth with si_azm_npts equal steps of 2 pi / si_azm_npts.
+void spatial_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& y, std::vector<double>& w) {
+    x.assign(1, 0.0);
+    y.assign(1, 0.0);
+    w.assign(1, 1.0);
+    if (!((L.si_rad_npts > 1 || L.si_azm_npts > 1) && (!is_zero_f(L.si_sigma) || !is_zero_f(L.si_beta)))) return;
+    const double kTwoPi = 6.283185307179586476925;
+    const double s2 = (double)L.si_sigma * L.si_sigma, b2 = (double)L.si_beta * L.si_beta;
+    const double a = is_zero_f(L.si_sigma) ? 0.0 : L.si_a / (kTwoPi * s2);
+    const double b = is_zero_f(L.si_sigma) ? 0.0 : 0.5 / s2;
+    const double c = is_zero_f(L.si_beta) ? 0.0 : (1.0 - L.si_a) / (kTwoPi * b2);
+    const double d = is_zero_f(L.si_beta) ? 0.0 : 1.0 / L.si_beta;
+    const double sigma_t = std::sqrt((2.0 * L.si_a * s2 + 6.0 * (1.0 - L.si_a) * b2) / 6.0);
+    const double b_q = 1.0 / sigma_t;
+    std::vector<double> r, wr;
+    gauss_laguerre1(L.si_rad_npts, r, wr);
+    for (int i = 0; i < L.si_rad_npts; i++) {
+        r[i] /= b_q;
+        wr[i] /= b_q * b_q;
+        const double ra = std::fabs(r[i]);
+        wr[i] *= a * std::exp(-b * ra * ra + b_q * ra) + c * std::exp(-d * ra + b_q * ra);
+    }
+    const double h = kTwoPi / L.si_azm_npts;
+    x.clear();
+    y.clear();
+    w.clear();
+    for (int i = 0; i < L.si_rad_npts; i++)
+        for (int j = 0; j < L.si_azm_npts; j++) {
+            const double th = j * h;
+            x.push_back(r[i] * std::cos(th));
+            y.push_back(r[i] * std::sin(th));
+            w.push_back(wr[i] * h);
+        }
 }
 
 // Temporal part of cond_lens_temporal_spatial_quadratures (src/cpu_fcns.hpp:1540-1571): the
@@ -963,11 +1051,10 @@ Model build_model(const mt_input_multislice* in) {
     // full integration, or with spatial incoherence only, the condenser has one defocus point
     if (m.is_EW()) m.illumination_model = 1;
     if ((m.is_CBED() || m.is_CBEI()) && m.illumination_model != 4) m.illumination_model = 1;
-    if ((m.is_CBED() || m.is_CBEI()) && m.illumination_model == 4)
-        fail(MT_ERR_UNSUPPORTED, "CBED/CBEI with full integration (source and defocus quadratures) is not implemented");
     if (is_zero_f(m.cond_lens.si_sigma)) m.temporal_spatial_incoh = 2;
     const bool full_integration = (m.illumination_model == 4);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.cond_lens.ti_npts = 1;
+    if (!full_integration || m.temporal_spatial_incoh == 2) m.cond_lens.si_rad_npts = m.cond_lens.si_azm_npts = 1;
     m.cond_lens.set_input_data(m.E_0, m.grid);
     if (!full_integration || m.temporal_spatial_incoh == 3) m.obj_lens.ti_npts = 1;
     m.obj_lens.set_input_data(m.E_0, m.grid);
@@ -975,6 +1062,13 @@ Model build_model(const mt_input_multislice* in) {
     // Multislice::STEM_ISTEM integrates the defocus spread only under full integration, and not
     // in its coherent-contribution branch, which comes first (src/tem_simulation.cuh:115-176)
     if (m.is_scanning() && full_integration && !m.pn_coh_contrib) temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
+    // CBED/CBEI under full integration: every configuration runs every (source point, defocus
+    // point) pair with the beams moved by the source offset (Multislice::CBED_CBEI,
+    // src/tem_simulation.cuh:203-259)
+    if ((m.is_CBED() || m.is_CBEI()) && full_integration) {
+        temporal_quadrature(m.cond_lens, m.ti_x, m.ti_w);
+        spatial_quadrature(m.cond_lens, m.si_x, m.si_y, m.si_w);
+    }
     m.cond_lens.zero_defocus_plane = A.size() ? m.cond_lens.get_zero_defocus_plane(A.z_min, A.z_max) : 0.0f;
     m.cond_lens.zero_defocus_type = 4;
     m.obj_lens.set_input_data(m.E_0, m.grid);

@@ -49,6 +49,8 @@ struct LensF {
     float c_50 = 0, c_52 = 0, phi_52 = 0, c_54 = 0, phi_54 = 0, c_56 = 0, phi_56 = 0;
     float inner_aper_ang = 0, outer_aper_ang = 0;
     float si_sigma = 0;
+    float si_a = 1, si_beta = 0;     // source spread (spatial incoherence): Gaussian share, exponential
+    int si_rad_npts = 1, si_azm_npts = 1;
     float ti_a = 1, ti_sigma = 0, ti_beta = 0;  // defocus spread (temporal incoherence)
     int ti_npts = 1;
     int zero_defocus_type = 1;
@@ -109,6 +111,8 @@ struct Model {
     // defocus offsets (A) and weights of the condenser's temporal-incoherence quadrature; one
     // point (0, 1) unless STEM integrates the illumination in full
     std::vector<double> ti_x{0.0}, ti_w{1.0};
+    // source-spread quadrature of CBED/CBEI under full integration: beam offsets (A) and weights
+    std::vector<double> si_x{0.0}, si_y{0.0}, si_w{1.0};
     // HRTEM image formation (Microscope_Effects): 1 coherent CTF, 2 partially coherent CTF
     // (envelopes), 4 numerical integration over the objective's defocus spread; obj_c10 and obj_w
     // are the defocus and weight of each point (one point unless 4)
@@ -208,6 +212,9 @@ Model build_prop_model(const mt_input_multislice* in);
 void snap_incident_angle(Model& m);
 void gauss_hermite(int n, std::vector<double>& x, std::vector<double>& w);
 void temporal_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& w);
+// Generalized Gauss-Laguerre rule of weight t exp(-t) on (0, inf) (alpha = 1): nodes and weights.
+void gauss_laguerre1(int n, std::vector<double>& x, std::vector<double>& w);
+void spatial_quadrature(const LensF& L, std::vector<double>& x, std::vector<double>& y, std::vector<double>& w);
 void hrtem_ctf_points(Model& m);
 
 // Per-element spline-table header needed on the host (R_max drives statistics and footprints).

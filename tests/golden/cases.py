@@ -496,3 +496,31 @@ def ew_ions_si001():
     a[1::2, 7] = 2
     p.spec_atoms = a
     return p
+
+
+def _full_integration(p):
+    """Condenser defocus spread (3 points, sigma 20 A) and source spread (2 radial x 3 azimuthal
+    points, sigma 0.15 A) under full integration (illumination_model 4, temporal_spatial_incoh 1)."""
+    p.illumination_model = 4
+    p.temporal_spatial_incoh = 1
+    p.cond_lens_ti_sigma = 20.0
+    p.cond_lens_ti_npts = 3
+    p.cond_lens_si_sigma = 0.15
+    p.cond_lens_si_rad_npts = 2
+    p.cond_lens_si_azm_npts = 3
+    return p
+
+
+def cbed_full_si001():
+    """cbed_si001 with the condenser's defocus and source spreads integrated (18 incident waves per
+    phonon configuration, Multislice::CBED_CBEI's full-integration branch)."""
+    return _full_integration(cbed_si001())
+
+
+def cbei_full_si001():
+    """cbei_si001 with the condenser's and the objective's defocus spreads integrated
+    (temporal_spatial_incoh 2: with the source spread too, the reference's objective-lens spatial
+    quadrature is empty and its images are zero, an input the engine refuses)."""
+    p = _full_integration(cbei_si001())
+    p.temporal_spatial_incoh = 2
+    return p
