@@ -47,6 +47,7 @@ class OutputBuffers:
         self.image_coh = np.zeros(max(1, d.n_thick * d.n_detector * nxy)) if d.has_image_coh else None
         self.m2psi_tot = np.zeros(max(1, d.n_thick * nxy)) if d.has_m2psi_tot else None
         self.psi_coh = np.zeros(max(1, 2 * d.n_thick * nxy)) if d.has_psi_coh else None
+        self.m2psi_coh = np.zeros(max(1, d.n_thick * nxy)) if d.has_m2psi_coh else None
         o = capi.MtOutputMultislice()
         o.x, o.y, o.thick = _dp(self.x), _dp(self.y), _dp(self.thick)
         if self.image_tot is not None:
@@ -57,6 +58,8 @@ class OutputBuffers:
             o.m2psi_tot = _dp(self.m2psi_tot)
         if self.psi_coh is not None:
             o.psi_coh = _dp(self.psi_coh)
+        if self.m2psi_coh is not None:
+            o.m2psi_coh = _dp(self.m2psi_coh)
         self.c = o
 
     def to_dict(self):
@@ -77,6 +80,8 @@ class OutputBuffers:
             if self.psi_coh is not None:
                 r = self.psi_coh.reshape(d.n_thick, nx, ny, 2)[it]
                 e["psi_coh"] = (r[..., 0] + 1j * r[..., 1]).T.copy()
+            if self.m2psi_coh is not None:
+                e["m2psi_coh"] = self.m2psi_coh.reshape(d.n_thick, nx, ny)[it].T.copy()
             res["data"].append(e)
         return res
 

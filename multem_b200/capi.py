@@ -79,13 +79,13 @@ class MtInputMultislice(C.Structure):
 class MtOutputDims(C.Structure):
     _fields_ = [("n_thick", c_int), ("n_detector", c_int), ("nx", c_int), ("ny", c_int),
                 ("has_image_tot", c_int), ("has_image_coh", c_int), ("has_m2psi_tot", c_int),
-                ("has_psi_coh", c_int), ("n_x", c_int), ("n_y", c_int)]
+                ("has_psi_coh", c_int), ("n_x", c_int), ("n_y", c_int), ("has_m2psi_coh", c_int)]
 
 
 class MtOutputMultislice(C.Structure):
     _fields_ = [("dx", c_double), ("dy", c_double), ("x", P_double), ("y", P_double), ("thick", P_double),
                 ("image_tot", P_double), ("image_coh", P_double), ("m2psi_tot", P_double),
-                ("psi_coh", P_double)]
+                ("psi_coh", P_double), ("m2psi_coh", P_double)]
 
 
 MT_OK = 0

@@ -126,6 +126,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         batch_ = 1;
         const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
         if (m_.is_EW()) d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
+        if (m_.pn_coh_contrib && !m_.is_EW()) d_ew_cohpsi_.alloc((size_t)n_thk * onxy * 2);
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
         niter_ = m_.number_conf() * m_.nrot * (int)(m_.si_x.size() * m_.ti_x.size());
@@ -218,6 +219,7 @@ void Engine::reset() {
     if (d_coh_.p) MTB_CUDA(cudaMemsetAsync(d_coh_.p, 0, sizeof(float2) * d_coh_.n, stream_));
     if (d_ew_psi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_psi_.p, 0, sizeof(double) * d_ew_psi_.n, stream_));
     if (d_ew_m2_.p) MTB_CUDA(cudaMemsetAsync(d_ew_m2_.p, 0, sizeof(double) * d_ew_m2_.n, stream_));
+    if (d_ew_cohpsi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_cohpsi_.p, 0, sizeof(double) * d_ew_cohpsi_.n, stream_));
     iter_ = 0;
     cancel_ = false;
     synchronize();
@@ -1127,6 +1129,11 @@ void Engine::run_ew(ConfData& cd) {
         launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
                              m_.is_EW() ? d_ew_psi_.p + (size_t)ithk * onxy * 2 : nullptr,
                              sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
+        // coherent contribution of ED / CBED / PED: the configuration-weighted wave (add_scale_psi_coh,
+        // src/output_multislice.hpp:770-780), kept cropped and shifted like the intensity
+        if (d_ew_cohpsi_.p)
+            launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, 0,
+                                 d_ew_cohpsi_.p + (size_t)ithk * onxy * 2, nullptr, stream_);
     }
     iter_ += 1;
     }
@@ -1152,6 +1159,7 @@ mt_output_dims output_dims(const Model& m_) {
         d.nx = m_.out_ix_e - m_.out_ix_0;
         d.ny = m_.out_iy_e - m_.out_iy_0;
         d.has_psi_coh = m_.is_EW() ? 1 : 0;
+        d.has_m2psi_coh = (m_.pn_coh_contrib && !m_.is_EW()) ? 1 : 0;
         d.has_m2psi_tot = m_.is_EW_SC() ? 0 : 1;
         d.n_x = d.nx;
         d.n_y = d.ny;
@@ -1202,6 +1210,13 @@ void Engine::write_output(mt_output_multislice* out) {
             MTB_CUDA(cudaMemcpy(out->psi_coh, d_ew_psi_.p, sizeof(double) * d_ew_psi_.n, cudaMemcpyDeviceToHost));
         if (out->m2psi_tot && d.has_m2psi_tot)
             MTB_CUDA(cudaMemcpy(out->m2psi_tot, d_ew_m2_.p, sizeof(double) * d_ew_m2_.n, cudaMemcpyDeviceToHost));
+        if (out->m2psi_coh && d.has_m2psi_coh) {
+            // |configuration-averaged wave|^2 of the output window (set_m2psi_coh's last branch,
+            // src/wave_function.cuh:219-226: the crop and shift commute with the average)
+            std::vector<double> h(d_ew_cohpsi_.n);
+            MTB_CUDA(cudaMemcpy(h.data(), d_ew_cohpsi_.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < h.size() / 2; i++) out->m2psi_coh[i] = h[2 * i] * h[2 * i] + h[2 * i + 1] * h[2 * i + 1];
+        }
     }
 }
 

@@ -158,6 +158,7 @@ class Engine {
     DevBuf<double> d_image_;         // [n_thk][n_det][n_scan]
     DevBuf<double> d_ew_psi_;        // [n_thk][out_nxy][2]
     DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
+    DevBuf<double> d_ew_cohpsi_;     // ED/CBED/PED with pn_coh_contrib: weighted wave sum [n_thk][out_nxy][2]
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny per rotation (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)

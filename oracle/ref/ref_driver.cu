@@ -255,6 +255,7 @@ int run(const mt_input_multislice* in, int nthreads, mt_output_multislice* out, 
         dims->has_image_coh = (int)om.image_coh.size() > 0;
         dims->has_m2psi_tot = (int)om.m2psi_tot.size() > 0;
         dims->has_psi_coh = (int)om.psi_coh.size() > 0;
+        dims->has_m2psi_coh = (int)om.m2psi_coh.size() > 0 && om.pn_coh_contrib && !om.is_EWFS_EWRS();
         dims->n_x = (int)om.x.size();
         dims->n_y = (int)om.y.size();
     }
@@ -273,6 +274,8 @@ int run(const mt_input_multislice* in, int nthreads, mt_output_multislice* out, 
             for (int idet = 0; idet < om.ndetector; idet++)
                 copy_real(om.image_coh[ithk].image[idet], out->image_coh + (ithk * om.ndetector + idet) * nxy, nxy);
         if (out->m2psi_tot && om.m2psi_tot.size()) copy_real(om.m2psi_tot[ithk], out->m2psi_tot + ithk * nxy, nxy);
+        if (out->m2psi_coh && om.m2psi_coh.size() && om.pn_coh_contrib && !om.is_EWFS_EWRS())
+            copy_real(om.m2psi_coh[ithk], out->m2psi_coh + ithk * nxy, nxy);
         // psi_coh is held at the full grid size; like set_struct_multislice (ilc_multem.cu:382-481)
         // only the first nx*ny values of the output area are returned
         if (out->psi_coh && om.psi_coh.size()) copy_cplx(om.psi_coh[ithk], out->psi_coh + 2 * ithk * nxy, nxy);

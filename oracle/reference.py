@@ -96,6 +96,9 @@ def run(params, precision=1, nthreads=1, device=False):
     if d.has_psi_coh:
         res["psi_coh_raw"] = np.zeros((d.n_thick, d.nx, d.ny, 2))
         o.psi_coh = _dp(res["psi_coh_raw"])
+    if d.has_m2psi_coh:
+        res["m2psi_coh"] = np.zeros((d.n_thick, d.nx, d.ny))
+        o.m2psi_coh = _dp(res["m2psi_coh"])
     if device:
         _chk(lib().mtref_run_device(C.byref(s), C.byref(o)))
     else:
@@ -108,6 +111,8 @@ def run(params, precision=1, nthreads=1, device=False):
         res["image_coh"] = np.swapaxes(res["image_coh"], -1, -2)
     if "m2psi_tot" in res:
         res["m2psi_tot"] = np.swapaxes(res["m2psi_tot"], -1, -2)
+    if "m2psi_coh" in res:
+        res["m2psi_coh"] = np.swapaxes(res["m2psi_coh"], -1, -2)
     if "psi_coh_raw" in res:
         r = res.pop("psi_coh_raw")
         res["psi_coh"] = np.swapaxes(r[..., 0] + 1j * r[..., 1], -1, -2)

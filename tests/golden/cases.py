@@ -524,3 +524,25 @@ def cbei_full_si001():
     p = _full_integration(cbei_si001())
     p.temporal_spatial_incoh = 2
     return p
+
+
+def _coherent(p):
+    p.pn_coh_contrib = 1
+    p.pn_nconf = 4
+    return p
+
+
+def ed_coh_si001():
+    """ed_si001 over four phonon configurations with the coherent contribution (pn_coh_contrib 1):
+    m2psi_coh, |configuration-averaged psi_hat|^2, beside m2psi_tot."""
+    return _coherent(ed_si001())
+
+
+def cbed_coh_si001():
+    """cbed_si001 over four phonon configurations with the coherent contribution."""
+    return _coherent(cbed_si001())
+
+
+def ped_coh_si001():
+    """ped_si001 over four phonon configurations with the coherent contribution."""
+    return _coherent(ped_si001())

@@ -28,7 +28,8 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    ew_rot_si001, stem_rot_srtio3, ped_si001, hctem_si001, istem_srtio3, ew_monolayer_au,
                    stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001,
                    ew_doyle_si001, ew_peng4_si001, ew_kirkland_si001, stem_peng12_srtio3, stem_kirkland_srtio3,
-                   stem_ions_srtio3, ew_ions_si001, cbed_full_si001, cbei_full_si001)
+                   stem_ions_srtio3, ew_ions_si001, cbed_full_si001, cbei_full_si001, ed_coh_si001,
+                   cbed_coh_si001, ped_coh_si001)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -71,7 +72,8 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("ew_kirkland_si001", ew_kirkland_si001), ("stem_peng12_srtio3", stem_peng12_srtio3),
              ("stem_kirkland_srtio3", stem_kirkland_srtio3), ("stem_ions_srtio3", stem_ions_srtio3),
              ("ew_ions_si001", ew_ions_si001), ("cbed_full_si001", cbed_full_si001),
-             ("cbei_full_si001", cbei_full_si001))
+             ("cbei_full_si001", cbei_full_si001), ("ed_coh_si001", ed_coh_si001), ("cbed_coh_si001", cbed_coh_si001),
+             ("ped_coh_si001", ped_coh_si001))
 
 SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
              ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))
@@ -99,7 +101,7 @@ def full_runs(rec, names=None):
         p = fn()
         for prec in (1, 2):
             out = R.run(p, precision=prec, nthreads=8)
-            for k in ("image_tot", "image_coh", "psi_coh", "m2psi_tot", "thick", "x", "y"):
+            for k in ("image_tot", "image_coh", "psi_coh", "m2psi_tot", "m2psi_coh", "thick", "x", "y"):
                 if k in out:
                     v = out[k]
                     rec[f"{name}_run_p{prec}_{k}"] = v.astype(np.complex64 if np.iscomplexobj(v) else np.float64)
