@@ -126,7 +126,11 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         batch_ = 1;
         const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
         if (m_.is_EW()) d_ew_psi_.alloc((size_t)n_thk * onxy * 2);
-        if (m_.pn_coh_contrib && !m_.is_EW()) d_ew_cohpsi_.alloc((size_t)n_thk * onxy * 2);
+        if (m_.pn_coh_contrib && !m_.is_EW() && !m_.is_imaging()) d_ew_cohpsi_.alloc((size_t)n_thk * onxy * 2);
+        if (m_.pn_coh_contrib && m_.is_imaging()) {
+            d_coh_img_.alloc((size_t)n_thk * nxy);
+            d_coh_m2_.alloc((size_t)n_thk * onxy);
+        }
         d_ew_m2_.alloc((size_t)n_thk * onxy);
         d_tmp_.alloc(nxy);
         niter_ = m_.number_conf() * m_.nrot * (int)(m_.si_x.size() * m_.ti_x.size());
@@ -220,6 +224,7 @@ void Engine::reset() {
     if (d_ew_psi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_psi_.p, 0, sizeof(double) * d_ew_psi_.n, stream_));
     if (d_ew_m2_.p) MTB_CUDA(cudaMemsetAsync(d_ew_m2_.p, 0, sizeof(double) * d_ew_m2_.n, stream_));
     if (d_ew_cohpsi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_cohpsi_.p, 0, sizeof(double) * d_ew_cohpsi_.n, stream_));
+    if (d_coh_img_.p) MTB_CUDA(cudaMemsetAsync(d_coh_img_.p, 0, sizeof(float2) * d_coh_img_.n, stream_));
     iter_ = 0;
     cancel_ = false;
     synchronize();
@@ -1093,6 +1098,9 @@ void Engine::run_ew(ConfData& cd) {
         cb.Px = prop + (size_t)(cd.n_slice + ithk) * pl;
         cb.Py = cb.Px + nx;
         if (m_.is_imaging()) {
+            // coherent contribution: the weighted wave of this thickness, imaged once at output
+            // (add_scale_psi_coh then set_m2psi_coh, src/wave_function.cuh:166-172, 210-218)
+            if (d_coh_img_.p) launch_axpy_wave(src, (float)w, nxy, d_coh_img_.p + (size_t)ithk * nxy, stream_);
             // image formation: transfer function per defocus point, inverse transform, |psi|^2
             // weighted (Microscope_Effects::operator(), src/microscope_effects.cuh:56-85)
             for (size_t j = 0; j < m_.obj_c10.size(); j++) {
@@ -1159,7 +1167,7 @@ mt_output_dims output_dims(const Model& m_) {
         d.nx = m_.out_ix_e - m_.out_ix_0;
         d.ny = m_.out_iy_e - m_.out_iy_0;
         d.has_psi_coh = m_.is_EW() ? 1 : 0;
-        d.has_m2psi_coh = (m_.pn_coh_contrib && !m_.is_EW()) ? 1 : 0;
+        d.has_m2psi_coh = (m_.pn_coh_contrib && m_.is_wave_sim() && !m_.is_EW()) ? 1 : 0;
         d.has_m2psi_tot = m_.is_EW_SC() ? 0 : 1;
         d.n_x = d.nx;
         d.n_y = d.ny;
@@ -1210,13 +1218,58 @@ void Engine::write_output(mt_output_multislice* out) {
             MTB_CUDA(cudaMemcpy(out->psi_coh, d_ew_psi_.p, sizeof(double) * d_ew_psi_.n, cudaMemcpyDeviceToHost));
         if (out->m2psi_tot && d.has_m2psi_tot)
             MTB_CUDA(cudaMemcpy(out->m2psi_tot, d_ew_m2_.p, sizeof(double) * d_ew_m2_.n, cudaMemcpyDeviceToHost));
-        if (out->m2psi_coh && d.has_m2psi_coh) {
+        if (out->m2psi_coh && d.has_m2psi_coh && d_coh_img_.p) {
+            coherent_image();
+            MTB_CUDA(cudaMemcpy(out->m2psi_coh, d_coh_m2_.p, sizeof(double) * d_coh_m2_.n, cudaMemcpyDeviceToHost));
+        } else if (out->m2psi_coh && d.has_m2psi_coh) {
             // |configuration-averaged wave|^2 of the output window (set_m2psi_coh's last branch,
             // src/wave_function.cuh:219-226: the crop and shift commute with the average)
             std::vector<double> h(d_ew_cohpsi_.n);
             MTB_CUDA(cudaMemcpy(h.data(), d_ew_cohpsi_.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < h.size() / 2; i++) out->m2psi_coh[i] = h[2 * i] * h[2 * i] + h[2 * i + 1] * h[2 * i + 1];
         }
+    }
+}
+
+// HRTEM / CBEI with pn_coh_contrib: the configuration-weighted wave of each thickness through the
+// objective, the same passes run_ew applies to each configuration's wave (back-propagation,
+// transfer function per defocus point, inverse transform, weighted |psi|^2), with weight 1 (the
+// ISTEM_CBEI_HRTEM branch of set_m2psi_coh, src/wave_function.cuh:210-218). The back-propagation
+// distance of a thickness does not depend on the configuration (z is never displaced).
+void Engine::coherent_image() {
+    const int nx = m_.grid.nx, ny = m_.grid.ny;
+    const size_t nxy = (size_t)nx * ny;
+    const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
+    MTB_CUDA(cudaMemsetAsync(d_coh_m2_.p, 0, sizeof(double) * d_coh_m2_.n, stream_));
+    const auto& TH = spec_->thicks();
+    std::vector<float2> tab((size_t)nx + ny);
+    DevBuf<float2> d_bp;
+    for (size_t t = 0; t < TH.size(); t++) {
+        prop_tables(TH[t].z_back_prop, tab.data(), tab.data() + nx, true, 0);
+        d_bp.upload(tab.data(), tab.size(), stream_);
+        for (size_t j = 0; j < m_.obj_c10.size(); j++) {
+            ColArgs cj{};
+            cj.ny = ny;
+            cj.nprobe = 1;
+            cj.g = gdev_;
+            cj.n_det = 0;
+            cj.in = d_coh_img_.p + t * nxy;
+            cj.out = d_tmp_.p;
+            cj.Px = d_bp.p;
+            cj.Py = d_bp.p + nx;
+            cj.P2 = d_ctf_.p + j * nxy;
+            cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cj);
+            RowArgs rb{};
+            rb.nx = nx;
+            rb.nprobe = 1;
+            rb.scale = 1.0f;
+            rb.in = d_tmp_.p;
+            rb.out = d_tmp_.p;
+            rows(ROW_INVERSE, rb);
+            launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e,
+                                 (double)(float)m_.obj_w[j], 0, nullptr, d_coh_m2_.p + t * onxy, stream_);
+        }
+        synchronize();  // the host table is rewritten for the next thickness
     }
 }
 

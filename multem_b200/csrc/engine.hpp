@@ -159,6 +159,9 @@ class Engine {
     DevBuf<double> d_ew_psi_;        // [n_thk][out_nxy][2]
     DevBuf<double> d_ew_m2_;         // [n_thk][out_nxy]
     DevBuf<double> d_ew_cohpsi_;     // ED/CBED/PED with pn_coh_contrib: weighted wave sum [n_thk][out_nxy][2]
+    DevBuf<float2> d_coh_img_;       // HRTEM/CBEI with pn_coh_contrib: weighted wave sum, row-pass layout [n_thk][nx*ny]
+    DevBuf<double> d_coh_m2_;        // its image through the objective [n_thk][out_nxy]
+    void coherent_image();
     DevBuf<float2> d_prop_bp_;       // back-propagation tables per thickness
     DevBuf<float2> d_ramp_;          // tilted beam: output phase ramp / ny per rotation (else empty)
     DevBuf<float> d_detmat_;         // matrix detectors [n_det][nx][ny] (else empty)

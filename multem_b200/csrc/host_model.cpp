@@ -958,9 +958,9 @@ Model build_model(const mt_input_multislice* in) {
     m.lambda = lambda_f(m.E_0);
     snap_incident_angle(m);
     if (m.is_EW()) m.pn_coh_contrib = true;
-    if ((m.is_imaging() || m.is_ISTEM()) && m.pn_coh_contrib)
-        fail(MT_ERR_UNSUPPORTED, "ISTEM/CBEI/HRTEM/HCTEM with pn_coh_contrib = 1 (the image of the coherent wave, "
-                                 "m2psi_coh) is not implemented; ED, CBED and PED have it");
+    if ((m.is_HCTEM() || m.is_ISTEM()) && m.pn_coh_contrib)
+        fail(MT_ERR_UNSUPPORTED, "ISTEM/HCTEM with pn_coh_contrib = 1 (the image of the coherent wave, m2psi_coh) "
+                                 "is not implemented; ED, CBED, PED, HRTEM and CBEI have it");
     if (m.pn_z && m.is_frozen_phonon()) m.clamps.push_back("pn_dim: z displacement switched off (no subslicing)");
     m.pn_z = false;  // no subslicing: pn_dim.z is switched off (input_multislice.cuh:705-708)
 

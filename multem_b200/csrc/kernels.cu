@@ -358,6 +358,20 @@ __global__ void sum_waves_kernel(const float2* __restrict__ src, int n, size_t n
     }
 }
 
+// dst += w * src over nxy complex values (add_scale, src/output_multislice.hpp:770-780)
+__global__ void axpy_wave_kernel(const float2* __restrict__ src, float w, size_t nxy, float2* __restrict__ dst) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nxy; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 v = src[i], d = dst[i];
+        dst[i] = make_float2(__fadd_rn(d.x, __fmul_rn(w, v.x)), __fadd_rn(d.y, __fmul_rn(w, v.y)));
+    }
+}
+
+void launch_axpy_wave(const float2* src, float w, size_t nxy, float2* dst, cudaStream_t s) {
+    axpy_wave_kernel<<<(unsigned)std::min<size_t>((nxy + 255) / 256, 148 * 8), 256, 0, s>>>(src, w, nxy, dst);
+    g_launches++;
+    MTB_CUDA(cudaGetLastError());
+}
+
 void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s) {
     sum_waves_kernel<<<(unsigned)std::min<size_t>((nxy + 255) / 256, 148 * 8), 256, 0, s>>>(src, n, nxy, dst);
     g_launches++;

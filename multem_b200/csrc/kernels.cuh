@@ -121,6 +121,8 @@ void launch_mul_tables(float2* a, const float2* b, size_t n, cudaStream_t s);
 
 // dst = sum over j < n of src[j * nxy + i] (the beams of a convergent incident wave, in order).
 void launch_sum_waves(const float2* src, int n, size_t nxy, float2* dst, cudaStream_t s);
+// dst[i] += w * src[i], i < nxy
+void launch_axpy_wave(const float2* src, float w, size_t nxy, float2* dst, cudaStream_t s);
 
 // STEM coherent images (Wave_Function::set_m2psi_coh, src/wave_function.cuh:189-209): for each
 // thickness and scan position, the detector sums of |psi_coh|^2 (weight 1) into

@@ -546,3 +546,14 @@ def cbed_coh_si001():
 def ped_coh_si001():
     """ped_si001 over four phonon configurations with the coherent contribution."""
     return _coherent(ped_si001())
+
+
+def hrtem_coh_si001():
+    """hrtem_coherent_si001 over four phonon configurations with the coherent contribution: m2psi_coh,
+    the objective's image of the configuration-averaged exit wave."""
+    return _coherent(hrtem_coherent_si001())
+
+
+def cbei_coh_si001():
+    """cbei_si001 over four phonon configurations with the coherent contribution."""
+    return _coherent(cbei_si001())

@@ -88,7 +88,7 @@ def test_unsupported_and_invalid_inputs_fail_loudly(field, value, status):
 @pytest.mark.parametrize("sim,fields", [
     (32, {"illumination_model": 3}),  # the reference's transmission-cross-coefficient branch computes nothing
     (32, {"illumination_model": 4, "temporal_spatial_incoh": 1, "cond_lens_si_sigma": 0.01}),  # its spatial quadrature is empty
-    (32, {"pn_coh_contrib": 1}),  # m2psi_coh
+    (42, {"pn_coh_contrib": 1}),  # HCTEM's m2psi_coh
 ])
 def test_image_formation_limits_are_refused(sim, fields):
     """Imaging and incident-wave variants outside what the engine implements fail with
