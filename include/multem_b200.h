@@ -179,9 +179,9 @@ typedef struct mt_output_dims {
     int n_x, n_y;                /* lengths of the x and y coordinate arrays: the output grid's
                                     axes, or every scan position for a STEM area scan (as the
                                     reference's output x/y, src/output_multislice.hpp:1207-1245) */
-    int has_m2psi_coh;           /* ED/CBED/PED with pn_coh_contrib: m2psi_coh[ithk][ny*nx], the
-                                    intensity of the configuration-averaged wave (set_m2psi_coh,
-                                    src/wave_function.cuh:189-227) */
+    int has_m2psi_coh;           /* ED/CBED/PED/HRTEM/CBEI with pn_coh_contrib: m2psi_coh[ithk][ny*nx],
+                                    the intensity of the configuration-averaged wave, or its image
+                                    through the objective (set_m2psi_coh, src/wave_function.cuh:189-227) */
 } mt_output_dims;
 
 /* Output buffers, caller-owned, sized from mt_output_dims (set_struct_multislice,
