@@ -204,6 +204,10 @@ typedef struct mt_engine mt_engine;
 /* ---- version / errors ---- */
 int mt_abi_version(void);
 const char* mt_last_error(void);
+/* Number of device allocations the library has made in this process (engine buffers and the
+ * scratch of the operator-level calls all come from its per-device memory pools); no
+ * counterpart in the reference. For callers that watch the library's allocations. */
+mt_status mt_device_alloc_count(long long* count);
 
 /* ---- whole simulation (ilc_multem / mt_run_multislice) ---- */
 
@@ -254,6 +258,13 @@ mt_status mt_engine_read_stem(mt_engine* eng, double* image_tot, size_t n);
 /* Cancel a run in progress from another thread (mt_stop_multislice, gui_multem/multem.cu:56-75).
  * The run returns MT_ERR_CANCELLED between launches. */
 mt_status mt_engine_cancel(mt_engine* eng);
+/* Bound (seconds, 0..60; default 2) of every wait of a line pass for the copies that feed it. A
+ * wait that runs out sets the engine's error flag: the pass stops issuing copies, waits (bounded)
+ * for those in flight and returns, later passes of the run return at once, and the run returns
+ * MT_ERR_TIMEOUT; the engine stays usable. 0: a copy not yet landed at the first check times out
+ * (a way to exercise the timeout path). No counterpart in the reference, whose GPU loop only
+ * stops between probes (ext_stop_sim, src/tem_simulation.cuh:47,512). */
+mt_status mt_engine_set_wait_limit(mt_engine* eng, double seconds);
 /* Progress counters (mt_niter / mt_iter, gui_multem/multem.cu:98-138): iterations are
  * (configuration, probe batch) pairs. */
 mt_status mt_engine_progress(mt_engine* eng, int* iter, int* niter);
@@ -322,18 +333,20 @@ mt_status mt_spline_tables_ex(const mt_system_conf* conf, int potential_type, co
                               double dR_min, double Vrl, int nR, double* heads, float* tab);
 
 /* Allocation-free form of mt_spline_tables; it has no counterpart in the reference. It is for
- * callers that cannot call cudaMalloc: code running inside a CUDA stream capture, code whose GPU
- * memory is owned by a framework's pool allocator (a stray cudaMalloc would bypass the pool's budget
- * or fail), or real-time loops where an allocation is not allowed. The caller passes the output:
+ * callers that cannot call cudaMalloc: code whose GPU memory is owned by a framework's pool
+ * allocator (an allocation outside the pool escapes its budget, or fails once the pool holds the
+ * device's memory), and loops that must not allocate while they run. The caller passes the output:
  * d_tab is a device buffer of n*5*nR floats on the current device, laid out as mt_spline_tables'
- * tab; heads (optional) is a host buffer of 4*n doubles. The only scratch is a fixed 32 KB device
- * array inside the library (held on every GPU that loads the library until the process exits):
- * n is limited to 128 elements and nR to 1024, larger requests return MT_ERR_INVALID_ARG. The work
- * is enqueued on `stream` (a cudaStream_t, NULL for the legacy default stream) and is complete when
- * that stream is; nothing is allocated and nothing is synchronised. The first call on a device looks
- * up the scratch array's device address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture. Calls share the scratch array: two calls that overlap on
- * the GPU (different streams or threads on one device) race on it. */
+ * tab; heads (optional) is a host buffer of 4*n doubles, written before the call returns. The only
+ * scratch is a fixed 32 KB device array inside the library (held on every GPU that loads the
+ * library until the process exits): n is limited to 128 elements and nR to 1024, larger requests
+ * return MT_ERR_INVALID_ARG. The call allocates nothing (no cudaMalloc, cudaFree or pool
+ * allocation). The element coefficients reach the scratch array as kernel parameters, so the work
+ * is a few kernel launches on `stream` (a cudaStream_t, NULL for the legacy default stream),
+ * complete when that stream is, and the call does not wait for the GPU. The first call on a device
+ * looks up the scratch array's device address (cudaGetSymbolAddress) with that device current and
+ * keeps it for that device's context. Calls share the scratch array: two calls that overlap on the
+ * GPU (different streams or threads on one device) race on it. */
 mt_status mt_spline_tables_noalloc(const int* Z, int n, double dR_min, double Vrl, int nR, double* heads,
                                    float* d_tab, void* stream);
 /* mt_spline_tables_noalloc for `potential_type` (as mt_spline_tables_ex); mt_spline_tables_noalloc

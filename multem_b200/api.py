@@ -194,6 +194,11 @@ class Engine:
     def cancel(self):
         capi.check(self.lib.mt_engine_cancel(self.h))
 
+    def set_wait_limit(self, seconds: float):
+        """Bound of every wait of a line pass for its bulk copies (0: no waiting beyond the first
+        check); a wait that runs out makes the run raise MT_ERR_TIMEOUT."""
+        capi.check(self.lib.mt_engine_set_wait_limit(self.h, float(seconds)))
+
     def set_timing(self, on: bool):
         capi.check(self.lib.mt_engine_set_timing(self.h, 1 if on else 0))
 

@@ -97,6 +97,7 @@ _VP = C.c_void_p
 SIGNATURES = {
     "mt_abi_version": (c_int, []),
     "mt_last_error": (C.c_char_p, []),
+    "mt_device_alloc_count": (c_int, [C.POINTER(C.c_longlong)]),
     "mt_output_query": (c_int, [C.POINTER(MtInputMultislice), C.POINTER(MtOutputDims)]),
     "mt_multislice_run": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice),
                                   C.POINTER(MtOutputMultislice)]),
@@ -109,6 +110,7 @@ SIGNATURES = {
     "mt_engine_reset": (c_int, [_VP]),
     "mt_engine_read_stem": (c_int, [_VP, P_double, C.c_size_t]),
     "mt_engine_cancel": (c_int, [_VP]),
+    "mt_engine_set_wait_limit": (c_int, [_VP, c_double]),
     "mt_engine_progress": (c_int, [_VP, P_int, P_int]),
     "mt_engine_prepare_confs": (c_int, [_VP, c_int, c_int]),
     "mt_engine_run_prepared": (c_int, [_VP, c_int, c_int]),

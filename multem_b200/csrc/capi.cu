@@ -10,6 +10,7 @@
 #include <string>
 
 #include "common.hpp"
+#include "devmem.hpp"
 #include "engine.hpp"
 #include "multem_b200.h"
 
@@ -58,6 +59,13 @@ extern "C" {
 int mt_abi_version(void) { return MT_ABI_VERSION; }
 
 const char* mt_last_error(void) { return g_last_error.c_str(); }
+
+mt_status mt_device_alloc_count(long long* count) {
+    return guarded([&] {
+        if (!count) mtb::fail(MT_ERR_INVALID_ARG, "count is NULL");
+        *count = mtb::dev_alloc_count();
+    });
+}
 
 mt_status mt_output_query(const mt_input_multislice* in, mt_output_dims* dims) {
     return guarded([&] {
@@ -116,6 +124,14 @@ mt_status mt_engine_cancel(mt_engine* eng) {
     return guarded([&] {
         if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
         eng->eng->cancel();
+    });
+}
+
+mt_status mt_engine_set_wait_limit(mt_engine* eng, double seconds) {
+    return guarded([&] {
+        if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
+        if (!(seconds >= 0.0) || seconds > 60.0) mtb::fail(MT_ERR_INVALID_ARG, "seconds must be in [0, 60]");
+        eng->eng->set_wait_limit((long long)(seconds * 1e9));
     });
 }
 

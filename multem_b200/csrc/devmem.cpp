@@ -5,6 +5,7 @@
 // allocation retried once when the device runs out of memory.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -21,6 +22,7 @@ struct DevicePool {
 };
 
 std::mutex g_mu;
+std::atomic<long long> g_alloc_count{0};
 std::map<int, DevicePool> g_pools;
 
 DevicePool& pool_of(int dev) {
@@ -58,11 +60,14 @@ void* dev_alloc(size_t bytes, int* dev_out) {
         e = cudaMallocFromPoolAsync(&p, bytes, P.pool, P.stream);
     }
     cuda_check(e, "cudaMallocFromPoolAsync");
+    g_alloc_count.fetch_add(1, std::memory_order_relaxed);
     // the allocation is complete once the pool's stream is, so any stream may use it afterwards
     MTB_CUDA(cudaStreamSynchronize(P.stream));
     *dev_out = dev;
     return p;
 }
+
+long long dev_alloc_count() { return g_alloc_count.load(std::memory_order_relaxed); }
 
 void dev_free(void* p, int dev) {
     if (!p) return;

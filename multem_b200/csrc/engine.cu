@@ -597,6 +597,7 @@ void Engine::tl_end() {
 void Engine::rows(RowMode mode, const RowArgs& a) {
     RowArgs b = a;
     b.err = (pipe_ & 1) ? d_err_.p : nullptr;
+    b.wait_ns = wait_ns_;
     tl_begin(0);
     launch_rows(m_.grid.ny, mode, b, 0, stream_);
     tl_end();
@@ -605,6 +606,7 @@ void Engine::rows(RowMode mode, const RowArgs& a) {
 void Engine::cols(int flags, const ColArgs& a) {
     ColArgs b = a;
     b.err = (pipe_ & 2) ? d_err_.p : nullptr;
+    b.wait_ns = wait_ns_;
     tl_begin(1);
     launch_cols(m_.grid.nx, flags, b, 0, stream_);
     tl_end();
@@ -680,6 +682,7 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
     put(ptrs, sizeof(ptrs));
     const int ints[3] = {cd.n_slice, cd.last_slice, pipe_};
     put(ints, sizeof(ints));
+    put(&wait_ns_, sizeof(wait_ns_));
     put(cd.probe_nz_c10.data(), cd.probe_nz_c10.size() * sizeof(int));
     put(cd.probe_c_c_10.data(), cd.probe_c_c_10.size() * sizeof(float));
     put(cd.slice_ithk.data(), cd.slice_ithk.size() * sizeof(int));
@@ -799,10 +802,12 @@ int Engine::tune_passes(int nprobe, ConfData& cd) {
     const int step = COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE;
     auto rows_t = [&](bool pipe) {
         ra.err = pipe ? d_err_.p : nullptr;
+        ra.wait_ns = wait_ns_;
         return time_of([&] { launch_rows(ny, ROW_STEP, ra, 0, stream_); });
     };
     auto cols_t = [&](bool pipe) {
         ca.err = pipe ? d_err_.p : nullptr;
+        ca.wait_ns = wait_ns_;
         return time_of([&] { launch_cols(nx, step, ca, 0, stream_); });
     };
     const int bits = (rows_t(true) < rows_t(false) ? 1 : 0) | (cols_t(true) < cols_t(false) ? 2 : 0);

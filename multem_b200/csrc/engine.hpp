@@ -108,6 +108,9 @@ class Engine {
 
     // device timing
     void set_timing(bool on) { timing_ = on; }
+    // Bound of each wait of a line pass for its bulk copies (ns); 0: a copy that has not landed at
+    // the first check is a timeout.
+    void set_wait_limit(long long ns) { wait_ns_ = ns < 0 ? 0 : ns; }
     int pass_variants() const { return pipe_; }
     void timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols);
 
@@ -148,6 +151,7 @@ class Engine {
     int batch_ = 1;
     DevBuf<int> d_err_;              // set by a line pass whose bounded wait gave up
     int pipe_ = 3;                   // bulk-copy-fed line passes where they fit (bit 0 rows, bit 1 cols)
+    long long wait_ns_ = 2000000000ll;  // bound of the line passes' waits for their copies
     bool tune_ = true;               // choose pipe_ per shape with tune_passes (MTB_PIPE unset)
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;

@@ -333,6 +333,15 @@ static size_t cols_smem() {
 // ---------------------------------------------------------------------------------------------
 // Bulk-copy-fed line passes.
 //
+// Bounded waits. Every wait for a copy gives up after the pass's wait_ns (from the first failed
+// check), sets the engine's error flag and returns false. Once the flag is set, by this CTA or any
+// other, waits return at once, no thread issues a new copy, and a pass launched later returns on
+// entry; each group's copy thread then waits (bounded by kDrainLimitNs) for the copies it issued
+// that nobody has seen land, so a CTA never exits with a copy in flight into its shared memory.
+// The loops keep their structure (the transforms of the remaining items run on stale data), so
+// every named barrier is still reached by all of its threads. The host reads the flag after the
+// run and reports MT_ERR_TIMEOUT.
+//
 // One CTA per SM with two groups of T threads; group g transforms the CTA's items k = g, g+2,
 // g+4, ... (line groups of the row pass, column tiles of the column pass). Each group owns a
 // landing buffer in shared memory that the copy engine fills with the input lines of its next
@@ -346,7 +355,7 @@ static size_t cols_smem() {
 // (stage_exchange_half), which is what makes two landing buffers fit. Results are stored
 // straight from registers.
 
-constexpr unsigned long long kWaitLimitNs = 4000000000ull;  // bounded waits: 4 s, then error flag
+constexpr long long kDrainLimitNs = 1000000000ll;  // bound of the wait for copies in flight at exit
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -366,21 +375,51 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
         : "memory");
     return ok != 0;
 }
+// non-blocking check of the phase with the given parity
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Wait for the phase with the given parity; after kWaitLimitNs record an error and go on (the
-// pass's results are then invalid and the host reports the error).
-__device__ __forceinline__ void mbar_wait(unsigned long long* bar, unsigned parity, int* err) {
-    if (mbar_try_wait(bar, parity)) return;
+__device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
+
+// Wait for the phase with the given parity. Returns false without waiting when the error flag is
+// already set; gives up after limit_ns (0: at the first failed check), sets the flag and returns
+// false. The spin is also capped in iterations.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* err, long long limit_ns) {
+    if (mbar_test_wait(bar, parity)) return true;
+    if (err_set(err)) return false;
+    if (limit_ns > 0) {
+        const unsigned long long t0 = global_ns();
+        for (unsigned it = 1; it < (1u << 30); it++) {
+            if (mbar_try_wait(bar, parity)) return true;
+            if ((it & 15u) == 0) {
+                if (err_set(err)) return false;
+                if ((long long)(global_ns() - t0) > limit_ns) break;
+            }
+        }
+    }
+    atomicOr(err, 1);
+    return false;
+}
+// Exit path after an error: wait for the phase of a copy this thread issued, bounded by
+// kDrainLimitNs whatever the flag says.
+__device__ __forceinline__ void mbar_drain(unsigned long long* bar, unsigned parity) {
+    if (mbar_test_wait(bar, parity)) return;
     const unsigned long long t0 = global_ns();
     for (unsigned it = 1; it < (1u << 30); it++) {
         if (mbar_try_wait(bar, parity)) return;
-        if ((it & 63u) == 0 && global_ns() - t0 > kWaitLimitNs) break;
+        if ((it & 15u) == 0 && (long long)(global_ns() - t0) > kDrainLimitNs) return;
     }
-    atomicOr(err, 1);
 }
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -447,6 +486,7 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     constexpr unsigned LINE_BYTES = NY * sizeof(float2);
     extern __shared__ __align__(1024) unsigned char pipe_smem[];
     __shared__ unsigned long long full[NG], tbar;
+    __shared__ int s_skip;
     float2* sm = reinterpret_cast<float2*>(pipe_smem);
     const float2* twI[3] = {nullptr, nullptr, nullptr};
     const float2* twF[3] = {nullptr, nullptr, nullptr};
@@ -459,19 +499,28 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     float2* buf = EARLY ? slots + NG * P::SLOT + grp * P::HBUF + (size_t)li * HalfLineSmem<NY>::value
                         : slot + (size_t)li * G::LS;
     if (threadIdx.x == 0) {
+        s_skip = err_set(a.err);  // an earlier pass timed out: the CTA returns (one decision for all)
         for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
         mbar_init(&tbar, 1);
         mbar_fence_init();
     }
     __syncthreads();
+    if (s_skip) return;
 
     // this CTA's items: [i0, i0 + K), item = g * nprobe + b, in units of NG
     const long long units = (long long)a.nx / LPC * a.nprobe / NG;
     const long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
     const long long i0 = NG * u0;
     const int K = (int)(NG * (u1 - u0));
+    // whether a warp may issue a copy: not once the error flag is set (lane 0 decides for the warp)
+    auto may_issue = [&](int lane) {
+        const int ok = lane == 0 ? !err_set(a.err) : 0;
+        return __shfl_sync(0xffffffffu, ok, 0) != 0;
+    };
     // issued by a whole warp: item k's LPC lines into slot k % NG
+    int last_k = -1;  // the last item this warp issued (drained at exit)
     auto issue = [&](int k, int lane) {
+        if (!may_issue(lane)) return;
         const long long item = i0 + k;
         const int g = (int)(item / a.nprobe), b = (int)(item % a.nprobe);
         const float2* src = a.in + ((size_t)b * a.nx + (size_t)g * LPC) * NY;
@@ -483,9 +532,12 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
         }
         __syncwarp();
         for (int l = lane; l < LPC; l += 32) bulk_load(dst + (size_t)l * NY, src + (size_t)l * NY, LINE_BYTES, bar);
+        last_k = k;
     };
-    // issued by warp 0: the transmission rows of line group g
-    auto issue_trans = [&](int g, int lane) {
+    // issued by warp 0: the transmission rows of line group g, phase `ph` of tbar
+    int last_tph = -1;  // parity of the last transmission copy warp 0 issued (drained at exit)
+    auto issue_trans = [&](int g, int lane, unsigned ph) {
+        if (!may_issue(lane)) return;
         const float2* src = a.trans + (size_t)g * LPC * NY;
         if (lane == 0) {
             fence_proxy_async();
@@ -493,12 +545,13 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
         }
         __syncwarp();
         for (int l = lane; l < LPC; l += 32) bulk_load(s_trans + (size_t)l * NY, src + (size_t)l * NY, LINE_BYTES, &tbar);
+        last_tph = (int)ph;
     };
     if (gtid < 32 && grp < K) issue(grp, gtid);
     int g_cur = K > 0 ? (int)(i0 / a.nprobe) : 0;
     unsigned tphase = 0;
     if constexpr (TRANS) {
-        if (threadIdx.x < 32 && K > 0) issue_trans(g_cur, threadIdx.x);
+        if (threadIdx.x < 32 && K > 0) issue_trans(g_cur, threadIdx.x, tphase);
     }
 
     using Sync = typename std::conditional<(TPL <= 32), WarpSync, GroupSync<GT>>::type;
@@ -512,14 +565,14 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
                 // every group reaches this point at the first unit of the new line group, after
                 // finishing its last item of the old one
                 asm volatile("bar.sync 15, %0;" ::"r"(NG * GT) : "memory");
-                if (threadIdx.x < 32) issue_trans(g, threadIdx.x);
-                g_cur = g;
                 tphase ^= 1u;
+                if (threadIdx.x < 32) issue_trans(g, threadIdx.x, tphase);
+                g_cur = g;
             }
         }
         const int ix = g * LPC + li;
         const size_t off = ((size_t)b * a.nx + ix) * NY;
-        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err);
+        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err, a.wait_ns);
         const float2* lsrc = slot + (size_t)li * NY;
         float2 x[E];
         if constexpr (MODE == ROW_FIRST_REAL) {
@@ -545,7 +598,7 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
 #pragma unroll
             for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::RL>(i, t)] = cscale(x[i], a.scale);
         } else {
-            mbar_wait(&tbar, tphase, a.err);
+            mbar_wait(&tbar, tphase, a.err, a.wait_ns);
             const float2* Tr = s_trans + (size_t)li * NY;
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], Tr[reg_pos<NY, G::RL>(i, t)]);
@@ -560,6 +613,9 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
             for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::R1>(i, t)] = x[i];
         }
     }
+    // copies this warp issued and nobody saw land (only after an error): wait them out
+    if (gtid == 0 && last_k >= 0) mbar_drain(&full[grp], (unsigned)(last_k / NG) & 1u);
+    if (threadIdx.x == 0 && last_tph >= 0) mbar_drain(&tbar, (unsigned)last_tph);
 }
 
 // Row-pass pipeline shape per line length: threads per group, groups, early issue (where the
@@ -619,6 +675,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     extern __shared__ __align__(1024) unsigned char pipe_smem[];
     __shared__ unsigned long long full[NG];
     __shared__ double s_red[NG][NWARP][kMaxDet];
+    __shared__ int s_skip;
     float2* sm = reinterpret_cast<float2*>(pipe_smem);
     const float2* twP[3] = {nullptr, nullptr, nullptr};  // plan order: the forward transform here
     const float2* twR[3] = {nullptr, nullptr, nullptr};  // reversed order: the inverse transform
@@ -633,18 +690,23 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
         for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
     }
     if (threadIdx.x == 0) {
+        s_skip = err_set(a.err);  // an earlier pass timed out: the CTA returns (one decision for all)
         for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
         mbar_fence_init();
     }
     __syncthreads();
+    if (s_skip) return;
 
     const int ldy = LDY ? LDY : a.ny;
     const int tiles = ldy / W;
     const int items = tiles * a.nprobe;
     const size_t pstride = (size_t)NX * ldy;
     const int K = (int)blockIdx.x < items ? (items - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
-    // issued by one thread: item k's tile into landing buffer k % NG
+    // issued by one thread: item k's tile into landing buffer k % NG (none once the error flag is set)
+    int last_k = -1;  // the last item this thread issued (drained at exit)
     auto issue = [&](int k) {
+        if (err_set(a.err)) return;
+        last_k = k;
         const int item = blockIdx.x + k * gridDim.x;
         unsigned long long* bar = &full[k % NG];
         float2* dst = land0 + (k % NG) * P::LAND;
@@ -664,7 +726,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
         const int iy = ct * W + c;
         const size_t off = (size_t)b * pstride + iy + (size_t)t * ldy;
         float2* dst = a.out + off;
-        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err);
+        mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err, a.wait_ns);
         float2 x[E];
 #pragma unroll
         for (int i = 0; i < E; i++) x[i] = land[(size_t)reg_pos<NX, G::R1>(i, t) * W + c];
@@ -727,6 +789,8 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::RL>(i, t) - t) * ldy] = x[i];
         }
     }
+    // a tile this thread issued and nobody saw land (only after an error): wait it out
+    if (gtid == 0 && last_k >= 0) mbar_drain(&full[grp], (unsigned)(last_k / NG) & 1u);
 }
 
 // Tensor map for cols_pipe_kernel over a probe batch at `base` (cuTensorMapEncodeTiled through

@@ -350,26 +350,68 @@ void build_tables(const std::vector<int>& Zs, int type, const std::vector<TableH
 // array is kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead)) bytes (about 32 KB) and is
 // held by every GPU that loads this library until the process exits. All calls share it: each
 // call overwrites the entries it uses before its kernel reads them (nothing has to start at zero),
-// and two calls whose copies and kernels overlap on the GPU (different streams, or different host
+// and two calls whose fills and kernels overlap on the GPU (different streams, or different host
 // threads on one device) race on it.
+//
+// The host-side values reach the scratch array as kernel parameters (noalloc_fill_kernel, a few
+// elements per launch), not through a host-to-device copy: the call then neither blocks on a
+// pageable-memory copy nor leaves a copy reading host memory that goes away when the call returns.
 constexpr int kNoAllocMaxElements = 128;
 static __device__ __align__(256) unsigned char
     g_noalloc_table_scratch[kNoAllocMaxElements * (sizeof(ElemCoef) + sizeof(TableHead))];
 
-// Device address of the scratch array on `dev`. Host code may not use the symbol itself (it names
-// a host-side stand-in, not device memory); the address is looked up once per device with that
-// device current and cached.
+// Elements per fill launch: their coefficients and heads travel in the launch's parameter block,
+// kept well inside the classic 4 KB parameter limit.
+constexpr int kNoAllocFillChunk = 12;
+struct NoAllocChunk {
+    ElemCoef coef[kNoAllocFillChunk];
+    TableHead head[kNoAllocFillChunk];
+    int first, count;
+};
+static_assert(sizeof(NoAllocChunk) < 4000, "fill chunk must fit a kernel parameter block");
+
+__global__ void noalloc_fill_kernel(const __grid_constant__ NoAllocChunk ch, ElemCoef* coef, TableHead* head) {
+    for (int i = threadIdx.x; i < ch.count; i += blockDim.x) {
+        coef[ch.first + i] = ch.coef[i];
+        head[ch.first + i] = ch.head[i];
+    }
+}
+
+// Device address of the scratch array on the current device. Host code may not use the symbol
+// itself (it names a host-side stand-in, not device memory). The address is looked up with
+// cudaGetSymbolAddress once per device, with that device current, and cached together with the
+// CUDA context it was taken in; a call made in another context (the device's primary context
+// destroyed and created anew) looks it up again.
+using CtxGetCurrentFn = int (*)(void**);
+static void* current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        MTB_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !f) fail(MT_ERR_CUDA, "cuCtxGetCurrent is not available");
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    void* ctx = nullptr;
+    if (fn(&ctx) != 0) fail(MT_ERR_CUDA, "cuCtxGetCurrent failed");
+    return ctx;
+}
+
 static unsigned char* noalloc_scratch_address(int dev) {
     constexpr int kMaxDevices = 64;
     static unsigned char* addr[kMaxDevices] = {};
+    static void* ctx_of[kMaxDevices] = {};
     static std::mutex mu;
     if (dev < 0 || dev >= kMaxDevices) fail(MT_ERR_INVALID_ARG, "device index out of range");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    // before the runtime's first call on this device no context is current (NULL): the lookup
+    // below then creates the primary context and the cache records it
+    void* ctx = current_context();
+    if (!addr[dev] || !ctx || ctx_of[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_table_scratch);
         if (e != cudaSuccess) throw Error(MT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         addr[dev] = static_cast<unsigned char*>(p);
+        ctx_of[dev] = current_context();
     }
     return addr[dev];
 }
@@ -386,11 +428,17 @@ void build_tables_noalloc(const std::vector<int>& Zs, int type, const std::vecto
     unsigned char* base = noalloc_scratch_address(dev);
     ElemCoef* d_coef = reinterpret_cast<ElemCoef*>(base);
     TableHead* d_head = reinterpret_cast<TableHead*>(base + kNoAllocMaxElements * sizeof(ElemCoef));
-    std::vector<ElemCoef> h(n);
-    for (int i = 0; i < n; i++) h[i] = element_coef(Zs[i], type, charges.empty() ? 0 : charges[i]);
-    // pageable sources: each copy returns once its source has been staged, so the vectors may go
-    MTB_CUDA(cudaMemcpyAsync(d_coef, h.data(), sizeof(ElemCoef) * n, cudaMemcpyHostToDevice, stream));
-    MTB_CUDA(cudaMemcpyAsync(d_head, heads.data(), sizeof(TableHead) * n, cudaMemcpyHostToDevice, stream));
+    for (int i0 = 0; i0 < n; i0 += kNoAllocFillChunk) {
+        NoAllocChunk ch{};
+        ch.first = i0;
+        ch.count = n - i0 < kNoAllocFillChunk ? n - i0 : kNoAllocFillChunk;
+        for (int i = 0; i < ch.count; i++) {
+            ch.coef[i] = element_coef(Zs[i0 + i], type, charges.empty() ? 0 : charges[i0 + i]);
+            ch.head[i] = heads[i0 + i];
+        }
+        noalloc_fill_kernel<<<1, 32, 0, stream>>>(ch, d_coef, d_head);
+        MTB_CUDA(cudaGetLastError());
+    }
     build_tables_kernel<<<n, 128, 3 * nR * sizeof(double), stream>>>(d_coef, d_head, n, nR, d_tab);
     MTB_CUDA(cudaGetLastError());
 }

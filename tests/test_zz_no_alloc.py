@@ -1,10 +1,13 @@
 """The allocation-free spline-table entry point (mt_spline_tables_noalloc).
 
-It serves callers that cannot call cudaMalloc (inside a stream capture, under a framework's GPU
-memory pool, in allocation-free real-time loops): they pass their own device output buffer, and the
-library's only scratch is a fixed device array. This test calls it (and mt_spline_tables_noalloc_ex
-for other parameterisations) through the C ABI several times in a row, on different element lists,
-and checks each result against the allocating entry with the tolerance the table-parity test uses. The file is named to be collected last.
+It is for callers that cannot call cudaMalloc: code whose GPU memory belongs to a framework's pool
+allocator (an allocation outside the pool escapes its budget, or fails once the pool holds the
+device's memory), and loops that must not allocate while they run. They pass their own device
+output buffer; the library's only scratch is a fixed device array inside the library. This test
+calls it (and mt_spline_tables_noalloc_ex for other parameterisations) through the C ABI several
+times in a row, on different element lists, checks each result against the allocating entry with
+the tolerance the table-parity test uses, and checks that the calls make no device allocation
+(the library's allocation counter does not move). The file is named to be collected last.
 """
 import ctypes as C
 
@@ -34,13 +37,21 @@ def _noalloc(lib, Z, dR, nR, torch, pt=6):
     return heads, d_tab.cpu().numpy().reshape(z.size, 5, nR)
 
 
+def _alloc_count(lib):
+    n = C.c_longlong(-1)
+    capi.check(lib.mt_device_alloc_count(C.byref(n)))
+    return n.value
+
+
 def test_noalloc_tables_match_allocating_entry_on_two_calls():
     torch = pytest.importorskip("torch")
     lib = capi.load()
     dR = np.float32(np.float32(15.62) / np.float32(128))
     for Z, pt in (([8, 22, 38], 6), ([14, 79, 6, 1, 78], 6), ([14, 79, 6, 1, 78], 4), ([8, 22, 38], 3)):
         heads_ref, tab_ref = api.spline_tables(Z, float(dR), potential_type=pt)
+        n0 = _alloc_count(lib)
         heads, tab = _noalloc(lib, Z, dR, 128, torch, pt)
+        assert _alloc_count(lib) == n0, "the allocation-free entry point allocated device memory"
         np.testing.assert_array_equal(heads, heads_ref)
         assert np.all(np.isfinite(tab))
         for i in range(len(Z)):
