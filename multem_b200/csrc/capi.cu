@@ -208,6 +208,98 @@ mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislic
     });
 }
 
+// The whole batch as one CUDA graph: every input's engine is created (on `workers` host threads)
+// and prepares all of its configurations, then one capture records each engine's complete run on
+// the engine's own stream, forked from and joined back into one origin stream, so that a single
+// graph launch advances every specimen, configuration and probe batch, the GPU running the
+// specimens' independent branches concurrently. An input whose engine cannot be set up gets its
+// status in st/msg and is left out of the graph; the others run. Returns false (nothing run, st
+// cleared) when the engines do not fit in device memory together; the caller then runs the inputs
+// on host workers instead.
+static bool run_batch_graph(const mt_system_conf& c, int n, const mt_input_multislice* in, mt_output_multislice* out,
+                            const std::vector<int>& order, int workers, std::vector<mt_status>& st,
+                            std::vector<std::string>& msg) {
+    std::vector<std::unique_ptr<mtb::Engine>> eng(n);
+    std::atomic<int> next{0};
+    std::atomic<bool> oom{false};
+    auto build = [&] {
+        for (;;) {
+            const int k = next++;
+            if (k >= n || oom) break;
+            const int i = order[k];
+            st[i] = guarded([&] {
+                MTB_CUDA(cudaSetDevice(c.gpu_device));
+                eng[i].reset(new mtb::Engine(&c, &in[i]));
+                eng[i]->prepare_run();
+            });
+            if (st[i] == MT_ERR_OOM) oom = true;
+            if (st[i] != MT_OK) msg[i] = g_last_error;
+        }
+    };
+    {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < workers; t++) pool.emplace_back(build);
+        build();
+        for (auto& t : pool) t.join();
+    }
+    if (oom) {  // the engines are released here; the host-worker path runs the batch
+        for (int i = 0; i < n; i++) {
+            st[i] = MT_OK;
+            msg[i].clear();
+        }
+        return false;
+    }
+    std::vector<int> ok;
+    for (int k = 0; k < n; k++)
+        if (st[order[k]] == MT_OK) ok.push_back(order[k]);
+    if (ok.empty()) return true;
+    MTB_CUDA(cudaSetDevice(c.gpu_device));
+    cudaStream_t origin = nullptr;
+    MTB_CUDA(cudaStreamCreateWithFlags(&origin, cudaStreamNonBlocking));
+    const int m = (int)ok.size();
+    std::vector<cudaEvent_t> ev(m + 1, nullptr);
+    for (auto& e : ev) MTB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto cleanup = [&] {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto& e : ev) cudaEventDestroy(e);
+        cudaStreamDestroy(origin);
+    };
+    try {
+        MTB_CUDA(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+        try {
+            MTB_CUDA(cudaEventRecord(ev[m], origin));
+            for (int k = 0; k < m; k++) {
+                mtb::Engine& e = *eng[ok[k]];
+                MTB_CUDA(cudaStreamWaitEvent(e.stream(), ev[m], 0));  // fork: the engine's stream joins the capture
+                e.record_run();
+                MTB_CUDA(cudaEventRecord(ev[k], e.stream()));
+                MTB_CUDA(cudaStreamWaitEvent(origin, ev[k], 0));      // join
+            }
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(origin, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        MTB_CUDA(cudaStreamEndCapture(origin, &graph));
+        MTB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        MTB_CUDA(cudaGraphLaunch(exec, origin));
+        MTB_CUDA(cudaStreamSynchronize(origin));
+        for (int i : ok) {
+            st[i] = guarded([&] { eng[i]->write_output(&out[i]); });
+            if (st[i] != MT_OK) msg[i] = g_last_error;
+        }
+    } catch (...) {
+        cleanup();
+        throw;
+    }
+    cleanup();
+    return true;
+}
+
 mt_status mt_multislice_run_batch(const mt_system_conf* conf, int n, const mt_input_multislice* in,
                                   mt_output_multislice* out, mt_status* status) {
     std::vector<mt_status> st(n > 0 ? n : 0, MT_OK);
@@ -228,7 +320,10 @@ mt_status mt_multislice_run_batch(const mt_system_conf* conf, int n, const mt_in
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
         const char* w = std::getenv("MTB_BATCH_WORKERS");
         const int workers = std::max(1, std::min(n, w ? std::atoi(w) : 4));
-        std::atomic<int> next{0};
+        const char* mode = std::getenv("MTB_BATCH_MODE");
+        const bool graph = n > 1 && !(mode && std::strcmp(mode, "threads") == 0) &&
+                           run_batch_graph(c, n, in, out, order, workers, st, msg);
+        std::atomic<int> next{graph ? n : 0};
         auto work = [&] {
             for (;;) {
                 const int k = next++;

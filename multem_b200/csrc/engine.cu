@@ -182,6 +182,7 @@ Engine::~Engine() {
         for (auto& cd : slot_) cd.release_idle();
         for (auto& g : graph_)
             if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (range_graph_.exec) cudaGraphExecDestroy(range_graph_.exec);
         for (auto* b : {&d_tab_, &d_Rmax_}) b->release_idle();
         for (auto* b : {&d_psi_, &d_trans_, &d_tmp_, &d_beam_, &d_prop_bp_, &d_ramp_}) b->release_idle();
         d_detmat_.release_idle();
@@ -219,15 +220,19 @@ void Engine::synchronize() {
 }
 
 void Engine::reset() {
+    zero_accumulators();
+    iter_ = 0;
+    cancel_ = false;
+    synchronize();
+}
+
+void Engine::zero_accumulators() {
     if (d_image_.p) MTB_CUDA(cudaMemsetAsync(d_image_.p, 0, sizeof(double) * d_image_.n, stream_));
     if (d_coh_.p) MTB_CUDA(cudaMemsetAsync(d_coh_.p, 0, sizeof(float2) * d_coh_.n, stream_));
     if (d_ew_psi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_psi_.p, 0, sizeof(double) * d_ew_psi_.n, stream_));
     if (d_ew_m2_.p) MTB_CUDA(cudaMemsetAsync(d_ew_m2_.p, 0, sizeof(double) * d_ew_m2_.n, stream_));
     if (d_ew_cohpsi_.p) MTB_CUDA(cudaMemsetAsync(d_ew_cohpsi_.p, 0, sizeof(double) * d_ew_cohpsi_.n, stream_));
     if (d_coh_img_.p) MTB_CUDA(cudaMemsetAsync(d_coh_img_.p, 0, sizeof(float2) * d_coh_img_.n, stream_));
-    iter_ = 0;
-    cancel_ = false;
-    synchronize();
 }
 
 // Element spline tables for the elements present (Spec::set_input_data builds all 103,
@@ -555,19 +560,70 @@ void Engine::check_cancel() {
     }
 }
 
+// Prepared configurations [c0, c1]: with graphs (and no per-launch timing) the whole range is one
+// CUDA graph, captured before the run's start event (so the capture is not in the device time)
+// and replayed while the range and every configuration's launch signature match; else direct
+// launches.
 void Engine::run_prepared(int c0, int c1) {
     if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
+    for (int c = c0; c <= c1; c++)
+        if (!find_conf(c)) fail(MT_ERR_INVALID_ARG, "configuration not prepared");
     long long l0 = launches_issued();
     tl_used_ = 0;
     if (!run_a_) {
         MTB_CUDA(cudaEventCreate(&run_a_));
         MTB_CUDA(cudaEventCreate(&run_b_));
     }
+    const bool graph = graphs_ && !timing_;
+    if (graph) {
+        ConfData* cd0 = find_conf(c0);
+        if (tune_) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, *cd0);
+        std::vector<char> sig;
+        const int range[2] = {c0, c1};
+        sig.insert(sig.end(), (const char*)range, (const char*)range + sizeof(range));
+        for (int c = c0; c <= c1; c++) {
+            std::vector<char> s = graph_signature(*find_conf(c));
+            sig.insert(sig.end(), s.begin(), s.end());
+        }
+        if (!range_graph_.exec || sig != range_graph_.sig) {
+            if (range_graph_.exec) {
+                MTB_CUDA(cudaGraphExecDestroy(range_graph_.exec));
+                range_graph_.exec = nullptr;
+            }
+            const int it0 = iter_;
+            const long long la = launches_issued();
+            cudaGraph_t g = nullptr;
+            MTB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            capturing_ = true;
+            try {
+                for (int c = c0; c <= c1; c++) run_conf(*find_conf(c));
+            } catch (...) {
+                capturing_ = false;
+                cudaStreamEndCapture(stream_, &g);
+                if (g) cudaGraphDestroy(g);
+                iter_ = it0;
+                throw;
+            }
+            capturing_ = false;
+            MTB_CUDA(cudaStreamEndCapture(stream_, &g));
+            cudaError_t e = cudaGraphInstantiate(&range_graph_.exec, g, 0);
+            cudaGraphDestroy(g);
+            MTB_CUDA(e);
+            range_graph_.sig = std::move(sig);
+            range_graph_.iters = iter_ - it0;
+            range_graph_.launches = launches_issued() - la;
+            iter_ = it0;
+            add_launches(-range_graph_.launches);
+        }
+    }
+    l0 = launches_issued();
     MTB_CUDA(cudaEventRecord(run_a_, stream_));
-    for (int c = c0; c <= c1; c++) {
-        ConfData* cd = find_conf(c);
-        if (!cd) fail(MT_ERR_INVALID_ARG, "configuration not prepared");
-        run_conf(*cd);
+    if (graph) {
+        MTB_CUDA(cudaGraphLaunch(range_graph_.exec, stream_));
+        iter_ += range_graph_.iters;
+        add_launches(range_graph_.launches);
+    } else {
+        for (int c = c0; c <= c1; c++) run_conf(*find_conf(c));
     }
     MTB_CUDA(cudaEventRecord(run_b_, stream_));
     launches_ = launches_issued() - l0;
@@ -637,10 +693,9 @@ void Engine::timing(double* total_ms, double* rows_ms, long long* n_rows, double
 void Engine::run_confs(int c0, int c1) {
     if (c0 < m_.fp_iconf_0 || c1 > m_.pn_nconf || c0 > c1) fail(MT_ERR_INVALID_ARG, "configuration range out of bounds");
     long long l0 = launches_issued();
-    // graphs where launch overhead matters: passes of at most 4 Mi points per launch (above that
-    // one launch runs for tens of microseconds and a recapture would cost more than it saves)
-    const size_t per_launch = (size_t)m_.grid.nx * m_.grid.ny * (m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1);
-    if (graphs_ && !timing_ && per_launch <= ((size_t)1 << 22)) {
+    // every configuration as its slot's CUDA graph: captured twice (once per slot) and replayed
+    // while the launch sequence and its arguments match
+    if (graphs_ && !timing_) {
         // configuration c is prepared in slot c % 2 (prepare_conf waits for the stream, so the
         // slot's previous user, c - 2, has finished) and runs as that slot's graph
         for (int c = c0; c <= c1; c++) {
@@ -672,6 +727,32 @@ void Engine::run_confs(int c0, int c1) {
     launches_ = launches_issued() - l0;
     synchronize();
     prev.release_idle();
+}
+
+void Engine::prepare_run() {
+    const int c0 = m_.fp_iconf_0, c1 = m_.pn_nconf;
+    prepare_confs(c0, c1);
+    ConfData* cd = find_conf(c0);
+    if (tune_ && cd) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, *cd);
+    synchronize();
+}
+
+void Engine::record_run() {
+    zero_accumulators();
+    iter_ = 0;
+    cancel_ = false;
+    capturing_ = true;  // no host synchronisation (check_cancel) while the work is recorded
+    try {
+        for (int c = m_.fp_iconf_0; c <= m_.pn_nconf; c++) {
+            ConfData* cd = find_conf(c);
+            if (!cd) fail(MT_ERR_INTERNAL, "configuration not prepared before recording");
+            run_conf(*cd);
+        }
+    } catch (...) {
+        capturing_ = false;
+        throw;
+    }
+    capturing_ = false;
 }
 
 // Everything a captured run_conf bakes into its launches besides the engine's own buffers.

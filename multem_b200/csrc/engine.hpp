@@ -92,6 +92,13 @@ class Engine {
     void prepare_confs(int c0, int c1);      // host RNG + slicing + uploads
     void run_prepared(int c0, int c1);       // device-only work for prepared confs
     void run_confs(int c0, int c1);          // prepare + run
+    // Whole-run recording, for one CUDA graph over a batch of engines: prepare_run prepares every
+    // configuration of the run in its own buffers and chooses the pass variants (host work, with
+    // synchronisation); record_run then issues all of the run's device work on this engine's
+    // stream without any host synchronisation (the caller has the stream in a capture); after the
+    // graph has run, write_output reads the results.
+    void prepare_run();
+    void record_run();
     void write_output(mt_output_multislice* out);
     void read_stem(double* image_tot, size_t n);
     void cancel() { cancel_ = true; }
@@ -200,6 +207,7 @@ class Engine {
     void build_bwl();
     void band_limit_trans(const ConfData& cd);
     void check_cancel();
+    void zero_accumulators();        // the accumulators' memsets on the stream (no synchronisation)
     ConfData* find_conf(int iconf);
 
     // CUDA graphs of run_conf, one per configuration slot (run_confs alternates two slots whose
@@ -214,6 +222,7 @@ class Engine {
     bool capturing_ = false;
     ConfData slot_[2];
     ConfGraph graph_[2];
+    ConfGraph range_graph_;  // run_prepared: one graph over a range of prepared configurations
     std::vector<char> graph_signature(const ConfData& cd) const;
     void run_conf_graph(ConfData& cd, ConfGraph& g);
 };

@@ -1,6 +1,6 @@
 """mt_multislice_run_batch: several different simulations in one call give exactly the outputs of
-one mt_multislice_run call each (engines are deterministic; running them on concurrent host
-workers and CUDA streams must not change a bit)."""
+one mt_multislice_run call each (engines are deterministic; running them as the branches of one
+CUDA graph, the default, or on concurrent host workers and CUDA streams must not change a bit)."""
 import numpy as np
 import pytest
 
@@ -27,9 +27,11 @@ def _same(a, b):
             np.testing.assert_array_equal(np.asarray(da[k]), np.asarray(db[k]))
 
 
+@pytest.mark.parametrize("mode", ["graph", "threads"])
 @pytest.mark.parametrize("workers", ["1", "4"])
-def test_batch_equals_single_runs(workers, monkeypatch):
+def test_batch_equals_single_runs(mode, workers, monkeypatch):
     monkeypatch.setenv("MTB_BATCH_WORKERS", workers)
+    monkeypatch.setenv("MTB_BATCH_MODE", mode)
     ps = _cases()
     got = api.ilc_multem_batch(None, ps)
     for p, g in zip(ps, got):
