@@ -31,6 +31,9 @@ the same workload: two raster sizes per step, so that the per-update slope exclu
 per-run set-up; --impl reference --ref-gpu times its GPU path the same way.
 --dry-run starts the ranks (gloo on CPU), shards the configurations and runs the final
 all-reduce and its check, without any simulation (a check of the multi-process plumbing).
+--profile-case NS runs one configuration of the workload with an NS x NS raster (the small case the
+ncu captures under profiles/ use: NS = 16 gives one launch of 256 probes, 512 MiB of waves) and
+prints its device time.
 """
 from __future__ import annotations
 
@@ -390,6 +393,24 @@ def large_field_live(conf):
             "api": "mt_multislice_run (host in/out, set-up included)"}
 
 
+def run_profile_case(args):
+    """One configuration of the workload on an NS x NS raster (a bounded case for profilers)."""
+    from multem_b200 import api
+    p = _raster(workload(1), args.profile_case)
+    e = api.Engine(p)
+    e.prepare_confs(1, 1)
+    e.run_prepared(1, 1)
+    t = e.timing()
+    img = e.read_stem()
+    tun = e.tuning()
+    n_launch = e.launch_count()
+    e.close()
+    print(json.dumps({"case": f"512^2 SrTiO3, {args.profile_case}x{args.profile_case} probes, 1 configuration",
+                      "device_ms": t["total_ms"], "launches": n_launch, "tuning": tun,
+                      "detector_sums": img.sum(axis=(2, 3)).ravel().tolist()}))
+    return 0
+
+
 def run_ours(args):
     world, rank, local, dist = init_ranks("nccl")
     import torch
@@ -525,6 +546,8 @@ def main():
     ap.add_argument("--dry-run", action="store_true",
                     help="ranks, shards and the final all-reduce check only (gloo, no GPU work)")
     ap.add_argument("--rank-timeout", type=int, default=1800, help="bound of a self-started multi-rank run (s)")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="NS",
+                    help="one configuration with an NS x NS raster, for profilers; prints its device time")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -534,6 +557,8 @@ def main():
         return run_reference(args)
     if args.dry_run:
         return run_dry(args)
+    if args.profile_case:
+        return run_profile_case(args)
     return run_ours(args)
 
 

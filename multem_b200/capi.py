@@ -116,6 +116,7 @@ SIGNATURES = {
     "mt_engine_run_prepared": (c_int, [_VP, c_int, c_int]),
     "mt_engine_launch_count": (c_int, [_VP, C.POINTER(C.c_longlong)]),
     "mt_engine_pass_variants": (c_int, [_VP, P_int]),
+    "mt_engine_tuning": (c_int, [_VP, P_int, P_int, P_int]),
     "mt_engine_destroy": (c_int, [_VP]),
     "mt_engine_set_timing": (c_int, [_VP, c_int]),
     "mt_engine_timing": (c_int, [_VP, P_double, P_double, C.POINTER(C.c_longlong), P_double,

@@ -1,5 +1,7 @@
 // extern "C" entry points declared in include/multem_b200.h.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
@@ -170,6 +172,13 @@ mt_status mt_engine_pass_variants(mt_engine* eng, int* variants) {
     });
 }
 
+mt_status mt_engine_tuning(mt_engine* eng, int* rows_variant, int* cols_variant, int* probes_per_launch) {
+    return guarded([&] {
+        if (!eng || !rows_variant || !cols_variant || !probes_per_launch) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        eng->eng->tuning(rows_variant, cols_variant, probes_per_launch);
+    });
+}
+
 mt_status mt_engine_set_timing(mt_engine* eng, int on) {
     return guarded([&] {
         if (!eng) mtb::fail(MT_ERR_INVALID_ARG, "eng is NULL");
@@ -222,6 +231,12 @@ static bool run_batch_graph(const mt_system_conf& c, int n, const mt_input_multi
     std::vector<std::unique_ptr<mtb::Engine>> eng(n);
     std::atomic<int> next{0};
     std::atomic<bool> oom{false};
+    const bool prof = std::getenv("MTB_BATCH_PROFILE") != nullptr;  // phase times on stderr
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+    };
+    const auto t0 = now();
     auto build = [&] {
         for (;;) {
             const int k = next++;
@@ -253,6 +268,7 @@ static bool run_batch_graph(const mt_system_conf& c, int n, const mt_input_multi
     for (int k = 0; k < n; k++)
         if (st[order[k]] == MT_OK) ok.push_back(order[k]);
     if (ok.empty()) return true;
+    const auto t1 = now();
     MTB_CUDA(cudaSetDevice(c.gpu_device));
     cudaStream_t origin = nullptr;
     MTB_CUDA(cudaStreamCreateWithFlags(&origin, cudaStreamNonBlocking));
@@ -285,9 +301,18 @@ static bool run_batch_graph(const mt_system_conf& c, int n, const mt_input_multi
             throw;
         }
         MTB_CUDA(cudaStreamEndCapture(origin, &graph));
+        const auto t2 = now();
         MTB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        const auto t3 = now();
         MTB_CUDA(cudaGraphLaunch(exec, origin));
         MTB_CUDA(cudaStreamSynchronize(origin));
+        const auto t4 = now();
+        if (prof) {
+            size_t nodes = 0;
+            cudaGraphGetNodes(graph, nullptr, &nodes);
+            std::fprintf(stderr, "batch graph: %d inputs, %zu nodes; set-up %.3f s, capture %.3f s, instantiate %.3f s, run %.3f s\n",
+                         m, nodes, secs(t0, t1), secs(t1, t2), secs(t2, t3), secs(t3, t4));
+        }
         for (int i : ok) {
             st[i] = guarded([&] { eng[i]->write_output(&out[i]); });
             if (st[i] != MT_OK) msg[i] = g_last_error;

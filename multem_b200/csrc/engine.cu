@@ -165,11 +165,14 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
     d_err_.alloc(1);
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
-    // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns), else tune_passes picks
+    // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns; MTB_SHAPE the alternative
+    // shapes, same bits), else the autotuner picks them and the probes per launch
     pipe_ = env_int("MTB_PIPE", -1);
     graphs_ = env_int("MTB_GRAPH", 1) != 0;
     tune_ = pipe_ < 0;
     if (tune_) pipe_ = 3;
+    shape_ = tune_ ? 0 : env_int("MTB_SHAPE", 0) & 3;
+    run_batch_ = batch_;
     if (m_.is_wave_sim() && m_.is_user_wave()) build_user_wave();
     reset();
 }
@@ -577,7 +580,7 @@ void Engine::run_prepared(int c0, int c1) {
     const bool graph = graphs_ && !timing_;
     if (graph) {
         ConfData* cd0 = find_conf(c0);
-        if (tune_) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, *cd0);
+        if (tune_) tune(*cd0);
         std::vector<char> sig;
         const int range[2] = {c0, c1};
         sig.insert(sig.end(), (const char*)range, (const char*)range + sizeof(range));
@@ -654,6 +657,7 @@ void Engine::rows(RowMode mode, const RowArgs& a) {
     RowArgs b = a;
     b.err = (pipe_ & 1) ? d_err_.p : nullptr;
     b.wait_ns = wait_ns_;
+    b.shape = shape_ & 1;
     tl_begin(0);
     launch_rows(m_.grid.ny, mode, b, 0, stream_);
     tl_end();
@@ -663,6 +667,7 @@ void Engine::cols(int flags, const ColArgs& a) {
     ColArgs b = a;
     b.err = (pipe_ & 2) ? d_err_.p : nullptr;
     b.wait_ns = wait_ns_;
+    b.shape = (shape_ >> 1) & 1;
     tl_begin(1);
     launch_cols(m_.grid.nx, flags, b, 0, stream_);
     tl_end();
@@ -733,7 +738,7 @@ void Engine::prepare_run() {
     const int c0 = m_.fp_iconf_0, c1 = m_.pn_nconf;
     prepare_confs(c0, c1);
     ConfData* cd = find_conf(c0);
-    if (tune_ && cd) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, *cd);
+    if (tune_ && cd) tune(*cd);
     synchronize();
 }
 
@@ -761,7 +766,7 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
     auto put = [&](const void* p, size_t n) { sig.insert(sig.end(), (const char*)p, (const char*)p + n); };
     const void* ptrs[3] = {cd.atoms.p, cd.ranges.p, cd.prop.p};
     put(ptrs, sizeof(ptrs));
-    const int ints[3] = {cd.n_slice, cd.last_slice, pipe_};
+    const int ints[5] = {cd.n_slice, cd.last_slice, pipe_, shape_, run_batch_};
     put(ints, sizeof(ints));
     put(&wait_ns_, sizeof(wait_ns_));
     put(cd.probe_nz_c10.data(), cd.probe_nz_c10.size() * sizeof(int));
@@ -777,7 +782,7 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
 // launch sequence and arguments (same slot buffers, slice count, thickness map and probe defocus).
 // The line-pass autotuner runs before the capture (it times launches and waits for them).
 void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
-    if (tune_) pipe_ = tune_passes(m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1, cd);
+    if (tune_) tune(cd);
     std::vector<char> sig = graph_signature(cd);
     if (!g.exec || sig != g.sig) {
         if (g.exec) {
@@ -834,14 +839,18 @@ void Engine::run_conf(ConfData& cd) {
     if (m_.is_scanning()) run_stem(cd); else run_ew(cd);
 }
 
-// Autotuner of the line passes: for each (nx, ny, probes per launch) the process times, once, the
-// per-thread-load and the bulk-copy-fed variant of the row pass and of the column pass (one warm-up
-// and three timed launches each, on this engine's probe buffer, transmission function and
-// propagator) and keeps the faster of each. The variants compute bit-identical results (same
-// transforms, same rounding), so the choice affects only the speed.
-int Engine::tune_passes(int nprobe, ConfData& cd) {
+// Autotuner of the line passes. For each (nx, ny, allocated probes per launch) the process times,
+// once, on this engine's probe buffer, transmission function and propagator (one warm-up and three
+// timed launches each): the row pass and the column pass of the slice step in each variant (per-
+// thread loads; bulk-copy fed; bulk-copy fed in the alternative pipeline shape, RowPipeShape<N, 1>
+// and ColPipeShape<N, 1>), keeping the fastest of each; then, for STEM batches of at least 16
+// probes, the chosen step at the full and at half the batch, keeping the batch with the lower
+// time per probe. Every variant computes the same transforms with the same rounding, so the
+// choice changes only the speed (the FP64 detector partials of other tile widths are added in
+// another order).
+Engine::Tuning Engine::tune_passes(int nprobe, ConfData& cd) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int>, int> chosen;
+    static std::map<std::tuple<int, int, int>, Tuning> chosen;
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const auto key = std::make_tuple(nx, ny, nprobe);
     {
@@ -869,34 +878,66 @@ int Engine::tune_passes(int nprobe, ConfData& cd) {
     ra.out = d_psi_.p;
     ra.trans = d_trans_.p;
     ra.nx = nx;
-    ra.nprobe = nprobe;
     ra.scale = 1.0f;
+    ra.wait_ns = wait_ns_;
     ColArgs ca{};
     ca.in = d_psi_.p;
     ca.out = d_psi_.p;
     ca.ny = ny;
-    ca.nprobe = nprobe;
     ca.g = gdev_;
     ca.Px = cd.prop.p;
     ca.Py = cd.prop.p + nx;
     ca.det_w = col_det_width(nx);
+    ca.wait_ns = wait_ns_;
     const int step = COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE;
-    auto rows_t = [&](bool pipe) {
-        ra.err = pipe ? d_err_.p : nullptr;
-        ra.wait_ns = wait_ns_;
+    // variant v: 0 per-thread loads, 1 bulk-copy fed, 2 bulk-copy fed in the alternative shape
+    auto rows_t = [&](int v, int nb) {
+        ra.nprobe = nb;
+        ra.err = v ? d_err_.p : nullptr;
+        ra.shape = v == 2;
         return time_of([&] { launch_rows(ny, ROW_STEP, ra, 0, stream_); });
     };
-    auto cols_t = [&](bool pipe) {
-        ca.err = pipe ? d_err_.p : nullptr;
-        ca.wait_ns = wait_ns_;
+    auto cols_t = [&](int v, int nb) {
+        ca.nprobe = nb;
+        ca.err = v ? d_err_.p : nullptr;
+        ca.shape = v == 2;
         return time_of([&] { launch_cols(nx, step, ca, 0, stream_); });
     };
-    const int bits = (rows_t(true) < rows_t(false) ? 1 : 0) | (cols_t(true) < cols_t(false) ? 2 : 0);
+    float tr[3], tc[3];
+    for (int v = 0; v < 3; v++) {
+        tr[v] = rows_t(v, nprobe);
+        tc[v] = cols_t(v, nprobe);
+    }
+    int vr = 0, vc = 0;
+    for (int v = 1; v < 3; v++) {
+        if (tr[v] < tr[vr]) vr = v;
+        if (tc[v] < tc[vc]) vc = v;
+    }
+    Tuning t{(vr ? 1 : 0) | (vc ? 2 : 0), (vr == 2 ? 1 : 0) | (vc == 2 ? 2 : 0), nprobe};
+    if (m_.is_scanning() && nprobe >= 16 && (nprobe / 2) % 8 == 0) {
+        const float full = tr[vr] + tc[vc];
+        const float half = rows_t(vr, nprobe / 2) + cols_t(vc, nprobe / 2);
+        if (2.0f * half < 0.99f * full) t.nprobe = nprobe / 2;
+    }
     MTB_CUDA(cudaEventDestroy(a));
     MTB_CUDA(cudaEventDestroy(b));
     synchronize();
     std::lock_guard<std::mutex> lk(mu);
-    return chosen.emplace(key, bits).first->second;
+    return chosen.emplace(key, t).first->second;
+}
+
+void Engine::tune(ConfData& cd) {
+    const int nprobe = m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1;
+    const Tuning t = tune_passes(nprobe, cd);
+    pipe_ = t.pipe;
+    shape_ = t.shape;
+    run_batch_ = m_.is_scanning() ? std::max(1, std::min(t.nprobe, batch_)) : batch_;
+}
+
+void Engine::tuning(int* rows_variant, int* cols_variant, int* probes_per_launch) const {
+    *rows_variant = (pipe_ & 1) ? 1 + (shape_ & 1) : 0;
+    *cols_variant = (pipe_ & 2) ? 1 + ((shape_ >> 1) & 1) : 0;
+    *probes_per_launch = run_batch_;
 }
 
 // User-defined incident wave (Incident_Wave, src/incident_wave.cuh:48-52 and 92-110): the wave
@@ -1010,14 +1051,14 @@ void Engine::run_stem(ConfData& cd) {
     ra.nx = nx;
     ra.scale = 1.0f;
 
-    if (tune_) pipe_ = tune_passes(std::min(batch_, n_scan), cd);
+    if (tune_) tune(cd);
     // defocus-spread points (one without full integration), each over every probe, weighted
     // w_pr_0 * qt.w as a float (Multislice::STEM_ISTEM, src/tem_simulation.cuh:146-176)
     for (size_t it = 0; it < m_.ti_x.size(); it++) {
     ca.probe = probe_params(cd.probe_c_c_10[it], cd.probe_nz_c10[it], false);
     const double w = (double)(float)((double)m_.phonon_weight() * m_.ti_w[it]);
-    for (int p0 = 0; p0 < n_scan; p0 += batch_) {
-        const int nb = std::min(batch_, n_scan - p0);
+    for (int p0 = 0; p0 < n_scan; p0 += run_batch_) {
+        const int nb = std::min(run_batch_, n_scan - p0);
         ca.nprobe = nb;
         ra.nprobe = nb;
         // incident probes, generated in Fourier space and brought to the hybrid layout
@@ -1124,7 +1165,7 @@ void Engine::run_ew(ConfData& cd) {
     ca.g = gdev_;
     ca.n_det = 0;
     ca.P2 = d_bwl_.p;  // band-width limit of every propagation (NULL without bwl)
-    if (tune_) pipe_ = tune_passes(1, cd);
+    if (tune_) tune(cd);
     const bool conv = m_.is_convergent_wave();
     const bool user = m_.is_user_wave();
     const size_t rblock = (size_t)(cd.n_slice + (int)cd.thick_z_back_prop.size()) * pl;

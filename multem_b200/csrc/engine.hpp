@@ -119,6 +119,9 @@ class Engine {
     // the first check is a timeout.
     void set_wait_limit(long long ns) { wait_ns_ = ns < 0 ? 0 : ns; }
     int pass_variants() const { return pipe_; }
+    // The autotuner's choice: row and column pass variant (0 per-thread loads, 1 bulk-copy fed,
+    // 2 bulk-copy fed in the alternative shape) and probes per launch.
+    void tuning(int* rows_variant, int* cols_variant, int* probes_per_launch) const;
     void timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols);
 
   private:
@@ -159,7 +162,9 @@ class Engine {
     DevBuf<int> d_err_;              // set by a line pass whose bounded wait gave up
     int pipe_ = 3;                   // bulk-copy-fed line passes where they fit (bit 0 rows, bit 1 cols)
     long long wait_ns_ = 2000000000ll;  // bound of the line passes' waits for their copies
-    bool tune_ = true;               // choose pipe_ per shape with tune_passes (MTB_PIPE unset)
+    bool tune_ = true;               // choose pipe_, shape_, run_batch_ per shape with tune (MTB_PIPE unset)
+    int shape_ = 0;                  // alternative pipeline shape of the step passes (bit 0 rows, bit 1 cols)
+    int run_batch_ = 1;              // probes per launch (<= batch_, the allocated batch)
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;
     DevBuf<float2> d_tmp_;
@@ -196,7 +201,11 @@ class Engine {
     void build_tilt_ramp();
     void prepare_conf(ConfData& cd, int iconf);
     void run_conf(ConfData& cd);
-    int tune_passes(int nprobe, ConfData& cd);
+    struct Tuning {
+        int pipe, shape, nprobe;
+    };
+    Tuning tune_passes(int nprobe, ConfData& cd);
+    void tune(ConfData& cd);         // tune_passes for this engine's shape; sets pipe_, shape_, run_batch_
     void run_stem(ConfData& cd);
     void run_ew(ConfData& cd);
     void prop_tables(float dz, float2* px, float2* py, bool output, int irot = 0) const;

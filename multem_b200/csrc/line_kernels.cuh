@@ -618,11 +618,13 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     if (threadIdx.x == 0 && last_tph >= 0) mbar_drain(&tbar, (unsigned)last_tph);
 }
 
-// Row-pass pipeline shape per line length: threads per group, groups, early issue (where the
-// plan has a half-line exchange).
-template <int NY>
+// Row-pass pipeline shapes per line length: threads per group, groups, early issue (where the
+// plan has a half-line exchange). Shape 0 is the default of every row pass; shape 1, one warp per
+// group (so a group synchronises with __syncwarp only) and 16 groups, is the alternative the
+// autotuner may pick for the slice step.
+template <int NY, int V = 0>
 struct RowPipeShape {
-    static constexpr int GT = 64, NG = 8;
+    static constexpr int GT = V == 0 ? 64 : 32, NG = V == 0 ? 8 : 16;
     static constexpr bool EARLY = HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK;
 };
 
@@ -657,9 +659,11 @@ struct ColPipe {
                                (HBUF % 2 == 0) && SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
 };
 
-template <int NX>
+// Column-pass pipeline shapes: 2 groups of 256 threads (default), or 4 groups of 128 threads
+// (narrower tiles), the alternative the autotuner may pick for the slice step.
+template <int NX, int V = 0>
 struct ColPipeShape {
-    static constexpr int GT = 256, NG = 2;
+    static constexpr int GT = V == 0 ? 256 : 128, NG = V == 0 ? 2 : 4;
 };
 
 template <int NX, int FLAGS, int LDY, int GT, int NG, bool EARLY>
@@ -823,6 +827,23 @@ static void rows_launch(const RowArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NY>;
     using S = RowPipeShape<NY>;
     using RP = RowPipe<NY, S::GT, S::NG, S::EARLY>;
+    if constexpr (MODE == ROW_STEP) {
+        using S1 = RowPipeShape<NY, 1>;
+        using RP1 = RowPipe<NY, S1::GT, S1::NG, S1::EARLY>;
+        if constexpr (RP1::OK) {
+            if (a.err && a.shape == 1 && a.nprobe % S1::NG == 0) {
+                auto kern = rows_pipe_kernel<NY, MODE, S1::GT, S1::NG, S1::EARLY>;
+                static const int cap = max_ctas(kern, S1::GT * S1::NG, RP1::SMEM);
+                const int units = (a.nx / RP1::LPC) * a.nprobe / S1::NG;
+                int grid = grid_ctas > 0 ? grid_ctas : cap;
+                if (grid > units) grid = units;
+                kern<<<grid, S1::GT * S1::NG, RP1::SMEM, s>>>(a);
+                note_launch();
+                MTB_CUDA(cudaGetLastError());
+                return;
+            }
+        }
+    }
     if constexpr (RP::OK && MODE != ROW_FIRST_ONE) {
         if (a.err && a.nprobe % S::NG == 0) {
             constexpr size_t sm = RP::SMEM;
@@ -862,6 +883,25 @@ static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NX>;
     using S = ColPipeShape<NX>;
     using CP = ColPipe<NX, S::GT, S::NG>;
+    if constexpr (FLAGS == (COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE)) {
+        using S1 = ColPipeShape<NX, 1>;
+        using CP1 = ColPipe<NX, S1::GT, S1::NG>;
+        if constexpr (CP1::OK) {
+            if (a.err && a.shape == 1) {
+                auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S1::GT, S1::NG, CP1::EARLY_V>;
+                static const int cap = max_ctas(kern, S1::GT * S1::NG, CP1::SMEM);
+                const int items = (a.ny / CP1::W) * a.nprobe;
+                int grid = grid_ctas > 0 ? grid_ctas : cap;
+                if (grid > items) grid = items;
+                CUtensorMap map;
+                encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP1::W, CP1::BOXR);
+                kern<<<grid, S1::GT * S1::NG, CP1::SMEM, s>>>(a, map);
+                note_launch();
+                MTB_CUDA(cudaGetLastError());
+                return;
+            }
+        }
+    }
     if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
         if (a.err) {
             constexpr size_t sm = CP::SMEM;

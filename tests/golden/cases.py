@@ -557,3 +557,37 @@ def hrtem_coh_si001():
 def cbei_coh_si001():
     """cbei_si001 over four phonon configurations with the coherent contribution."""
     return _coherent(cbei_si001())
+
+
+def stem_bench512():
+    """The benchmark workload (SrTiO3(001) 8 x 8 x 25 cells, 8000 atoms, 512^2 grid, 50 dz_Proj
+    slices of 1.95 A, 300 kV, 21 mrad probe, ADF 40-80 and 80-200 mrad, seed 1) with a 16 x 16
+    raster over the same unit cell: 256 probes, one full probe batch of the engine at 512^2, and
+    two frozen-phonon configurations."""
+    from multem_b200 import specimens
+    p = specimens.stem_srtio3(nconf=2, seed=1)
+    p.scanning_ns = 16
+    return p
+
+
+def _au110_ac_2048(sim_type):
+    """Amorphous carbon (2 nm, 2.0 g/cm^3, minimum spacing 1.4 A) on Au(110) 12 x 17 x 60 cells
+    (29,292 atoms), 2048^2 grid, 200 kV, 2 A slices, two frozen-phonon configurations, written to a
+    256 x 256 window at the centre of the grid."""
+    from multem_b200 import specimens
+    p = specimens.au110_amorphous_carbon(nx=2048, ny=2048, nconf=2)
+    p.simulation_type = sim_type
+    p.output_area_ix_0, p.output_area_ix_e = 896, 1152
+    p.output_area_iy_0, p.output_area_iy_e = 896, 1152
+    return p
+
+
+def ew_au110_ac_2048():
+    """Exit wave (EWRS) of the large-field precision case on the 2048^2 grid (see _au110_ac_2048)."""
+    return _au110_ac_2048(52)
+
+
+def ed_au110_ac_2048():
+    """Electron diffraction pattern (ED) of the large-field precision case on the 2048^2 grid (see
+    _au110_ac_2048); the window is the centre of the shifted pattern."""
+    return _au110_ac_2048(31)

@@ -29,7 +29,8 @@ from cases import (amorph_au110, ew_1024, ew_384x256, prop_case, prop_tilt_case,
                    stem_monolayer_au, ew_po_si001, ew_wpo_si001, ew_bwl_si001, stem_bwl_srtio3, hrtem_bwl_si001,
                    ew_doyle_si001, ew_peng4_si001, ew_kirkland_si001, stem_peng12_srtio3, stem_kirkland_srtio3,
                    stem_ions_srtio3, ew_ions_si001, cbed_full_si001, cbei_full_si001, ed_coh_si001,
-                   cbed_coh_si001, ped_coh_si001, hrtem_coh_si001, cbei_coh_si001)
+                   cbed_coh_si001, ped_coh_si001, hrtem_coh_si001, cbei_coh_si001, stem_bench512,
+                   ew_au110_ac_2048, ed_au110_ac_2048)
 from oracle import reference as R  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -73,7 +74,9 @@ FULL_RUNS = (("ew_384x256", ew_384x256), ("stem_384", stem_384), ("ew_1024", ew_
              ("stem_kirkland_srtio3", stem_kirkland_srtio3), ("stem_ions_srtio3", stem_ions_srtio3),
              ("ew_ions_si001", ew_ions_si001), ("cbed_full_si001", cbed_full_si001),
              ("cbei_full_si001", cbei_full_si001), ("ed_coh_si001", ed_coh_si001), ("cbed_coh_si001", cbed_coh_si001),
-             ("ped_coh_si001", ped_coh_si001), ("hrtem_coh_si001", hrtem_coh_si001), ("cbei_coh_si001", cbei_coh_si001))
+             ("ped_coh_si001", ped_coh_si001), ("hrtem_coh_si001", hrtem_coh_si001), ("cbei_coh_si001", cbei_coh_si001),
+             ("stem_bench512", stem_bench512), ("ew_au110_ac_2048", ew_au110_ac_2048),
+             ("ed_au110_ac_2048", ed_au110_ac_2048))
 
 SPECIMENS = (("ew_rot_si001", ew_rot_si001), ("stem_rot_srtio3", stem_rot_srtio3), ("ew_monolayer_au", ew_monolayer_au),
              ("stem_monolayer_au", stem_monolayer_au), ("ew_po_si001", ew_po_si001), ("ew_wpo_si001", ew_wpo_si001))

@@ -58,3 +58,28 @@ def test_exit_wave_pipelined_matches_per_thread_kernels(nx, monkeypatch):
         r = api.ilc_multem(None, p)
         out[pipe] = np.stack([np.asarray(d["psi_coh"]) for d in r["data"]])
     np.testing.assert_array_equal(out[3], out[0])
+
+
+@pytest.mark.parametrize("nx", [256, 512, 1024])
+def test_alternative_pipeline_shapes_match(nx, monkeypatch):
+    """The autotuner's alternative pipeline shapes of the slice step (one-warp row groups, 4 x 128
+    column groups) give the waves of the per-thread-load kernels bit for bit."""
+    p = specimens.stem_srtio3(nx=nx, ny=nx, na=4, nb=4, nc=6, ns=4, nconf=1, seed=3)
+    ref = _stem(p, 0, monkeypatch)
+    monkeypatch.setenv("MTB_SHAPE", "3")
+    img = _stem(p, 3, monkeypatch)
+    monkeypatch.delenv("MTB_SHAPE")
+    if nx == 1024:
+        np.testing.assert_allclose(img, ref, rtol=1e-13, atol=0)
+    else:
+        np.testing.assert_array_equal(img, ref)
+
+
+def test_autotuner_reports_its_choice():
+    p = specimens.stem_srtio3(nx=512, ny=512, na=8, nb=8, nc=3, ns=16, nconf=1, seed=3)
+    e = api.Engine(p)
+    e.run()
+    t = e.tuning()
+    e.close()
+    assert t["rows"] in (0, 1, 2) and t["cols"] in (0, 1, 2)
+    assert t["probes_per_launch"] in (128, 256)
