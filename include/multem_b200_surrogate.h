@@ -5,9 +5,11 @@
  * averaged over a few, with a per-pixel error estimate used to fall back to the plain simulation.
  *
  * Tensors are device pointers in NCHW layout; "bf16" arguments point to __nv_bfloat16 data, the
- * others to float. Convolutions are 3x3 with zero padding 1, FP32 accumulation; all reductions run
- * in a fixed order. Every call is asynchronous on `stream` (a cudaStream_t, NULL = default) and
- * returns MT_OK or an error status without a message. */
+ * others to float. Convolutions are 3x3 with zero padding 1, computed as BF16 GEMMs on the tensor
+ * cores (tcgen05) with FP32 accumulation; all reductions run in a fixed order. Every call is
+ * asynchronous on `stream` (a cudaStream_t, NULL = default) and returns MT_OK or an error status
+ * without a message. The convolutions of one device share a workspace from the library's memory
+ * pool (grown on demand): issue them on one stream, or order them. */
 #ifndef MULTEM_B200_SURROGATE_H
 #define MULTEM_B200_SURROGATE_H
 
@@ -50,6 +52,9 @@ mt_status mt_sg_upsample2(const void* in, void* out, int B, int C, int H, int W,
 mt_status mt_sg_add(const void* a, const void* b, void* out, long long n, void* stream);
 /* b (bf16) = a (float), n values. */
 mt_status mt_sg_to_bf16(const float* a, void* b, int n, void* stream);
+/* Synchronises `stream`; MT_ERR_TIMEOUT (and the flag cleared) when a convolution's GEMM issued
+ * before gave up waiting for its operands (every wait is bounded at 1 s), MT_OK otherwise. */
+mt_status mt_sg_check(void* stream);
 
 #ifdef __cplusplus
 }

@@ -145,6 +145,7 @@ SIGNATURES = {
     "mt_sg_loss": (c_int, [_VP, _VP, _VP, _VP, _VP, _VP, c_int, c_int, c_int, C.c_float, _VP]),
     "mt_sg_adam": (c_int, [_VP, _VP, _VP, _VP, _VP, c_int, C.c_float, C.c_float, C.c_float, C.c_float, c_int, _VP]),
     "mt_sg_to_bf16": (c_int, [_VP, _VP, c_int, _VP]),
+    "mt_sg_check": (c_int, [_VP]),
     "mt_sg_pool2": (c_int, [_VP, _VP, c_int, c_int, c_int, c_int, C.c_float, _VP]),
     "mt_sg_upsample2": (c_int, [_VP, _VP, c_int, c_int, c_int, c_int, C.c_float, _VP]),
     "mt_sg_add": (c_int, [_VP, _VP, _VP, C.c_longlong, _VP]),

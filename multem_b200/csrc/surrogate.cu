@@ -8,134 +8,134 @@
 //   data grad    din[b,i,y,x]   = sum_{o,ky,kx} w[o,i,ky,kx] * dout'[b,o,y-ky+1,x-kx+1]
 //   weight grad  dw[o,i,ky,kx]  = sum_{b,y,x} dout'[b,o,y,x] * in[b,i,y+ky-1,x+kx-1]
 // where dout' is the output gradient masked by the ReLU of the output when the layer has one.
-// Reductions run in a fixed order (deterministic results).
+//
+// The three convolutions run on the tensor cores as GEMMs (umma_gemm.cuh), with k = c*9 + ky*3 + kx
+// and pixels p = (b, y, x):
+//   forward      C[p][o]   = A[p][k] . Wf[o][k],      A = im2col(in),     Wf[o][k] = w[o][k]
+//   data grad    C[p][i]   = A'[p][k'] . Wd[i][k'],   A' = im2col(dout'), Wd[i][o*9+q] = w[o][i][8-q]
+//   weight grad  C[k][o]   = X[k][p] . Y[o][p],       X = im2col(in) transposed plus a row of ones
+//                                                     (its C row is the bias gradient), Y = dout'
+// The operand layouts are written by small gather kernels into a per-device workspace; the GEMM
+// writes FP32 partial sums per K split, and a finalize kernel adds them in split order (fixed-order
+// reductions: deterministic results), applies bias and ReLU and writes the NCHW (or [o][k]) result.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 #include "common.hpp"
+#include "devmem.hpp"
 #include "multem_b200_surrogate.h"
+#include "umma_gemm.cuh"
 
 namespace {
 
-constexpr int TILE = 16;  // output tile edge per CTA (16 x 16 threads)
-constexpr int OB = 8;     // output channels per CTA
-
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
 
-// Forward (and, with TRANSPOSE, the data gradient: channels swapped and the kernel flipped).
-// grid: (ceil(W/16) * ceil(H/16), ceil(Cout/OB), B); block 16 x 16.
-template <bool TRANSPOSE>
-__global__ void __launch_bounds__(256) conv3x3_kernel(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ w,
-                                                      const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
-                                                      __nv_bfloat16* __restrict__ out_bf, float* __restrict__ out_f,
-                                                      int B, int Cin, int Cout, int H, int W, int relu) {
-    __shared__ float tile[TILE + 2][TILE + 2];
-    __shared__ float wt[OB][9];
-    const int tiles_x = (W + TILE - 1) / TILE;
-    const int tx0 = (blockIdx.x % tiles_x) * TILE, ty0 = (blockIdx.x / tiles_x) * TILE;
-    const int o0 = blockIdx.y * OB, b = blockIdx.z;
-    const int lx = threadIdx.x, ly = threadIdx.y, tid = ly * TILE + lx;
-    const int x = tx0 + lx, y = ty0 + ly;
-    float acc[OB];
-#pragma unroll
-    for (int k = 0; k < OB; k++) acc[k] = 0.0f;
-    for (int i = 0; i < Cin; i++) {
-        // input tile with a one-pixel halo; in the data-gradient form the "input" is the masked
-        // output gradient of channel i
-        for (int e = tid; e < (TILE + 2) * (TILE + 2); e += TILE * TILE) {
-            const int yy = ty0 - 1 + e / (TILE + 2), xx = tx0 - 1 + e % (TILE + 2);
-            float v = 0.0f;
+// ---------------------------------------------------------------------------------------------
+// GEMM operand layouts
+
+// A[m][k] = in[b][c][y+ky-1][x+kx-1] for k = c*9 + ky*3 + kx < 9*C (zero outside the image and for
+// the padding k in [9C, ldk)); with `mask`, zero where mask (same layout as in) is not positive.
+__global__ void im2col_kernel(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ mask,
+                              __nv_bfloat16* __restrict__ A, int B, int C, int H, int W, int ldk) {
+    const int HW = H * W;
+    const size_t n = (size_t)B * HW * ldk;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(e % ldk);
+        const int m = (int)(e / ldk);
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (k < 9 * C) {
+            const int c = k / 9, q = k % 9, b = m / HW, yx = m % HW;
+            const int yy = yx / W + q / 3 - 1, xx = yx % W + q % 3 - 1;
             if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
-                const size_t idx = (((size_t)b * Cin + i) * H + yy) * W + xx;
-                v = bf(in[idx]);
-                if (mask && !(bf(mask[idx]) > 0.0f)) v = 0.0f;
+                const size_t idx = (((size_t)b * C + c) * H + yy) * W + xx;
+                v = in[idx];
+                if (mask && !(bf(mask[idx]) > 0.0f)) v = __float2bfloat16_rn(0.0f);
             }
-            tile[e / (TILE + 2)][e % (TILE + 2)] = v;
         }
-        for (int e = tid; e < OB * 9; e += TILE * TILE) {
-            const int k = e / 9, q = e % 9, o = o0 + k;
-            float v = 0.0f;
-            if (o < Cout) {
-                // forward: w[o][i][q]; data gradient: w[i][o][8 - q] (flipped, channels swapped)
-                v = TRANSPOSE ? bf(w[((size_t)i * Cout + o) * 9 + (8 - q)]) : bf(w[((size_t)o * Cin + i) * 9 + q]);
-            }
-            wt[k][q] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int ky = 0; ky < 3; ky++)
-#pragma unroll
-            for (int kx = 0; kx < 3; kx++) {
-                const float v = tile[ly + ky][lx + kx];
-#pragma unroll
-                for (int k = 0; k < OB; k++) acc[k] = __fmaf_rn(wt[k][ky * 3 + kx], v, acc[k]);
-            }
-        __syncthreads();
-    }
-    if (x >= W || y >= H) return;
-#pragma unroll
-    for (int k = 0; k < OB; k++) {
-        const int o = o0 + k;
-        if (o >= Cout) break;
-        float v = acc[k] + (bias ? bias[o] : 0.0f);
-        if (relu) v = fmaxf(v, 0.0f);
-        const size_t idx = (((size_t)b * Cout + o) * H + y) * W + x;
-        if (out_bf) out_bf[idx] = __float2bfloat16_rn(v);
-        if (out_f) out_f[idx] = v;
+        A[e] = v;
     }
 }
 
-// Weight and bias gradients: one CTA per (o, i) pair (i == Cin computes the bias gradient of o).
-// 256 threads stride over the B*H*W output pixels; per-thread partial sums are reduced in a fixed
-// tree order.
-__global__ void __launch_bounds__(256) conv3x3_wgrad_kernel(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ dout,
-                                                            const __nv_bfloat16* __restrict__ mask, float* __restrict__ dw,
-                                                            float* __restrict__ db, int B, int Cin, int Cout, int H, int W) {
-    const int o = blockIdx.x / (Cin + 1), i = blockIdx.x % (Cin + 1);
-    const bool bias_only = (i == Cin);
-    float acc[9];
-#pragma unroll
-    for (int q = 0; q < 9; q++) acc[q] = 0.0f;
-    const int npix = B * H * W;
-    for (int p = threadIdx.x; p < npix; p += blockDim.x) {
-        const int b = p / (H * W), yx = p % (H * W), y = yx / W, x = yx % W;
-        const size_t oi = (((size_t)b * Cout + o) * H + y) * W + x;
-        float g = bf(dout[oi]);
-        if (mask && !(bf(mask[oi]) > 0.0f)) g = 0.0f;
-        if (g == 0.0f) continue;
-        if (bias_only) {
-            acc[0] += g;
-            continue;
-        }
-#pragma unroll
-        for (int ky = 0; ky < 3; ky++)
-#pragma unroll
-            for (int kx = 0; kx < 3; kx++) {
-                const int yy = y + ky - 1, xx = x + kx - 1;
-                if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                    acc[ky * 3 + kx] = __fmaf_rn(g, bf(in[(((size_t)b * Cin + i) * H + yy) * W + xx]), acc[ky * 3 + kx]);
+// X[k][p] = in[b][c][y+ky-1][x+kx-1] (the transposed im2col, p = (b, y, x)) for k < 9C, X[9C][p] = 1,
+// zero for the padding p in [B*H*W, ldp).
+__global__ void im2col_t_kernel(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ X, int B, int C,
+                                int H, int W, int ldp) {
+    const int HW = H * W, P = B * HW;
+    const size_t n = (size_t)(9 * C + 1) * ldp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(e % ldp);
+        const int k = (int)(e / ldp);
+        float v = 0.0f;
+        if (p < P) {
+            if (k == 9 * C) {
+                v = 1.0f;
+            } else {
+                const int c = k / 9, q = k % 9, b = p / HW, yx = p % HW;
+                const int yy = yx / W + q / 3 - 1, xx = yx % W + q % 3 - 1;
+                if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = bf(in[(((size_t)b * C + c) * H + yy) * W + xx]);
             }
-    }
-    __shared__ float red[9][256];
-#pragma unroll
-    for (int q = 0; q < 9; q++) red[q][threadIdx.x] = acc[q];
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s)
-#pragma unroll
-            for (int q = 0; q < 9; q++) red[q][threadIdx.x] += red[q][threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        if (bias_only) {
-            db[o] = red[0][0];
-        } else {
-#pragma unroll
-            for (int q = 0; q < 9; q++) dw[((size_t)o * Cin + i) * 9 + q] = red[q][0];
         }
+        X[e] = __float2bfloat16_rn(v);
+    }
+}
+
+// Y[c][p] = d[b][c][y][x] (channel-major, p = (b, y, x)), zero where mask is not positive and for
+// the padding p in [B*HW, ldp).
+__global__ void channel_major_kernel(const __nv_bfloat16* __restrict__ d, const __nv_bfloat16* __restrict__ mask,
+                                     __nv_bfloat16* __restrict__ Y, int B, int C, int HW, int ldp) {
+    const int P = B * HW;
+    const size_t n = (size_t)C * ldp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(e % ldp);
+        const int c = (int)(e / ldp);
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (p < P) {
+            const size_t idx = ((size_t)(p / HW) * C + c) * HW + p % HW;
+            v = d[idx];
+            if (mask && !(bf(mask[idx]) > 0.0f)) v = __float2bfloat16_rn(0.0f);
+        }
+        Y[e] = v;
+    }
+}
+
+// Weights as the GEMM's B operand [rows][ldk]: forward Wf[o][k] = w[o][k] (k < 9*Cin); data
+// gradient Wd[i][o*9 + q] = w[o][i][8 - q] (k < 9*Cout, the kernel flipped); zero padding.
+__global__ void pack_weights_kernel(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ Bm, int Cout,
+                                    int Cin, int ldk, int data_grad) {
+    const int rows = data_grad ? Cin : Cout, K = data_grad ? 9 * Cout : 9 * Cin;
+    const size_t n = (size_t)rows * ldk;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(e % ldk), r = (int)(e / ldk);
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (k < K) v = data_grad ? w[((size_t)(k / 9) * Cin + r) * 9 + (8 - k % 9)] : w[(size_t)r * K + k];
+        Bm[e] = v;
+    }
+}
+
+// out[(m / mdiv) * s_mq + (m % mdiv) * s_mr + n * s_n] = act(bias[n] + sum over splits s, in order,
+// of part[s][row0 + m][n]) for m < M, n < N; m runs fastest over the threads (coalesced stores for
+// the NCHW and [o][k] layouts).
+__global__ void gemm_finalize_kernel(const float* __restrict__ part, int splits, int Mtot, int N, int row0, int M,
+                                     const float* __restrict__ bias, int relu, __nv_bfloat16* __restrict__ out_bf,
+                                     float* __restrict__ out_f, long long mdiv, long long s_mq, long long s_mr,
+                                     long long s_n) {
+    const size_t n_all = (size_t)M * N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_all; e += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(e % M), n = (int)(e / M);
+        float acc = 0.0f;
+        for (int s = 0; s < splits; s++) acc += part[((size_t)s * Mtot + row0 + m) * N + n];
+        float v = acc + (bias ? bias[n] : 0.0f);
+        if (relu) v = fmaxf(v, 0.0f);
+        const long long idx = (m / mdiv) * s_mq + (m % mdiv) * s_mr + n * s_n;
+        if (out_bf) out_bf[idx] = __float2bfloat16_rn(v);
+        if (out_f) out_f[idx] = v;
     }
 }
 
@@ -237,9 +237,141 @@ void check_shape(int B, int Cin, int Cout, int H, int W) {
         mtb::fail(MT_ERR_INVALID_ARG, "bad convolution shape");
 }
 
-dim3 conv_grid(int B, int Cout, int H, int W) {
-    return dim3((unsigned)(((W + TILE - 1) / TILE) * ((H + TILE - 1) / TILE)), (unsigned)((Cout + OB - 1) / OB),
-                (unsigned)B);
+constexpr long long kWaitNs = 1000000000ll;  // bound of every wait of the GEMM (1 s)
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+int round8(int v) { return (v + 7) / 8 * 8; }
+
+// Per-device workspace of the convolutions (GEMM operands and partial sums), grown on demand from
+// the library's pool, and the error flag of the GEMM's bounded waits. Calls on one device share
+// them, so they must be issued on one stream (or otherwise ordered), as the surrogate's host code
+// does.
+struct Workspace {
+    unsigned char* p = nullptr;
+    size_t bytes = 0;
+    int* err = nullptr;
+    int dev = 0;
+};
+std::mutex g_ws_mu;
+std::map<int, Workspace> g_ws;
+
+Workspace& workspace(size_t bytes) {
+    int dev = 0;
+    MTB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    Workspace& w = g_ws[dev];
+    if (!w.err) {
+        w.err = static_cast<int*>(mtb::dev_alloc(256, &w.dev));
+        MTB_CUDA(cudaMemset(w.err, 0, sizeof(int)));
+    }
+    if (w.bytes < bytes) {
+        if (w.p) mtb::dev_free(w.p, w.dev);  // waits for the device: earlier calls may still use it
+        w.p = nullptr;
+        w.bytes = 0;
+        const size_t nb = std::max(bytes, 2 * w.bytes);
+        w.p = static_cast<unsigned char*>(mtb::dev_alloc(nb, &w.dev));
+        w.bytes = nb;
+    }
+    return w;
+}
+
+// Tensor map of a bf16 [rows][ld] K-major operand: boxes of 64 k x box_rows rows with the 128-byte
+// swizzle (the canonical layout of the MMA's shared-memory descriptors); out-of-bounds reads are 0.
+void encode_kmajor(CUtensorMap* map, const void* base, int rows, int ld, int box_rows) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        MTB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) mtb::fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    const cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)mtb::umma::BK, (cuuint32_t)box_rows};
+    const cuuint32_t estride[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) mtb::fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled failed for a GEMM operand");
+}
+
+int gemm_bn(int N) { return N <= 16 ? 16 : N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256; }
+
+// K split of an M x N x K product: enough CTAs to cover the SMs twice when the tiles alone do not,
+// at least two K blocks per split.
+void gemm_split(int M, int N, int K, int* splits, int* kb_per_split) {
+    const int nkb = (K + mtb::umma::BK - 1) / mtb::umma::BK;
+    const int bn = gemm_bn(N);
+    const int tiles = ((M + mtb::umma::BM - 1) / mtb::umma::BM) * ((N + bn - 1) / bn);
+    int want = tiles >= 296 ? 1 : (296 + tiles - 1) / tiles;
+    int kps = std::max(2, (nkb + want - 1) / want);
+    if (kps > nkb) kps = nkb;
+    *kb_per_split = kps;
+    *splits = (nkb + kps - 1) / kps;
+}
+
+template <int BN>
+void gemm_launch(const CUtensorMap& ma, const CUtensorMap& mb, float* part, int M, int N, int nkb, int splits,
+                 int kps, int* err, cudaStream_t st) {
+    using T = mtb::umma::Tile<BN>;
+    auto kern = mtb::umma::gemm_kernel<BN>;
+    MTB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    // resident CTAs per SM are bounded by shared memory; their tensor-memory columns must fit the
+    // SM's 512, or an allocation would wait for another CTA to exit
+    int occ = 0;
+    MTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, T::SMEM));
+    if (occ < 1 || occ * T::TCOLS > 512) mtb::fail(MT_ERR_INTERNAL, "GEMM tile does not fit an SM's tensor memory");
+    const dim3 grid((unsigned)((M + mtb::umma::BM - 1) / mtb::umma::BM), (unsigned)splits, (unsigned)((N + BN - 1) / BN));
+    kern<<<grid, 128, T::SMEM, st>>>(ma, mb, part, M, N, nkb, kps, err, kWaitNs);
+    MTB_CUDA(cudaGetLastError());
+}
+
+// part[s][m][n] = sum over split s of A[m][:] . B[n][:] (A [M][lda], B [N][ldb], bf16, K valid).
+void gemm(const __nv_bfloat16* A, int M, int lda, const __nv_bfloat16* Bm, int N, int ldb, int K, float* part,
+          int splits, int kps, int* err, cudaStream_t st) {
+    const int bn = gemm_bn(N);
+    CUtensorMap ma, mb;
+    encode_kmajor(&ma, A, M, lda, mtb::umma::BM);
+    encode_kmajor(&mb, Bm, N, ldb, bn);
+    const int nkb = (K + mtb::umma::BK - 1) / mtb::umma::BK;
+    switch (bn) {
+        case 16: gemm_launch<16>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+        case 32: gemm_launch<32>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+        case 64: gemm_launch<64>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+        case 128: gemm_launch<128>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+        default: gemm_launch<256>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+    }
+}
+
+void finalize(const float* part, int splits, int Mtot, int N, int row0, int M, const float* bias, int relu,
+              __nv_bfloat16* out_bf, float* out_f, long long mdiv, long long s_mq, long long s_mr, long long s_n,
+              cudaStream_t st) {
+    gemm_finalize_kernel<<<elem_grid((size_t)M * N), 256, 0, st>>>(part, splits, Mtot, N, row0, M, bias, relu, out_bf,
+                                                                  out_f, mdiv, s_mq, s_mr, s_n);
+    MTB_CUDA(cudaGetLastError());
+}
+
+// out (NCHW, Cout channels) = conv of `in` (Cin channels, masked where given) with the forward
+// or data-gradient weight layout.
+void conv_as_gemm(const __nv_bfloat16* in, const __nv_bfloat16* mask, int Cin_eff, const __nv_bfloat16* w, int Cout,
+                  int Cin, bool data_grad, const float* bias, int relu, __nv_bfloat16* out_bf, float* out_f, int B,
+                  int H, int W, cudaStream_t st) {
+    const int P = B * H * W, K = 9 * Cin_eff, ldk = round8(K);
+    const int N = data_grad ? Cin : Cout;
+    int splits = 1, kps = 1;
+    gemm_split(P, N, K, &splits, &kps);
+    const size_t offB = align256((size_t)P * ldk * 2), offP = offB + align256((size_t)N * ldk * 2);
+    Workspace& ws = workspace(offP + (size_t)splits * P * N * 4);
+    auto* A = reinterpret_cast<__nv_bfloat16*>(ws.p);
+    auto* Bm = reinterpret_cast<__nv_bfloat16*>(ws.p + offB);
+    auto* part = reinterpret_cast<float*>(ws.p + offP);
+    im2col_kernel<<<elem_grid((size_t)P * ldk), 256, 0, st>>>(in, mask, A, B, Cin_eff, H, W, ldk);
+    MTB_CUDA(cudaGetLastError());
+    pack_weights_kernel<<<elem_grid((size_t)N * ldk), 256, 0, st>>>(w, Bm, Cout, Cin, ldk, data_grad ? 1 : 0);
+    MTB_CUDA(cudaGetLastError());
+    gemm(A, P, ldk, Bm, N, ldk, K, part, splits, kps, ws.err, st);
+    const long long HW = (long long)H * W;
+    finalize(part, splits, P, N, 0, P, bias, relu, out_bf, out_f, HW, (long long)N * HW, 1, HW, st);
 }
 
 }  // namespace
@@ -251,10 +383,8 @@ mt_status mt_sg_conv3x3_forward(const void* in, const void* w, const float* bias
     return run([&] {
         check_shape(B, Cin, Cout, H, W);
         if (!in || !w || (!out_bf16 && !out_f32)) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
-        conv3x3_kernel<false><<<conv_grid(B, Cout, H, W), dim3(TILE, TILE), 0, (cudaStream_t)stream>>>(
-            (const __nv_bfloat16*)in, (const __nv_bfloat16*)w, bias, nullptr, (__nv_bfloat16*)out_bf16, out_f32, B, Cin,
-            Cout, H, W, relu);
-        MTB_CUDA(cudaGetLastError());
+        conv_as_gemm((const __nv_bfloat16*)in, nullptr, Cin, (const __nv_bfloat16*)w, Cout, Cin, false, bias, relu,
+                     (__nv_bfloat16*)out_bf16, out_f32, B, H, W, (cudaStream_t)stream);
     });
 }
 
@@ -263,11 +393,10 @@ mt_status mt_sg_conv3x3_backward_data(const void* dout, const void* out_mask, co
     return run([&] {
         check_shape(B, Cin, Cout, H, W);
         if (!dout || !w || !din) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
-        // the data gradient is a convolution from Cout "input" channels to Cin outputs
-        conv3x3_kernel<true><<<conv_grid(B, Cin, H, W), dim3(TILE, TILE), 0, (cudaStream_t)stream>>>(
-            (const __nv_bfloat16*)dout, (const __nv_bfloat16*)w, nullptr, (const __nv_bfloat16*)out_mask,
-            (__nv_bfloat16*)din, nullptr, B, Cout, Cin, H, W, 0);
-        MTB_CUDA(cudaGetLastError());
+        // the data gradient is a convolution of the masked output gradient (Cout channels) with the
+        // flipped, transposed kernel
+        conv_as_gemm((const __nv_bfloat16*)dout, (const __nv_bfloat16*)out_mask, Cout, (const __nv_bfloat16*)w, Cout,
+                     Cin, true, nullptr, 0, (__nv_bfloat16*)din, nullptr, B, H, W, (cudaStream_t)stream);
     });
 }
 
@@ -276,10 +405,45 @@ mt_status mt_sg_conv3x3_backward_weight(const void* in, const void* dout, const 
     return run([&] {
         check_shape(B, Cin, Cout, H, W);
         if (!in || !dout || !dw || !db) mtb::fail(MT_ERR_INVALID_ARG, "NULL tensor");
-        conv3x3_wgrad_kernel<<<(unsigned)(Cout * (Cin + 1)), 256, 0, (cudaStream_t)stream>>>(
-            (const __nv_bfloat16*)in, (const __nv_bfloat16*)dout, (const __nv_bfloat16*)out_mask, dw, db, B, Cin, Cout,
-            H, W);
+        const cudaStream_t st = (cudaStream_t)stream;
+        const int HW = H * W, P = B * HW, ldp = round8(P), M = 9 * Cin + 1;
+        int splits = 1, kps = 1;
+        gemm_split(M, Cout, P, &splits, &kps);
+        const size_t offY = align256((size_t)M * ldp * 2), offP = offY + align256((size_t)Cout * ldp * 2);
+        Workspace& ws = workspace(offP + (size_t)splits * M * Cout * 4);
+        auto* X = reinterpret_cast<__nv_bfloat16*>(ws.p);
+        auto* Y = reinterpret_cast<__nv_bfloat16*>(ws.p + offY);
+        auto* part = reinterpret_cast<float*>(ws.p + offP);
+        im2col_t_kernel<<<elem_grid((size_t)M * ldp), 256, 0, st>>>((const __nv_bfloat16*)in, X, B, Cin, H, W, ldp);
         MTB_CUDA(cudaGetLastError());
+        channel_major_kernel<<<elem_grid((size_t)Cout * ldp), 256, 0, st>>>(
+            (const __nv_bfloat16*)dout, (const __nv_bfloat16*)out_mask, Y, B, Cout, HW, ldp);
+        MTB_CUDA(cudaGetLastError());
+        gemm(X, M, ldp, Y, Cout, ldp, P, part, splits, kps, ws.err, st);
+        // rows k < 9*Cin: dw[o][k]; row 9*Cin: db[o]
+        finalize(part, splits, M, Cout, 0, M - 1, nullptr, 0, nullptr, dw, M - 1, 0, 1, M - 1, st);
+        finalize(part, splits, M, Cout, M - 1, 1, nullptr, 0, nullptr, db, 1, 0, 0, 1, st);
+    });
+}
+
+mt_status mt_sg_check(void* stream) {
+    return run([&] {
+        MTB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        int dev = 0;
+        MTB_CUDA(cudaGetDevice(&dev));
+        int* err = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(g_ws_mu);
+            auto it = g_ws.find(dev);
+            if (it != g_ws.end()) err = it->second.err;
+        }
+        if (!err) return;
+        int e = 0;
+        MTB_CUDA(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            MTB_CUDA(cudaMemset(err, 0, sizeof(int)));
+            mtb::fail(MT_ERR_TIMEOUT, "a tensor-core GEMM gave up waiting for its operands");
+        }
     });
 }
 

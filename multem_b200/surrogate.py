@@ -189,12 +189,14 @@ class Net:
             wb = self.wb[k] if k < len(self.w) else None
             capi.check(self.lib.mt_sg_adam(_p(p), None if wb is None else _p(wb), _p(g), _p(self.m[k]), _p(self.v[k]),
                                            p.numel(), float(lr), 0.9, 0.999, 1e-8, self.step, None))
+        capi.check(self.lib.mt_sg_check(None))  # raises if a convolution's bounded wait ran out
         return float(terms.sum().item()) / terms.numel()
 
     def predict(self, x, scale=None):
         """x: bf16 [B,in_ch,H,W] -> (prediction, error estimate), fp32 numpy [B,H,W] each; `scale`
         (numpy [B] or None) as in training."""
         _, head = self.forward(x)
+        capi.check(self.lib.mt_sg_check(None))
         h = head.cpu().numpy()
         xn = x.float().cpu().numpy()[:, 0]
         sc = np.ones(h.shape[0], np.float32) if scale is None else np.asarray(scale, np.float32)

@@ -22,7 +22,9 @@ def _rel(a, b):
     return float((a - b).norm() / b.norm())
 
 
-@pytest.mark.parametrize("B,Cin,Cout,H,W", [(2, 3, 5, 20, 37), (3, 8, 16, 32, 32), (1, 16, 2, 16, 16)])
+@pytest.mark.parametrize("B,Cin,Cout,H,W", [(2, 3, 5, 20, 37), (3, 8, 16, 32, 32), (1, 16, 2, 16, 16),
+                                             (2, 64, 128, 32, 32), (1, 256, 256, 8, 8), (4, 32, 32, 64, 64),
+                                             (3, 128, 64, 16, 24)])
 def test_conv3x3_forward_and_gradients_match_torch(B, Cin, Cout, H, W):
     torch = pytest.importorskip("torch")
     F = torch.nn.functional
