@@ -241,6 +241,29 @@ mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislic
 mt_status mt_multislice_run_batch(const mt_system_conf* conf, int n, const mt_input_multislice* in,
                                   mt_output_multislice* out, mt_status* status);
 
+/* ---- MATLAB files (level-5 MAT-files, MATLAB -v6 / -v7) ----
+ * The file-level form of the MATLAB entry `output_multislice = ilc_multem(prms.system_conf, prms)`
+ * (mex_files_multem/ilc_multem.cu:520-546, matlab_functions/+multem_input/parameters.m:247-250):
+ * the input is the struct that multem_input.parameters.toStruct returns, saved with `save`
+ * (read as read_input_multislice reads it, mex_files_multem/ilc_multem.cu:38-379; absent fields
+ * take the class defaults); the output is the struct set_struct_multislice builds
+ * (mex_files_multem/ilc_multem.cu:382-481). Big-endian, -v7.3 (HDF5), sparse and object values are
+ * rejected with MT_ERR_INVALID_ARG. */
+typedef struct mt_mat_input mt_mat_input;
+/* Reads struct variable `var` (NULL or "": the first struct in the file) of the MAT-file at `path`
+ * into *in (pointers into storage owned by *handle, valid until mt_mat_input_close) and, when conf
+ * is not NULL, its system_conf field into *conf (defaults when the struct has none). Host only. */
+mt_status mt_mat_input_open(const char* path, const char* var, mt_mat_input** handle, mt_system_conf* conf,
+                            mt_input_multislice* in);
+mt_status mt_mat_input_close(mt_mat_input* handle);
+/* Writes the output of a run of `in` (sizes from mt_output_query) as the struct variable
+ * "output_multislice" (or `var`) of a new MAT-file at `path`; compress != 0 writes -v7 (zlib)
+ * elements. Host only. */
+mt_status mt_mat_output_write(const char* path, const char* var, const mt_input_multislice* in,
+                              const mt_output_multislice* out, int compress);
+/* mt_mat_input_open + mt_multislice_run on the file's system_conf + mt_mat_output_write. */
+mt_status mt_multislice_run_mat(const char* in_path, const char* var, const char* out_path, int compress);
+
 /* Handle-based form: set-up once (tables, specimen, buffers), run many times.
  * mt_engine_create = Multislice::set_input_data (src/tem_simulation.cuh:51-69). */
 mt_status mt_engine_create(const mt_system_conf* conf, const mt_input_multislice* in, mt_engine** eng);

@@ -97,6 +97,66 @@ def ilc_multem(system_conf: SystemConf | None, params: Parameters) -> dict:
     return buf.to_dict()
 
 
+def ilc_multem_mat(in_path, out_path, var: str | None = None, compress: bool = False) -> None:
+    """File-level form of ilc_multem for MATLAB users (mt_multislice_run_mat): reads the input struct
+    (variable `var`, else the first struct) from the MAT-file `in_path`, runs it on the GPU of its
+    system_conf, and writes `output_multislice` to the MAT-file `out_path` (-v7 compressed when
+    `compress`)."""
+    lib = capi.load()
+    capi.check(lib.mt_multislice_run_mat(str(in_path).encode(), var.encode() if var else None,
+                                         str(out_path).encode(), int(compress)))
+
+
+class MatInput:
+    """An input struct read from a MAT-file (mt_mat_input_open): .conf and .c are the C ABI
+    structs, valid while the object lives."""
+
+    def __init__(self, path, var: str | None = None):
+        self.lib = capi.load()
+        self.h = C.c_void_p()
+        self.conf = capi.MtSystemConf()
+        self.c = capi.MtInputMultislice()
+        capi.check(self.lib.mt_mat_input_open(str(path).encode(), var.encode() if var else None, C.byref(self.h),
+                                              C.byref(self.conf), C.byref(self.c)))
+
+    def close(self):
+        if self.h:
+            self.lib.mt_mat_input_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_output_mat(path, params: Parameters, out: dict, var: str | None = None, compress: bool = False) -> None:
+    """Write an ilc_multem output dict of a run of `params` as MATLAB's output struct
+    (mt_mat_output_write)."""
+    lib = capi.load()
+    d = output_dims(params)
+    buf = OutputBuffers(d)
+    buf.c.dx, buf.c.dy = float(out["dx"]), float(out["dy"])
+    buf.x[:d.n_x], buf.y[:d.n_y], buf.thick[:d.n_thick] = out["x"], out["y"], out["thick"]
+    nx, ny = d.nx, d.ny
+    for it, e in enumerate(out["data"]):
+        if buf.image_tot is not None:
+            buf.image_tot.reshape(d.n_thick, d.n_detector, nx, ny)[it] = np.stack([im.T for im in e["image_tot"]])
+        if buf.image_coh is not None:
+            buf.image_coh.reshape(d.n_thick, d.n_detector, nx, ny)[it] = np.stack([im.T for im in e["image_coh"]])
+        if buf.m2psi_tot is not None:
+            buf.m2psi_tot.reshape(d.n_thick, nx, ny)[it] = e["m2psi_tot"].T
+        if buf.psi_coh is not None:
+            r = buf.psi_coh.reshape(d.n_thick, nx, ny, 2)[it]
+            r[..., 0], r[..., 1] = e["psi_coh"].T.real, e["psi_coh"].T.imag
+        if buf.m2psi_coh is not None:
+            buf.m2psi_coh.reshape(d.n_thick, nx, ny)[it] = e["m2psi_coh"].T
+    s, keep = params.to_c()
+    capi.check(lib.mt_mat_output_write(str(path).encode(), var.encode() if var else None, C.byref(s),
+                                       C.byref(buf.c), int(compress)))
+
+
 def input_report(params: Parameters) -> list:
     """The changes the reference's validate_parameters would apply silently to `params`
     (mt_input_report), one string each; host only."""

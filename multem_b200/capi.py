@@ -104,6 +104,12 @@ SIGNATURES = {
     "mt_input_report": (c_int, [C.POINTER(MtInputMultislice), C.c_char_p, C.c_size_t, P_int]),
     "mt_multislice_run_batch": (c_int, [C.POINTER(MtSystemConf), c_int, C.POINTER(MtInputMultislice),
                                         C.POINTER(MtOutputMultislice), P_int]),
+    "mt_mat_input_open": (c_int, [C.c_char_p, C.c_char_p, C.POINTER(_VP), C.POINTER(MtSystemConf),
+                                  C.POINTER(MtInputMultislice)]),
+    "mt_mat_input_close": (c_int, [_VP]),
+    "mt_mat_output_write": (c_int, [C.c_char_p, C.c_char_p, C.POINTER(MtInputMultislice),
+                                    C.POINTER(MtOutputMultislice), c_int]),
+    "mt_multislice_run_mat": (c_int, [C.c_char_p, C.c_char_p, C.c_char_p, c_int]),
     "mt_engine_create": (c_int, [C.POINTER(MtSystemConf), C.POINTER(MtInputMultislice), C.POINTER(_VP)]),
     "mt_engine_run": (c_int, [_VP, C.POINTER(MtOutputMultislice)]),
     "mt_engine_run_confs": (c_int, [_VP, c_int, c_int]),

@@ -14,10 +14,15 @@
 #include "common.hpp"
 #include "devmem.hpp"
 #include "engine.hpp"
+#include "matio.hpp"
 #include "multem_b200.h"
 
 struct mt_engine {
     std::unique_ptr<mtb::Engine> eng;
+};
+
+struct mt_mat_input {
+    std::unique_ptr<mtb::matio::Input> h;
 };
 
 namespace {
@@ -214,6 +219,59 @@ mt_status mt_multislice_run(const mt_system_conf* conf, const mt_input_multislic
         mtb::Engine e(&c, in);
         e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
         e.write_output(out);
+    });
+}
+
+mt_status mt_mat_input_open(const char* path, const char* var, mt_mat_input** handle, mt_system_conf* conf,
+                            mt_input_multislice* in) {
+    return guarded([&] {
+        if (!path || !handle || !in) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        *handle = nullptr;
+        auto h = std::make_unique<mt_mat_input>();
+        h->h = mtb::matio::read_input(path, var ? var : "");
+        *in = h->h->in;
+        if (conf) *conf = h->h->conf;
+        *handle = h.release();
+    });
+}
+
+mt_status mt_mat_input_close(mt_mat_input* handle) {
+    delete handle;
+    return MT_OK;
+}
+
+mt_status mt_mat_output_write(const char* path, const char* var, const mt_input_multislice* in,
+                              const mt_output_multislice* out, int compress) {
+    return guarded([&] {
+        if (!path || !in || !out) mtb::fail(MT_ERR_INVALID_ARG, "NULL argument");
+        const mt_output_dims d = mtb::output_dims(mtb::build_model(in));
+        mtb::matio::write_output(path, var ? var : "", d, *out, compress != 0);
+    });
+}
+
+mt_status mt_multislice_run_mat(const char* in_path, const char* var, const char* out_path, int compress) {
+    return guarded([&] {
+        if (!in_path || !out_path) mtb::fail(MT_ERR_INVALID_ARG, "NULL path");
+        auto h = mtb::matio::read_input(in_path, var ? var : "");
+        const mt_input_multislice& in = h->in;
+        const mt_output_dims d = mtb::output_dims(mtb::build_model(&in));
+        const size_t nxy = (size_t)d.nx * d.ny;
+        std::vector<double> x(std::max(1, d.n_x)), y(std::max(1, d.n_y)), th(std::max(1, d.n_thick));
+        std::vector<double> itot, icoh, m2, psi, m2c;
+        mt_output_multislice out{};
+        out.x = x.data();
+        out.y = y.data();
+        out.thick = th.data();
+        auto sized = [](std::vector<double>& v, size_t n) { v.assign(std::max<size_t>(1, n), 0.0); return v.data(); };
+        if (d.has_image_tot) out.image_tot = sized(itot, (size_t)d.n_thick * d.n_detector * nxy);
+        if (d.has_image_coh) out.image_coh = sized(icoh, (size_t)d.n_thick * d.n_detector * nxy);
+        if (d.has_m2psi_tot) out.m2psi_tot = sized(m2, (size_t)d.n_thick * nxy);
+        if (d.has_psi_coh) out.psi_coh = sized(psi, 2 * (size_t)d.n_thick * nxy);
+        if (d.has_m2psi_coh) out.m2psi_coh = sized(m2c, (size_t)d.n_thick * nxy);
+        mtb::Engine e(&h->conf, &in);
+        e.run_confs(e.model().fp_iconf_0, e.model().pn_nconf);
+        e.write_output(&out);
+        mtb::matio::write_output(out_path, "", d, out, compress != 0);
     });
 }
 

@@ -184,3 +184,37 @@ class Parameters:
         fr = [np.asarray(m["fR"], dtype=np.float64).T.ravel() for m in mats]
         s.detector_fR, _ = darr(np.concatenate(fr) if fr else [0.0])
         return s, keep
+
+    def to_struct(self) -> dict:
+        """The MATLAB struct of these parameters as multem_input.parameters.toStruct builds it
+        (matlab_functions/+multem_input/parameters.m:283-303): flat fields, system_conf as a nested
+        struct, spec_amorp and detector.cir / detector.matrix as 1 x n struct arrays. Values are
+        numpy arrays in MATLAB's shapes (column vectors and matrices as MATLAB sees them), so
+        scipy.io.savemat writes a file that mt_mat_input_open (and MATLAB) reads."""
+        def sarr(rows, names):
+            a = np.empty((1, len(rows)), dtype=[(n, object) for n in names])
+            for i, r in enumerate(rows):
+                a[0, i] = tuple(np.atleast_2d(np.asarray(r[n], dtype=np.float64)) for n in names)
+            return a
+
+        d = {}
+        for k, v in vars(self).items():
+            if k in ("system_conf", "spec_amorp", "detector", "iw_psi"):
+                continue
+            d[k] = np.atleast_2d(np.asarray(v, dtype=np.float64))
+        d["spec_atoms"] = np.atleast_2d(np.asarray(self.spec_atoms, dtype=np.float64))
+        d["thick"] = np.atleast_2d(np.asarray(self.thick, dtype=np.float64))
+        c = self.system_conf
+        d["system_conf"] = {"precision": float(c.precision), "device": float(c.device),
+                            "cpu_nthread": float(c.cpu_nthread), "gpu_device": float(c.gpu_device)}
+        amorp = [a for a in self.spec_amorp if a is not None]
+        d["spec_amorp"] = sarr([{"z_0": a["z_0"], "z_e": a["z_e"], "dz": a.get("dz", 2.0)} for a in amorp],
+                               ["z_0", "z_e", "dz"])
+        if self.iw_psi is not None:
+            d["iw_psi"] = np.asarray(self.iw_psi, dtype=np.complex128)
+        det = self.detector or {"type": 1, "cir": []}
+        d["detector"] = {"type": float(det.get("type", 1)),
+                         "cir": sarr(det.get("cir", []), ["inner_ang", "outer_ang"]),
+                         "matrix": sarr([{"fR": m["fR"]} for m in det.get("matrix", [])], ["fR"])}
+        return d
+
