@@ -1369,11 +1369,13 @@ void Engine::coherent_image() {
     const size_t onxy = (size_t)(m_.out_ix_e - m_.out_ix_0) * (m_.out_iy_e - m_.out_iy_0);
     MTB_CUDA(cudaMemsetAsync(d_coh_m2_.p, 0, sizeof(double) * d_coh_m2_.n, stream_));
     const auto& TH = spec_->thicks();
-    std::vector<float2> tab((size_t)nx + ny);
+    // back-propagation factors of every thickness, uploaded once
+    const size_t pl = (size_t)nx + ny;
+    std::vector<float2> tab(pl * TH.size());
+    for (size_t t = 0; t < TH.size(); t++) prop_tables(TH[t].z_back_prop, &tab[t * pl], &tab[t * pl] + nx, true, 0);
     DevBuf<float2> d_bp;
+    d_bp.upload(tab.data(), tab.size(), stream_);
     for (size_t t = 0; t < TH.size(); t++) {
-        prop_tables(TH[t].z_back_prop, tab.data(), tab.data() + nx, true, 0);
-        d_bp.upload(tab.data(), tab.size(), stream_);
         for (size_t j = 0; j < m_.obj_c10.size(); j++) {
             ColArgs cj{};
             cj.ny = ny;
@@ -1382,8 +1384,8 @@ void Engine::coherent_image() {
             cj.n_det = 0;
             cj.in = d_coh_img_.p + t * nxy;
             cj.out = d_tmp_.p;
-            cj.Px = d_bp.p;
-            cj.Py = d_bp.p + nx;
+            cj.Px = d_bp.p + t * pl;
+            cj.Py = cj.Px + nx;
             cj.P2 = d_ctf_.p + j * nxy;
             cols(COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE, cj);
             RowArgs rb{};
@@ -1396,8 +1398,8 @@ void Engine::coherent_image() {
             launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e,
                                  (double)(float)m_.obj_w[j], 0, nullptr, d_coh_m2_.p + t * onxy, stream_);
         }
-        synchronize();  // the host table is rewritten for the next thickness
     }
+    synchronize();  // before the tables' device buffer is released
 }
 
 // Projected potential / transmission of one slice, reference stored layout.
