@@ -165,13 +165,14 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
     d_trans_.alloc((size_t)spec_->slices().size() * nxy);
     d_err_.alloc(1);
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
-    // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns; MTB_SHAPE the alternative
-    // shapes, same bits), else the autotuner picks them and the probes per launch
+    // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns: bulk-copy fed) and
+    // MTB_SHAPE the pipeline shapes of the slice step (bits 0-1 rows, bits 2-3 columns: 0 default,
+    // 1 or 2 alternatives), else the autotuner picks them and the probes per launch
     pipe_ = env_int("MTB_PIPE", -1);
     graphs_ = env_int("MTB_GRAPH", 1) != 0;
     tune_ = pipe_ < 0;
     if (tune_) pipe_ = 3;
-    shape_ = tune_ ? 0 : env_int("MTB_SHAPE", 0) & 3;
+    shape_ = tune_ ? 0 : env_int("MTB_SHAPE", 0) & 15;
     run_batch_ = batch_;
     if (m_.is_wave_sim() && m_.is_user_wave()) build_user_wave();
     reset();
@@ -657,7 +658,7 @@ void Engine::rows(RowMode mode, const RowArgs& a) {
     RowArgs b = a;
     b.err = (pipe_ & 1) ? d_err_.p : nullptr;
     b.wait_ns = wait_ns_;
-    b.shape = shape_ & 1;
+    b.shape = shape_ & 3;
     tl_begin(0);
     launch_rows(m_.grid.ny, mode, b, 0, stream_);
     tl_end();
@@ -667,7 +668,7 @@ void Engine::cols(int flags, const ColArgs& a) {
     ColArgs b = a;
     b.err = (pipe_ & 2) ? d_err_.p : nullptr;
     b.wait_ns = wait_ns_;
-    b.shape = (shape_ >> 1) & 1;
+    b.shape = (shape_ >> 2) & 3;
     tl_begin(1);
     launch_cols(m_.grid.nx, flags, b, 0, stream_);
     tl_end();
@@ -842,8 +843,9 @@ void Engine::run_conf(ConfData& cd) {
 // Autotuner of the line passes. For each (nx, ny, allocated probes per launch) the process times,
 // once, on this engine's probe buffer, transmission function and propagator (one warm-up and three
 // timed launches each): the row pass and the column pass of the slice step in each variant (per-
-// thread loads; bulk-copy fed; bulk-copy fed in the alternative pipeline shape, RowPipeShape<N, 1>
-// and ColPipeShape<N, 1>), keeping the fastest of each; then, for STEM batches of at least 16
+// thread loads; bulk-copy fed; bulk-copy fed in the alternative pipeline shapes RowPipeShape<N, 1|2>
+// and ColPipeShape<N, 1|2>: narrower groups, and early issue with full exchange buffers in as many
+// groups as shared memory holds), keeping the fastest of each; then, for STEM batches of at least 16
 // probes, the chosen step at the full and at half the batch, keeping the batch with the lower
 // time per probe. Every variant computes the same transforms with the same rounding, so the
 // choice changes only the speed (the FP64 detector partials of other tile widths are added in
@@ -890,30 +892,32 @@ Engine::Tuning Engine::tune_passes(int nprobe, ConfData& cd) {
     ca.det_w = col_det_width(nx);
     ca.wait_ns = wait_ns_;
     const int step = COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE;
-    // variant v: 0 per-thread loads, 1 bulk-copy fed, 2 bulk-copy fed in the alternative shape
+    // variant v: 0 per-thread loads, 1 bulk-copy fed, 2 and 3 bulk-copy fed in the alternative
+    // pipeline shapes 1 and 2 (a shape that does not fit this length runs the default one)
     auto rows_t = [&](int v, int nb) {
         ra.nprobe = nb;
         ra.err = v ? d_err_.p : nullptr;
-        ra.shape = v == 2;
+        ra.shape = v > 1 ? v - 1 : 0;
         return time_of([&] { launch_rows(ny, ROW_STEP, ra, 0, stream_); });
     };
     auto cols_t = [&](int v, int nb) {
         ca.nprobe = nb;
         ca.err = v ? d_err_.p : nullptr;
-        ca.shape = v == 2;
+        ca.shape = v > 1 ? v - 1 : 0;
         return time_of([&] { launch_cols(nx, step, ca, 0, stream_); });
     };
-    float tr[3], tc[3];
-    for (int v = 0; v < 3; v++) {
+    constexpr int NV = 4;
+    float tr[NV], tc[NV];
+    for (int v = 0; v < NV; v++) {
         tr[v] = rows_t(v, nprobe);
         tc[v] = cols_t(v, nprobe);
     }
     int vr = 0, vc = 0;
-    for (int v = 1; v < 3; v++) {
+    for (int v = 1; v < NV; v++) {
         if (tr[v] < tr[vr]) vr = v;
         if (tc[v] < tc[vc]) vc = v;
     }
-    Tuning t{(vr ? 1 : 0) | (vc ? 2 : 0), (vr == 2 ? 1 : 0) | (vc == 2 ? 2 : 0), nprobe};
+    Tuning t{(vr ? 1 : 0) | (vc ? 2 : 0), (vr > 1 ? vr - 1 : 0) | ((vc > 1 ? vc - 1 : 0) << 2), nprobe};
     if (m_.is_scanning() && nprobe >= 16 && (nprobe / 2) % 8 == 0) {
         const float full = tr[vr] + tc[vc];
         const float half = rows_t(vr, nprobe / 2) + cols_t(vc, nprobe / 2);
@@ -935,8 +939,8 @@ void Engine::tune(ConfData& cd) {
 }
 
 void Engine::tuning(int* rows_variant, int* cols_variant, int* probes_per_launch) const {
-    *rows_variant = (pipe_ & 1) ? 1 + (shape_ & 1) : 0;
-    *cols_variant = (pipe_ & 2) ? 1 + ((shape_ >> 1) & 1) : 0;
+    *rows_variant = (pipe_ & 1) ? 1 + (shape_ & 3) : 0;
+    *cols_variant = (pipe_ & 2) ? 1 + ((shape_ >> 2) & 3) : 0;
     *probes_per_launch = run_batch_;
 }
 

@@ -120,7 +120,7 @@ class Engine {
     void set_wait_limit(long long ns) { wait_ns_ = ns < 0 ? 0 : ns; }
     int pass_variants() const { return pipe_; }
     // The autotuner's choice: row and column pass variant (0 per-thread loads, 1 bulk-copy fed,
-    // 2 bulk-copy fed in the alternative shape) and probes per launch.
+    // 2 and 3 bulk-copy fed in the alternative pipeline shapes 1 and 2) and probes per launch.
     void tuning(int* rows_variant, int* cols_variant, int* probes_per_launch) const;
     void timing(double* total_ms, double* rows_ms, long long* n_rows, double* cols_ms, long long* n_cols);
 
@@ -163,7 +163,7 @@ class Engine {
     int pipe_ = 3;                   // bulk-copy-fed line passes where they fit (bit 0 rows, bit 1 cols)
     long long wait_ns_ = 2000000000ll;  // bound of the line passes' waits for their copies
     bool tune_ = true;               // choose pipe_, shape_, run_batch_ per shape with tune (MTB_PIPE unset)
-    int shape_ = 0;                  // alternative pipeline shape of the step passes (bit 0 rows, bit 1 cols)
+    int shape_ = 0;                  // pipeline shapes of the step passes (bits 0-1 rows, bits 2-3 cols)
     int run_batch_ = 1;              // probes per launch (<= batch_, the allocated batch)
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;

@@ -49,7 +49,7 @@ struct RowArgs {
     float scale;
     int* err;              // device flag, set when a bounded wait inside the pass gives up
     long long wait_ns;     // bound of each wait for a bulk copy (0: a copy not landed at the first check times out)
-    int shape;             // pipeline shape of the bulk-copy-fed step pass (0 default, 1 alternative)
+    int shape;             // pipeline shape of the bulk-copy-fed step pass (0 default, 1 or 2 alternatives)
 };
 void launch_rows(int ny, RowMode mode, const RowArgs& a, int grid_ctas, cudaStream_t s);
 
@@ -97,7 +97,7 @@ struct ColArgs {
     int det_w;                 // columns per detector partial (col_det_width)
     int* err;                  // device flag, set when a bounded wait inside the pass gives up
     long long wait_ns;         // bound of each wait for a bulk copy (0: a copy not landed at the first check times out)
-    int shape;                 // pipeline shape of the bulk-copy-fed step pass (0 default, 1 alternative)
+    int shape;                 // pipeline shape of the bulk-copy-fed step pass (0 default, 1 or 2 alternatives)
 };
 void launch_cols(int nx, int flags, const ColArgs& a, int grid_ctas, cudaStream_t s);
 int col_det_width(int nx);      // columns per detector partial

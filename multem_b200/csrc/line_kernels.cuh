@@ -391,29 +391,33 @@ constexpr size_t kPipeSmemMax = 232448 - 2048;  // opt-in shared memory per CTA 
 // line group g, and its LPC = GT/TPL transmission rows stay in shared memory (one bulk copy per
 // change of g, after every group has finished with the previous rows). Group x transforms the
 // items k = x, x+NG, ... from its own landing slot (mbarrier full[x], the group's j-th item being
-// its phase j). With EARLY, the group issues the copy of its next item as soon as it has read
-// the slot, and exchanges through its own half-line buffer (stage_exchange_half); otherwise the
-// slot, sized for the full exchange buffer, serves as the exchange buffer and the next copy is
-// issued once the forward transform's exchange has been read back.
-template <int NY, int GT, int NG, bool EARLY>
+// its phase j). The pipeline mode PM says where the exchanges go and when the next copy is issued:
+//   PM 1: the group issues the copy of its next item as soon as it has read the slot, and exchanges
+//         through its own half-line buffer (stage_exchange_half; plans with a half-line exchange);
+//   PM 2: early issue as in PM 1, exchanges through its own full line buffer;
+//   PM 0: the slot, sized for the full exchange buffer, serves as the exchange buffer and the next
+//         copy is issued once the forward transform's exchange has been read back.
+template <int NY, int GT, int NG, int PM>
 struct RowPipe {
     using G = LineGeom<NY>;
     static constexpr int TPL = G::TPL;
     static constexpr int LPC = GT / TPL;
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
     static constexpr size_t LAND = (size_t)LPC * NY;
-    static constexpr size_t SLOT = EARLY ? LAND : ((size_t)LPC * G::LS > LAND ? (size_t)LPC * G::LS : LAND);
-    static constexpr size_t HBUF = EARLY ? (size_t)LPC * HalfLineSmem<NY>::value : 0;
+    static constexpr size_t SLOT = PM != 0 ? LAND : ((size_t)LPC * G::LS > LAND ? (size_t)LPC * G::LS : LAND);
+    static constexpr size_t LBUF = PM == 1 ? (size_t)HalfLineSmem<NY>::value : (size_t)G::LS;  // per line
+    static constexpr size_t HBUF = PM != 0 ? (size_t)LPC * LBUF : 0;
     static constexpr size_t SMEM = sizeof(float2) * (TW + LAND + NG * SLOT + NG * HBUF);
     static constexpr bool OK = (GT % TPL == 0) && (GT % 32 == 0) && (SLOT % 2 == 0) && (HBUF % 2 == 0) &&
                                SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14) &&
-                               (!EARLY || (HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK));
+                               (PM != 1 || (HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK));
 };
 
-template <int NY, int MODE, int GT, int NG, bool EARLY>
+template <int NY, int MODE, int GT, int NG, int PM>
 __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     using G = LineGeom<NY>;
-    using P = RowPipe<NY, GT, NG, EARLY>;
+    using P = RowPipe<NY, GT, NG, PM>;
+    constexpr bool EARLY = PM != 0, HALF = PM == 1;
     constexpr int E = G::E, TPL = G::TPL, LPC = P::LPC;
     static_assert(MODE == ROW_STEP || MODE == ROW_INVERSE || MODE == ROW_FIRST_REAL, "mode without a load");
     constexpr bool TRANS = MODE != ROW_INVERSE;
@@ -430,8 +434,7 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
     const int li = gtid / TPL, t = gtid % TPL;
     float2* slot = slots + grp * P::SLOT;
-    float2* buf = EARLY ? slots + NG * P::SLOT + grp * P::HBUF + (size_t)li * HalfLineSmem<NY>::value
-                        : slot + (size_t)li * G::LS;
+    float2* buf = EARLY ? slots + NG * P::SLOT + grp * P::HBUF + (size_t)li * P::LBUF : slot + (size_t)li * G::LS;
     if (threadIdx.x == 0) {
         s_skip = err_set(a.err);  // an earlier pass timed out: the CTA returns (one decision for all)
         for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
@@ -521,7 +524,7 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
             if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
         }
         if constexpr (MODE == ROW_STEP || MODE == ROW_INVERSE) {
-            if constexpr (EARLY) line_fft_half<NY, false, +1>(x, buf, twI, t, Sync{grp});
+            if constexpr (HALF) line_fft_half<NY, false, +1>(x, buf, twI, t, Sync{grp});
             else line_fft<NY, false, +1>(x, buf, twI, t, Sync{grp});
         }
         if constexpr (MODE == ROW_INVERSE) {
@@ -536,12 +539,14 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
             const float2* Tr = s_trans + (size_t)li * NY;
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], Tr[reg_pos<NY, G::RL>(i, t)]);
-            if constexpr (EARLY) {
+            if constexpr (HALF) {
                 line_fft_half<NY, true, -1>(x, buf, twF, t, Sync{grp});
             } else {
                 line_fft<NY, true, -1>(x, buf, twF, t, Sync{grp});
-                gsync();  // every exchange read of the slot is done
-                if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
+                if constexpr (!EARLY) {
+                    gsync();  // every exchange read of the slot is done
+                    if (gtid < 32 && k + NG < K) issue(k + NG, gtid);
+                }
             }
 #pragma unroll
             for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::R1>(i, t)] = x[i];
@@ -552,14 +557,20 @@ __global__ void __launch_bounds__(GT * NG, 1) rows_pipe_kernel(RowArgs a) {
     if (threadIdx.x == 0 && last_tph >= 0) mbar_drain(&tbar, (unsigned)last_tph);
 }
 
-// Row-pass pipeline shapes per line length: threads per group, groups, early issue (where the
-// plan has a half-line exchange). Shape 0 is the default of every row pass; shape 1, one warp per
-// group (so a group synchronises with __syncwarp only) and 16 groups, is the alternative the
-// autotuner may pick for the slice step.
+// Row-pass pipeline shapes per line length: threads per group, groups, pipeline mode. Shape 0 is
+// the default of every row pass (early issue with the half-line exchange where the plan has one,
+// else late issue); shape 1, one warp per group (so a group synchronises with __syncwarp only) and
+// 16 groups, and shape 2, early issue with full exchange buffers in as many groups (8, 4 or 2) as
+// shared memory holds, are the alternatives the autotuner may pick for the slice step.
 template <int NY, int V = 0>
 struct RowPipeShape {
     static constexpr int GT = V == 0 ? 64 : 32, NG = V == 0 ? 8 : 16;
-    static constexpr bool EARLY = HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK;
+    static constexpr int PM = (HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK) ? 1 : 0;
+};
+template <int NY>
+struct RowPipeShape<NY, 2> {
+    static constexpr int GT = 64, PM = 2;
+    static constexpr int NG = RowPipe<NY, 64, 8, 2>::OK ? 8 : RowPipe<NY, 64, 4, 2>::OK ? 4 : 2;
 };
 
 // Column pass, bulk-copy fed: NG groups of GT threads, W = GT/TPL columns per tile. The tensor
@@ -567,17 +578,20 @@ struct RowPipeShape {
 // of 2W x BOXR x 1: one box is BOXR rows of a W-column tile, landing as [row][W]. Group x
 // transforms the items k = x, x+NG, ... of the CTA (item = blockIdx.x + k*gridDim.x) from its
 // own landing buffer, issues the copy of its next item as soon as it has read the buffer, and
-// exchanges through its own half-line buffers.
-// EARLY: the next tile is issued as soon as the group has read its slot, the exchanges use a separate
-// half-line buffer (HalfExchange). Otherwise (lengths without a half-line exchange, 1024) the slot
-// doubles as the full exchange buffer and the next tile is issued once the group's last exchange
-// read is done; the other groups keep the copy engine busy meanwhile.
-template <int NX, int GT, int NG, bool EARLY = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)>
+// exchanges through its own buffers. Pipeline mode PM:
+//   PM 1: the next tile is issued as soon as the group has read its slot, the exchanges use a
+//         separate half-line buffer (HalfExchange);
+//   PM 2: early issue as in PM 1, the exchanges use a separate full line buffer per column;
+//   PM 0: (lengths without a half-line exchange, 1024) the slot doubles as the full exchange
+//         buffer and the next tile is issued once the group's last exchange read is done; the other
+//         groups keep the copy engine busy meanwhile.
+template <int NX, int GT, int NG, int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0>
 struct ColPipe {
     using G = LineGeom<NX>;
-    static constexpr bool EARLY_V = EARLY;
+    static constexpr int PM_V = PM;
+    static constexpr bool EARLY = PM != 0;
     static constexpr int W = GT / G::TPL;
-    static constexpr int LSH = HalfLineSmem<NX>::value;
+    static constexpr int LSH = PM == 1 ? HalfLineSmem<NX>::value : G::LS;  // exchange buffer per column
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
     static constexpr size_t LAND0 = (size_t)W * NX;
     static constexpr size_t LAND1 = EARLY ? LAND0 : ((size_t)W * G::LS > LAND0 ? (size_t)W * G::LS : LAND0);
@@ -587,23 +601,32 @@ struct ColPipe {
     // rows per bulk-copy box: the boxes must tile the NX rows exactly (a box reaching past NX would
     // write past the slot and count bytes the barrier does not expect)
     static constexpr int BOXR = (NX <= 256) ? NX : (NX % 256 == 0) ? 256 : (NX % 128 == 0) ? 128 : 0;
-    static constexpr bool OK = (!EARLY || (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)) &&
+    static constexpr bool OK = (PM != 1 || (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)) &&
                                (BOXR > 0) && (NX % (BOXR > 0 ? BOXR : 1) == 0) && ((size_t)NX * W <= LAND) &&
                                (GT % G::TPL == 0) && (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) &&
                                (HBUF % 2 == 0) && SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
 };
 
-// Column-pass pipeline shapes: 2 groups of 256 threads (default), or 4 groups of 128 threads
-// (narrower tiles), the alternative the autotuner may pick for the slice step.
+// Column-pass pipeline shapes: 2 groups of 256 threads (default), and the alternatives the
+// autotuner may pick for the slice step: 4 groups of 128 threads (narrower tiles), and groups of
+// 128 threads in early-issue mode with full exchange buffers, as many (4, 3 or 2) as shared memory
+// holds.
 template <int NX, int V = 0>
 struct ColPipeShape {
     static constexpr int GT = V == 0 ? 256 : 128, NG = V == 0 ? 2 : 4;
+    static constexpr int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0;
+};
+template <int NX>
+struct ColPipeShape<NX, 2> {
+    static constexpr int GT = 128, PM = 2;
+    static constexpr int NG = ColPipe<NX, 128, 4, 2>::OK ? 4 : ColPipe<NX, 128, 3, 2>::OK ? 3 : 2;
 };
 
-template <int NX, int FLAGS, int LDY, int GT, int NG, bool EARLY>
+template <int NX, int FLAGS, int LDY, int GT, int NG, int PM>
 __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const __grid_constant__ CUtensorMap map) {
     using G = LineGeom<NX>;
-    using P = ColPipe<NX, GT, NG, EARLY>;
+    using P = ColPipe<NX, GT, NG, PM>;
+    constexpr bool EARLY = PM != 0, HALF = PM == 1;
     constexpr int E = G::E, W = P::W, NWARP = GT / 32;
     constexpr bool PROP = FLAGS & COL_PROP, DET = FLAGS & COL_DETECT;
     constexpr bool INV = FLAGS & COL_INVERSE, STORE = FLAGS & COL_STORE;
@@ -624,6 +647,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     const int c = gtid % W, t = gtid / W;
     float2* land = land0 + grp * P::LAND;
     float2* buf = EARLY ? land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH : land + (size_t)c * G::LS;
+    (void)HALF;
     if constexpr (PROP) {
         for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
     }
@@ -671,10 +695,9 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
         gsync();  // the whole group has read its landing buffer
         if constexpr (EARLY) {
             if (gtid == 0 && k + NG < K) issue(k + NG);
-            line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
-        } else {
-            line_fft<NX, false, -1>(x, buf, twP, t, gsync);
         }
+        if constexpr (HALF) line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
+        else line_fft<NX, false, -1>(x, buf, twP, t, gsync);
         if constexpr (PROP) {
             const float2 py = a.Py[iy];
 #pragma unroll
@@ -707,12 +730,14 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             gsync();
         }
         if constexpr (INV) {
-            if constexpr (EARLY) {
+            if constexpr (HALF) {
                 line_fft_half<NX, true, +1>(x, buf, twR, t, gsync);
             } else {
                 line_fft<NX, true, +1>(x, buf, twR, t, gsync);
-                gsync();  // every exchange read of the slot is done
-                if (gtid == 0 && k + NG < K) issue(k + NG);
+                if constexpr (!EARLY) {
+                    gsync();  // every exchange read of the slot is done
+                    if (gtid == 0 && k + NG < K) issue(k + NG);
+                }
             }
 #pragma unroll
             for (int i = 0; i < E; i++) dst[(reg_pos<NX, G::R1>(i, t) - t) * ldy] = x[i];
@@ -753,44 +778,41 @@ static int max_ctas(K kernel, int threads, size_t smem) {
     return nsm * occ;
 }
 
+// Launches the bulk-copy-fed row pass in pipeline shape V when that shape fits this line length and
+// the probe count; returns false otherwise.
+template <int NY, int MODE, int V>
+static bool rows_pipe_try(const RowArgs& a, int grid_ctas, cudaStream_t s) {
+    using S = RowPipeShape<NY, V>;
+    using RP = RowPipe<NY, S::GT, S::NG, S::PM>;
+    if constexpr (RP::OK && MODE != ROW_FIRST_ONE) {
+        if (a.nprobe % S::NG != 0) return false;
+        auto kern = rows_pipe_kernel<NY, MODE, S::GT, S::NG, S::PM>;
+        static const int cap = max_ctas(kern, S::GT * S::NG, RP::SMEM);
+        const int units = (a.nx / RP::LPC) * a.nprobe / S::NG;
+        int grid = grid_ctas > 0 ? grid_ctas : cap;
+        if (grid > units) grid = units;
+        kern<<<grid, S::GT * S::NG, RP::SMEM, s>>>(a);
+        note_launch();
+        MTB_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        (void)a, (void)grid_ctas, (void)s;
+        return false;
+    }
+}
+
 // The bulk-copy-fed kernels run where their shared memory fits and the pass loads its input;
 // they need the error flag of their bounded waits (a.err), and without it the per-thread-load
-// kernels run.
+// kernels run. The slice step may use an alternative pipeline shape (a.shape 1 or 2).
 template <int NY, int MODE>
 static void rows_launch(const RowArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NY>;
-    using S = RowPipeShape<NY>;
-    using RP = RowPipe<NY, S::GT, S::NG, S::EARLY>;
-    if constexpr (MODE == ROW_STEP) {
-        using S1 = RowPipeShape<NY, 1>;
-        using RP1 = RowPipe<NY, S1::GT, S1::NG, S1::EARLY>;
-        if constexpr (RP1::OK) {
-            if (a.err && a.shape == 1 && a.nprobe % S1::NG == 0) {
-                auto kern = rows_pipe_kernel<NY, MODE, S1::GT, S1::NG, S1::EARLY>;
-                static const int cap = max_ctas(kern, S1::GT * S1::NG, RP1::SMEM);
-                const int units = (a.nx / RP1::LPC) * a.nprobe / S1::NG;
-                int grid = grid_ctas > 0 ? grid_ctas : cap;
-                if (grid > units) grid = units;
-                kern<<<grid, S1::GT * S1::NG, RP1::SMEM, s>>>(a);
-                note_launch();
-                MTB_CUDA(cudaGetLastError());
-                return;
-            }
+    if (a.err) {
+        if constexpr (MODE == ROW_STEP) {
+            if (a.shape == 1 && rows_pipe_try<NY, MODE, 1>(a, grid_ctas, s)) return;
+            if (a.shape == 2 && rows_pipe_try<NY, MODE, 2>(a, grid_ctas, s)) return;
         }
-    }
-    if constexpr (RP::OK && MODE != ROW_FIRST_ONE) {
-        if (a.err && a.nprobe % S::NG == 0) {
-            constexpr size_t sm = RP::SMEM;
-            auto kern = rows_pipe_kernel<NY, MODE, S::GT, S::NG, S::EARLY>;
-            static const int cap = max_ctas(kern, S::GT * S::NG, sm);
-            const int units = (a.nx / RP::LPC) * a.nprobe / S::NG;
-            int grid = grid_ctas > 0 ? grid_ctas : cap;
-            if (grid > units) grid = units;
-            kern<<<grid, S::GT * S::NG, sm, s>>>(a);
-            note_launch();
-            MTB_CUDA(cudaGetLastError());
-            return;
-        }
+        if (rows_pipe_try<NY, MODE, 0>(a, grid_ctas, s)) return;
     }
     const size_t sm = rows_smem<NY>();
     static const int cap = max_ctas(rows_kernel<NY, MODE>, G::THREADS, sm);
@@ -812,45 +834,39 @@ void rows_dispatch_mode(RowMode mode, const RowArgs& a, int grid_ctas, cudaStrea
     }
 }
 
+// Launches the bulk-copy-fed column pass in pipeline shape V when that shape fits this line length;
+// returns false otherwise.
+template <int NX, int FLAGS, int LDY, int V>
+static bool cols_pipe_try(const ColArgs& a, int grid_ctas, cudaStream_t s) {
+    using S = ColPipeShape<NX, V>;
+    using CP = ColPipe<NX, S::GT, S::NG, S::PM>;
+    if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
+        auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG, S::PM>;
+        static const int cap = max_ctas(kern, S::GT * S::NG, CP::SMEM);
+        const int items = (a.ny / CP::W) * a.nprobe;
+        int grid = grid_ctas > 0 ? grid_ctas : cap;
+        if (grid > items) grid = items;
+        CUtensorMap map;
+        encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP::W, CP::BOXR);
+        kern<<<grid, S::GT * S::NG, CP::SMEM, s>>>(a, map);
+        note_launch();
+        MTB_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        (void)a, (void)grid_ctas, (void)s;
+        return false;
+    }
+}
+
 template <int NX, int FLAGS, int LDY>
 static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
     using G = LineGeom<NX>;
-    using S = ColPipeShape<NX>;
-    using CP = ColPipe<NX, S::GT, S::NG>;
-    if constexpr (FLAGS == (COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE)) {
-        using S1 = ColPipeShape<NX, 1>;
-        using CP1 = ColPipe<NX, S1::GT, S1::NG>;
-        if constexpr (CP1::OK) {
-            if (a.err && a.shape == 1) {
-                auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S1::GT, S1::NG, CP1::EARLY_V>;
-                static const int cap = max_ctas(kern, S1::GT * S1::NG, CP1::SMEM);
-                const int items = (a.ny / CP1::W) * a.nprobe;
-                int grid = grid_ctas > 0 ? grid_ctas : cap;
-                if (grid > items) grid = items;
-                CUtensorMap map;
-                encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP1::W, CP1::BOXR);
-                kern<<<grid, S1::GT * S1::NG, CP1::SMEM, s>>>(a, map);
-                note_launch();
-                MTB_CUDA(cudaGetLastError());
-                return;
-            }
+    if (a.err) {
+        if constexpr (FLAGS == (COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE)) {
+            if (a.shape == 1 && cols_pipe_try<NX, FLAGS, LDY, 1>(a, grid_ctas, s)) return;
+            if (a.shape == 2 && cols_pipe_try<NX, FLAGS, LDY, 2>(a, grid_ctas, s)) return;
         }
-    }
-    if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
-        if (a.err) {
-            constexpr size_t sm = CP::SMEM;
-            auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG, CP::EARLY_V>;
-            static const int cap = max_ctas(kern, S::GT * S::NG, sm);
-            const int items = (a.ny / CP::W) * a.nprobe;
-            int grid = grid_ctas > 0 ? grid_ctas : cap;
-            if (grid > items) grid = items;
-            CUtensorMap map;
-            encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP::W, CP::BOXR);
-            kern<<<grid, S::GT * S::NG, sm, s>>>(a, map);
-            note_launch();
-            MTB_CUDA(cudaGetLastError());
-            return;
-        }
+        if (cols_pipe_try<NX, FLAGS, LDY, 0>(a, grid_ctas, s)) return;
     }
     const size_t sm = cols_smem<NX, FLAGS>();
     static const int cap = max_ctas(cols_kernel<NX, FLAGS, LDY>, G::THREADS, sm);
@@ -880,7 +896,8 @@ template <int NX>
 int cols_det_width() {
     constexpr int wc = LineGeom<NX>::LPC;
     using S = ColPipeShape<NX>;
-    constexpr int wp = ColPipe<NX, S::GT, S::NG>::OK ? ColPipe<NX, S::GT, S::NG>::W : wc;
+    using CP = ColPipe<NX, S::GT, S::NG, S::PM>;
+    constexpr int wp = CP::OK ? CP::W : wc;
     return wp < wc ? wp : wc;
 }
 
