@@ -231,7 +231,7 @@ class Net:
 # data from the engine
 
 def haadf_specimen(i: int, seed: int = 11, ns: int = 32, scan_cells: int = 2, nconf: int = 64,
-                   t_nm=(4.0, 24.0), tilt_deg: float = 2.0):
+                   t_nm=(4.0, 40.0), tilt_deg: float = 2.0):
     """Seeded random fcc(001) Au or Pt specimen: a ~ U[3.92, 4.08] A, thickness ~ U[t_nm] nm, beam
     tilt ~ U[0, tilt_deg] deg at a uniform azimuth; HAADF 70-200 mrad on a 512^2 grid (see
     specimens.haadf_fcc001) with an ns x ns raster over scan_cells x scan_cells unit cells."""
@@ -272,7 +272,7 @@ def error_estimate(pred, err):
     return float(np.sqrt(np.mean(err ** 2)) / np.sqrt(np.mean(pred ** 2)))
 
 
-TIERS = (4, 16, 64)  # configurations run before each gate; the last tier is the plain result
+TIERS = (4, 6, 8, 16, 64)  # configurations run before each gate; the last tier is the plain result
 
 
 def noise_level(n):
@@ -392,6 +392,12 @@ def generate(args):
     configuration took), saved to args.data after every specimen."""
     out = Path(args.data)
     rec = {"train": [], "test": [], "test_times": [], "test_meta": []}
+    if out.exists():  # resume a partial file: keep its specimens, generate the rest
+        z = np.load(out)
+        rec["train"] = list(z["train"])
+        rec["test"] = list(z["test"])
+        rec["test_times"] = list(z["test_times"])
+        rec["test_meta"] = json.loads(str(z["test_meta"]))
 
     def save():
         tmp = out.with_suffix(".tmp.npz")
@@ -402,11 +408,12 @@ def generate(args):
         tmp.replace(out)
 
     t0 = time.perf_counter()
-    for i in range(args.train + args.val):
+    for i in range(len(rec["train"]), args.train + args.val):
         rec["train"].append(per_configuration_images(haadf_specimen(i))[0])
         if i % 8 == 7:
             save()
-    for i in range(args.train + args.val, args.train + args.val + args.test):
+    save()
+    for i in range(args.train + args.val + len(rec["test"]), args.train + args.val + args.test):
         p = haadf_specimen(i, ns=args.test_ns, scan_cells=max(1, args.test_ns // 16))
         im, tc = per_configuration_images(p)
         rec["test"].append(im)
@@ -429,8 +436,8 @@ def noise_floor(im, n_small=4):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=80, help="training specimens")
-    ap.add_argument("--val", type=int, default=8, help="specimens for the gate calibration")
+    ap.add_argument("--train", type=int, default=96, help="training specimens")
+    ap.add_argument("--val", type=int, default=16, help="specimens for the gate calibration")
     ap.add_argument("--test", type=int, default=10, help="unseen evaluation specimens")
     ap.add_argument("--test-ns", type=int, default=64, help="evaluation raster (over test-ns/16 unit cells)")
     ap.add_argument("--data", default=None, help="per-configuration images: read if present, else generated here")
@@ -445,12 +452,16 @@ def main():
     import torch
 
     t_gen = None
-    if args.data is None or not Path(args.data).exists():
-        args.data = args.data or "surrogate_data.npz"
+    args.data = args.data or "surrogate_data.npz"
+    have = 0
+    if Path(args.data).exists():
+        z = np.load(args.data)
+        have = (z["train"].shape[0] >= args.train + args.val) and (z["test"].shape[0] >= args.test)
+    if not have:
         t_gen = generate(args)
-        if args.generate_only:
-            print(json.dumps({"data": args.data, "generation_s": round(t_gen, 1)}))
-            return
+    if args.generate_only:
+        print(json.dumps({"data": args.data, "generation_s": None if t_gen is None else round(t_gen, 1)}))
+        return
     z = np.load(args.data)
     imgs = z["train"]
     tests, test_times, test_meta = z["test"], z["test_times"], json.loads(str(z["test_meta"]))
@@ -497,7 +508,7 @@ def main():
     summary = {
         "metric": "STEM probe-slice updates/s at 512^2 FP32, learned path (4 or 16 configurations + surrogate, "
                   "64 on fallback) counted as the 64-configuration run it replaces",
-        "workload": f"{len(tests)} unseen fcc(001) Au/Pt specimens, 4-24 nm, tilt 0-2 deg, 512^2 grid, "
+        "workload": f"{len(tests)} unseen fcc(001) Au/Pt specimens, 4-40 nm, tilt 0-2 deg, 512^2 grid, "
                     f"{args.test_ns}x{args.test_ns} HAADF raster (70-200 mrad), 300 kV, 25 mrad, 64 phonons",
         "gate": args.gate, "calib": calib, "params": net.n_params(), "widths": list(net.widths),
         "train_specimens": int(P.shape[0]), "train_steps": args.steps, "batch": args.batch,

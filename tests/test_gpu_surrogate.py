@@ -195,7 +195,7 @@ def test_training_reduces_the_loss():
 
 def test_trained_surrogate_gains_over_the_plain_few_configuration_image():
     """What the committed network gains over the method without it, on a specimen outside its
-    training, calibration and evaluation sets (fcc Au(001), 11 nm, beam tilted 1.7 deg, 32 x 32
+    training, calibration and evaluation sets (fcc Au(001), 16 nm, beam tilted 1.7 deg, 32 x 32
     HAADF raster over 2 x 2 cells, 64 phonon configurations): its estimate from the first 4
     configurations is closer to the 64-configuration image than the plain 4-configuration mean,
     with and without the lattice fold, and so is the folded estimate from 16 configurations; an
