@@ -56,14 +56,16 @@ void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int 
 // of a slice and every pixel of its footprint box (get_bn, src/cpu_fcns.hpp:1670-1684),
 //   R2 = (ix*dRx + Rx_0 - x)^2 + (iy*dRy + Ry_0 - y)^2;  if R2 < R2_max:
 //   V[ind_col_pbc_shift(ix, iy)] += occ * cubic(R2)   (eval_cubic_poly, src/cgpu_fcns.cuh:1498-1567)
-// with an FP32 atomicAdd per contribution. Here one CTA owns a 16 x 32 tile of the stored
-// (shifted) grid of one slice, culls the slice's atoms against its tile, and sums the
-// contributions of the surviving atoms in atom order in registers (deterministic, no atomics).
+// with an FP32 atomicAdd per contribution. Here one CTA owns a 64 x 32 tile of the stored
+// (shifted) grid of one slice (8 pixels per thread, 8 rows apart), culls the slice's atoms against
+// its tile, and sums the contributions of the surviving atoms in atom order in registers
+// (deterministic, no atomics; the tile size changes no sum).
 // The epilogue writes T = exp(i*w*V) (functor::transmission_function, src/cgpu_fcns.cuh:3072-3086)
 // directly; V never goes to HBM unless asked for. Float products and sums use the _rn intrinsics
 // so they are not fused into FMAs and round like the reference's host float path.
 // =============================================================================================
-constexpr int SPLAT_TX = 16;   // tile extent along x (slow index)
+constexpr int SPLAT_TX = 64;   // tile extent along x (slow index)
+constexpr int SPLAT_PX = SPLAT_TX / 8;  // pixels per thread along x
 constexpr int SPLAT_TY = 32;   // tile extent along y (contiguous index)
 constexpr int SPLAT_THREADS = 256;
 constexpr int SPLAT_MAXT_SMEM = 8;
@@ -96,10 +98,11 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
     const int tx0 = blockIdx.y * SPLAT_TX;
     const int ty0 = blockIdx.x * SPLAT_TY;
     const int ly = threadIdx.x % SPLAT_TY;
-    const int lx = threadIdx.x / SPLAT_TY;  // 0..7
+    const int lx = threadIdx.x / SPLAT_TY;  // 0..7: this thread's pixels are tx0 + lx + 8p
     const int jy = ty0 + ly;
-    const int jx0 = tx0 + lx, jx1 = tx0 + lx + 8;
-    float V0 = 0.0f, V1 = 0.0f;
+    float V[SPLAT_PX];
+#pragma unroll
+    for (int p = 0; p < SPLAT_PX; p++) V[p] = 0.0f;
 
     const int2 rng = a.slice_range[islice];
     __syncthreads();
@@ -153,12 +156,17 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
             const float* T = tab + (size_t)af.type * 5 * nR;
             const float Rm = a.R_max[af.type];
             const float R2_max = __fmul_rn(Rm, Rm);
-            // y offsets are shared by both pixels of this thread
-            int offy = pmod(jy - af.sy, g.ny);
+            // knot index guess: the knots are log-spaced in R, so log2(R^2) is linear in the index
+            const float lg0 = __log2f(T[0]);
+            const float lgs = (float)(nR - 1) / (__log2f(T[nR - 1]) - lg0);
+            // y offset, shared by every pixel of this thread (jy and sy are both in [0, ny))
+            int offy = jy - af.sy;
+            if (offy < 0) offy += g.ny;
 #pragma unroll
-            for (int p = 0; p < 2; p++) {
-                const int jx = p == 0 ? jx0 : jx1;
-                int offx = pmod(jx - af.sx, g.nx);
+            for (int p = 0; p < SPLAT_PX; p++) {
+                const int jx = tx0 + lx + 8 * p;
+                int offx = jx - af.sx;
+                if (offx < 0) offx += g.nx;
                 for (int ox = offx; ox < af.nxa; ox += g.nx) {
                     const int ix = af.ix0 + ox;
                     const float Rx = __fsub_rn(__fadd_rn(__fmul_rn((float)ix, g.dRx), g.Rx_0), af.x);
@@ -167,20 +175,20 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
                         const float Ry = __fsub_rn(__fadd_rn(__fmul_rn((float)iy, g.dRy), g.Ry_0), af.y);
                         const float R2 = __fadd_rn(__fmul_rn(Rx, Rx), __fmul_rn(Ry, Ry));
                         if (R2 < R2_max) {
-                            // unrolledBinarySearch_c_nR (src/cgpu_fcns.cuh:1498-1518) over 128 knots
-                            int i0 = 0, ie = nR - 1;
-#pragma unroll
-                            for (int it = 0; it < 7; it++) {
-                                int im = (i0 + ie) >> 1;
-                                if (R2 < T[im]) ie = im; else i0 = im;
-                            }
+                            // the interval of unrolledBinarySearch_c_nR (src/cgpu_fcns.cuh:1498-1518):
+                            // the largest i0 in [0, nR-2] with T[i0] <= R2 (0 below the first knot),
+                            // from the logarithmic guess and exact comparisons with the knots
+                            int i0 = (int)fmaxf(__fmul_rn(__log2f(R2) - lg0, lgs), 0.0f);
+                            i0 = i0 < nR - 2 ? i0 : nR - 2;
+                            while (i0 > 0 && R2 < T[i0]) i0--;
+                            while (i0 < nR - 2 && !(R2 < T[i0 + 1])) i0++;
                             const float dx = __fsub_rn(R2, T[i0]);
                             const float c3 = T[4 * nR + i0], c2 = T[3 * nR + i0], c1 = T[2 * nR + i0], c0v = T[nR + i0];
                             float v = __fadd_rn(__fmul_rn(c3, dx), c2);
                             v = __fadd_rn(__fmul_rn(v, dx), c1);
                             v = __fadd_rn(__fmul_rn(v, dx), c0v);
                             v = __fmul_rn(af.occ, v);
-                            if (p == 0) V0 += v; else V1 += v;
+                            V[p] += v;
                         }
                     }
                 }
@@ -189,14 +197,13 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
         __syncthreads();
     }
     const size_t base = (size_t)islice * g.nx * g.ny;
-    const float Vs[2] = {V0, V1};
 #pragma unroll
-    for (int p = 0; p < 2; p++) {
-        const int jx = p == 0 ? jx0 : jx1;
+    for (int p = 0; p < SPLAT_PX; p++) {
+        const int jx = tx0 + lx + 8 * p;
         const size_t idx = base + (size_t)jx * g.ny + jy;
-        if (a.V) a.V[idx] = Vs[p];
+        if (a.V) a.V[idx] = V[p];
         if (a.trans) {
-            const float th = __fmul_rn(a.w, Vs[p]);
+            const float th = __fmul_rn(a.w, V[p]);
             float sn, cs;
             if (a.wpo) {
                 cs = 1.0f;
@@ -210,7 +217,7 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
 }
 
 void launch_splat(const SplatArgs& a, int islice_0, int n_slice, cudaStream_t s) {
-    if (a.g.nx % SPLAT_TX || a.g.ny % SPLAT_TY) fail(MT_ERR_UNSUPPORTED, "grid must be a multiple of 16 x 32");
+    if (a.g.nx % SPLAT_TX || a.g.ny % SPLAT_TY) fail(MT_ERR_UNSUPPORTED, "grid must be a multiple of 64 x 32");
     dim3 grid(a.g.ny / SPLAT_TY, a.g.nx / SPLAT_TX, n_slice);
     size_t sm = (a.n_types <= SPLAT_MAXT_SMEM) ? (size_t)a.n_types * 5 * a.nR * sizeof(float) : 0;
     splat_kernel<<<grid, SPLAT_THREADS, sm, s>>>(a, islice_0);

@@ -42,66 +42,97 @@ __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162f
 
 // A[m][k] = in[b][c][y+ky-1][x+kx-1] for k = c*9 + ky*3 + kx < 9*C (zero outside the image and for
 // the padding k in [9C, ldk)); with `mask`, zero where mask (same layout as in) is not positive.
-__global__ void im2col_kernel(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ mask,
-                              __nv_bfloat16* __restrict__ A, int B, int C, int H, int W, int ldk) {
-    const int HW = H * W;
-    const size_t n = (size_t)B * HW * ldk;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(e % ldk);
-        const int m = (int)(e / ldk);
+// One CTA of 32 x 8 threads per tile of 32 pixels x 64 k: the gather reads consecutive pixels with
+// consecutive threads, the tile is transposed through shared memory, and each pixel's 64 k values
+// leave as 16-byte stores. grid: (ceil(M/32), ceil(ldk/64)).
+__global__ void __launch_bounds__(256) im2col_kernel(const __nv_bfloat16* __restrict__ in,
+                                                     const __nv_bfloat16* __restrict__ mask,
+                                                     __nv_bfloat16* __restrict__ A, int B, int C, int H, int W,
+                                                     int ldk) {
+    __shared__ __nv_bfloat16 tile[64][34];
+    const int HW = H * W, M = B * HW, K = 9 * C;
+    const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int m = m0 + tx;
+    int b = 0, y = 0, x = 0;
+    if (m < M) {
+        b = m / HW;
+        const int yx = m - b * HW;
+        y = yx / W;
+        x = yx - y * W;
+    }
+    for (int kk = ty; kk < 64; kk += 8) {
+        const int k = k0 + kk;
         __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
-        if (k < 9 * C) {
-            const int c = k / 9, q = k % 9, b = m / HW, yx = m % HW;
-            const int yy = yx / W + q / 3 - 1, xx = yx % W + q % 3 - 1;
+        if (m < M && k < K) {
+            const int c = k / 9, q = k - 9 * c;
+            const int yy = y + q / 3 - 1, xx = x + q % 3 - 1;
             if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
                 const size_t idx = (((size_t)b * C + c) * H + yy) * W + xx;
                 v = in[idx];
                 if (mask && !(bf(mask[idx]) > 0.0f)) v = __float2bfloat16_rn(0.0f);
             }
         }
-        A[e] = v;
+        tile[kk][tx] = v;
+    }
+    __syncthreads();
+    const int t = ty * 32 + tx, r = t / 8, ch = t % 8;
+    const int mr = m0 + r, k = k0 + ch * 8;
+    if (mr < M && k < ldk) {  // ldk and k are multiples of 8: the 8 values stay inside the row
+        __align__(16) __nv_bfloat16 v8[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v8[j] = tile[ch * 8 + j][r];
+        *reinterpret_cast<uint4*>(A + (size_t)mr * ldk + k) = *reinterpret_cast<const uint4*>(v8);
     }
 }
 
-// X[k][p] = in[b][c][y+ky-1][x+kx-1] (the transposed im2col, p = (b, y, x)) for k < 9C, X[9C][p] = 1,
-// zero for the padding p in [B*H*W, ldp).
-__global__ void im2col_t_kernel(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ X, int B, int C,
-                                int H, int W, int ldp) {
+// X[k][p] = in[b][c][y+ky-1][x+kx-1] (the transposed im2col, p = (b, y, x)) for k = c*9 + q < 9C,
+// X[9C][p] = 1, zero for the padding p in [B*H*W, ldp). grid: (ceil(ldp/256), C + 1); the CTA row
+// c writes the nine rows of channel c (the last CTA row the row of ones), consecutive threads
+// consecutive pixels.
+__global__ void __launch_bounds__(256) im2col_t_kernel(const __nv_bfloat16* __restrict__ in,
+                                                       __nv_bfloat16* __restrict__ X, int B, int C, int H, int W,
+                                                       int ldp) {
     const int HW = H * W, P = B * HW;
-    const size_t n = (size_t)(9 * C + 1) * ldp;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int p = (int)(e % ldp);
-        const int k = (int)(e / ldp);
-        float v = 0.0f;
-        if (p < P) {
-            if (k == 9 * C) {
-                v = 1.0f;
-            } else {
-                const int c = k / 9, q = k % 9, b = p / HW, yx = p % HW;
-                const int yy = yx / W + q / 3 - 1, xx = yx % W + q % 3 - 1;
-                if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = bf(in[(((size_t)b * C + c) * H + yy) * W + xx]);
-            }
+    const int c = blockIdx.y;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ldp; p += gridDim.x * blockDim.x) {
+        if (c == C) {
+            X[(size_t)9 * C * ldp + p] = __float2bfloat16_rn(p < P ? 1.0f : 0.0f);
+            continue;
         }
-        X[e] = __float2bfloat16_rn(v);
+        int b = 0, y = 0, x = 0;
+        if (p < P) {
+            b = p / HW;
+            const int yx = p - b * HW;
+            y = yx / W;
+            x = yx - y * W;
+        }
+        const __nv_bfloat16* plane = in + ((size_t)b * C + c) * HW;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int yy = y + q / 3 - 1, xx = x + q % 3 - 1;
+            const float v = (p < P && yy >= 0 && yy < H && xx >= 0 && xx < W) ? bf(plane[yy * W + xx]) : 0.0f;
+            X[(size_t)(9 * c + q) * ldp + p] = __float2bfloat16_rn(v);
+        }
     }
 }
 
 // Y[c][p] = d[b][c][y][x] (channel-major, p = (b, y, x)), zero where mask is not positive and for
-// the padding p in [B*HW, ldp).
-__global__ void channel_major_kernel(const __nv_bfloat16* __restrict__ d, const __nv_bfloat16* __restrict__ mask,
-                                     __nv_bfloat16* __restrict__ Y, int B, int C, int HW, int ldp) {
-    const int P = B * HW;
-    const size_t n = (size_t)C * ldp;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int p = (int)(e % ldp);
-        const int c = (int)(e / ldp);
+// the padding p in [B*HW, ldp). grid: (ceil(ldp/256), C).
+__global__ void __launch_bounds__(256) channel_major_kernel(const __nv_bfloat16* __restrict__ d,
+                                                            const __nv_bfloat16* __restrict__ mask,
+                                                            __nv_bfloat16* __restrict__ Y, int B, int C, int HW,
+                                                            int ldp) {
+    const int P = B * HW, c = blockIdx.y;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ldp; p += gridDim.x * blockDim.x) {
         __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
         if (p < P) {
-            const size_t idx = ((size_t)(p / HW) * C + c) * HW + p % HW;
+            const int b = p / HW;
+            const size_t idx = ((size_t)b * C + c) * HW + (p - b * HW);
             v = d[idx];
             if (mask && !(bf(mask[idx]) > 0.0f)) v = __float2bfloat16_rn(0.0f);
         }
-        Y[e] = v;
+        Y[(size_t)c * ldp + p] = v;
     }
 }
 
@@ -120,15 +151,15 @@ __global__ void pack_weights_kernel(const __nv_bfloat16* __restrict__ w, __nv_bf
 }
 
 // out[(m / mdiv) * s_mq + (m % mdiv) * s_mr + n * s_n] = act(bias[n] + sum over splits s, in order,
-// of part[s][row0 + m][n]) for m < M, n < N; m runs fastest over the threads (coalesced stores for
-// the NCHW and [o][k] layouts).
+// of part[s][row0 + m][n]) for m < M, n < N; n runs fastest over the threads, so the reads of the
+// partial sums (splits times the output) are contiguous.
 __global__ void gemm_finalize_kernel(const float* __restrict__ part, int splits, int Mtot, int N, int row0, int M,
                                      const float* __restrict__ bias, int relu, __nv_bfloat16* __restrict__ out_bf,
                                      float* __restrict__ out_f, long long mdiv, long long s_mq, long long s_mr,
                                      long long s_n) {
     const size_t n_all = (size_t)M * N;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_all; e += (size_t)gridDim.x * blockDim.x) {
-        const int m = (int)(e % M), n = (int)(e / M);
+        const int n = (int)(e % N), m = (int)(e / N);
         float acc = 0.0f;
         for (int s = 0; s < splits; s++) acc += part[((size_t)s * Mtot + row0 + m) * N + n];
         float v = acc + (bias ? bias[n] : 0.0f);
@@ -311,8 +342,8 @@ void gemm_split(int M, int N, int K, int* splits, int* kb_per_split) {
 }
 
 template <int BN>
-void gemm_launch(const CUtensorMap& ma, const CUtensorMap& mb, float* part, int M, int N, int nkb, int splits,
-                 int kps, int* err, cudaStream_t st) {
+void gemm_launch(const CUtensorMap& ma, const CUtensorMap& mb, const mtb::umma::GemmOut& out, int M, int N, int nkb,
+                 int splits, int kps, int* err, cudaStream_t st) {
     using T = mtb::umma::Tile<BN>;
     auto kern = mtb::umma::gemm_kernel<BN>;
     MTB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
@@ -322,24 +353,26 @@ void gemm_launch(const CUtensorMap& ma, const CUtensorMap& mb, float* part, int 
     MTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, T::SMEM));
     if (occ < 1 || occ * T::TCOLS > 512) mtb::fail(MT_ERR_INTERNAL, "GEMM tile does not fit an SM's tensor memory");
     const dim3 grid((unsigned)((M + mtb::umma::BM - 1) / mtb::umma::BM), (unsigned)splits, (unsigned)((N + BN - 1) / BN));
-    kern<<<grid, 128, T::SMEM, st>>>(ma, mb, part, M, N, nkb, kps, err, kWaitNs);
+    kern<<<grid, 128, T::SMEM, st>>>(ma, mb, out, M, N, nkb, kps, err, kWaitNs);
     MTB_CUDA(cudaGetLastError());
 }
 
-// part[s][m][n] = sum over split s of A[m][:] . B[n][:] (A [M][lda], B [N][ldb], bf16, K valid).
-void gemm(const __nv_bfloat16* A, int M, int lda, const __nv_bfloat16* Bm, int N, int ldb, int K, float* part,
-          int splits, int kps, int* err, cudaStream_t st) {
+// A[M][lda] . B[N][ldb]^T over the first K columns (bf16): the partial sums of each split, or the
+// finished result with one split (mtb::umma::GemmOut).
+void gemm(const __nv_bfloat16* A, int M, int lda, const __nv_bfloat16* Bm, int N, int ldb, int K,
+          const mtb::umma::GemmOut& out, int splits, int kps, int* err, cudaStream_t st) {
+    if (!out.part && splits != 1) mtb::fail(MT_ERR_INTERNAL, "a split-K product needs a partial-sum buffer");
     const int bn = gemm_bn(N);
     CUtensorMap ma, mb;
     encode_kmajor(&ma, A, M, lda, mtb::umma::BM);
     encode_kmajor(&mb, Bm, N, ldb, bn);
     const int nkb = (K + mtb::umma::BK - 1) / mtb::umma::BK;
     switch (bn) {
-        case 16: gemm_launch<16>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
-        case 32: gemm_launch<32>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
-        case 64: gemm_launch<64>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
-        case 128: gemm_launch<128>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
-        default: gemm_launch<256>(ma, mb, part, M, N, nkb, splits, kps, err, st); break;
+        case 16: gemm_launch<16>(ma, mb, out, M, N, nkb, splits, kps, err, st); break;
+        case 32: gemm_launch<32>(ma, mb, out, M, N, nkb, splits, kps, err, st); break;
+        case 64: gemm_launch<64>(ma, mb, out, M, N, nkb, splits, kps, err, st); break;
+        case 128: gemm_launch<128>(ma, mb, out, M, N, nkb, splits, kps, err, st); break;
+        default: gemm_launch<256>(ma, mb, out, M, N, nkb, splits, kps, err, st); break;
     }
 }
 
@@ -361,17 +394,24 @@ void conv_as_gemm(const __nv_bfloat16* in, const __nv_bfloat16* mask, int Cin_ef
     int splits = 1, kps = 1;
     gemm_split(P, N, K, &splits, &kps);
     const size_t offB = align256((size_t)P * ldk * 2), offP = offB + align256((size_t)N * ldk * 2);
-    Workspace& ws = workspace(offP + (size_t)splits * P * N * 4);
+    Workspace& ws = workspace(offP + (splits > 1 ? (size_t)splits * P * N * 4 : 0));
     auto* A = reinterpret_cast<__nv_bfloat16*>(ws.p);
     auto* Bm = reinterpret_cast<__nv_bfloat16*>(ws.p + offB);
-    auto* part = reinterpret_cast<float*>(ws.p + offP);
-    im2col_kernel<<<elem_grid((size_t)P * ldk), 256, 0, st>>>(in, mask, A, B, Cin_eff, H, W, ldk);
+    const dim3 ig((unsigned)((P + 31) / 32), (unsigned)((ldk + 63) / 64));
+    im2col_kernel<<<ig, dim3(32, 8), 0, st>>>(in, mask, A, B, Cin_eff, H, W, ldk);
     MTB_CUDA(cudaGetLastError());
     pack_weights_kernel<<<elem_grid((size_t)N * ldk), 256, 0, st>>>(w, Bm, Cout, Cin, ldk, data_grad ? 1 : 0);
     MTB_CUDA(cudaGetLastError());
-    gemm(A, P, ldk, Bm, N, ldk, K, part, splits, kps, ws.err, st);
     const long long HW = (long long)H * W;
-    finalize(part, splits, P, N, 0, P, bias, relu, out_bf, out_f, HW, (long long)N * HW, 1, HW, st);
+    mtb::umma::GemmOut o{};
+    if (splits == 1) {  // the GEMM's epilogue writes the NCHW result itself
+        o = {nullptr, bias, relu, out_bf, out_f, HW, (long long)N * HW, 1, HW};
+        gemm(A, P, ldk, Bm, N, ldk, K, o, 1, kps, ws.err, st);
+        return;
+    }
+    o.part = reinterpret_cast<float*>(ws.p + offP);
+    gemm(A, P, ldk, Bm, N, ldk, K, o, splits, kps, ws.err, st);
+    finalize(o.part, splits, P, N, 0, P, bias, relu, out_bf, out_f, HW, (long long)N * HW, 1, HW, st);
 }
 
 }  // namespace
@@ -414,12 +454,15 @@ mt_status mt_sg_conv3x3_backward_weight(const void* in, const void* dout, const 
         auto* X = reinterpret_cast<__nv_bfloat16*>(ws.p);
         auto* Y = reinterpret_cast<__nv_bfloat16*>(ws.p + offY);
         auto* part = reinterpret_cast<float*>(ws.p + offP);
-        im2col_t_kernel<<<elem_grid((size_t)M * ldp), 256, 0, st>>>((const __nv_bfloat16*)in, X, B, Cin, H, W, ldp);
+        const unsigned gx = (unsigned)std::min((ldp + 255) / 256, 1024);
+        im2col_t_kernel<<<dim3(gx, (unsigned)(Cin + 1)), 256, 0, st>>>((const __nv_bfloat16*)in, X, B, Cin, H, W, ldp);
         MTB_CUDA(cudaGetLastError());
-        channel_major_kernel<<<elem_grid((size_t)Cout * ldp), 256, 0, st>>>(
+        channel_major_kernel<<<dim3(gx, (unsigned)Cout), 256, 0, st>>>(
             (const __nv_bfloat16*)dout, (const __nv_bfloat16*)out_mask, Y, B, Cout, HW, ldp);
         MTB_CUDA(cudaGetLastError());
-        gemm(X, M, ldp, Y, Cout, ldp, P, part, splits, kps, ws.err, st);
+        mtb::umma::GemmOut o{};
+        o.part = part;
+        gemm(X, M, ldp, Y, Cout, ldp, P, o, splits, kps, ws.err, st);
         // rows k < 9*Cin: dw[o][k]; row 9*Cin: db[o]
         finalize(part, splits, M, Cout, 0, M - 1, nullptr, 0, nullptr, dw, M - 1, 0, 1, M - 1, st);
         finalize(part, splits, M, Cout, M - 1, 1, nullptr, 0, nullptr, db, 1, 0, 0, 1, st);

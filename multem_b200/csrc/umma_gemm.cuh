@@ -7,7 +7,8 @@
 // A [M][K] and B [N][K] are bf16, K-major (k contiguous), row pitch a multiple of 8 elements;
 // the K range is cut into blocks of 64 (one 128-byte row of the 128-byte swizzle) and the blocks
 // into `splits` contiguous ranges, one per grid.y, whose FP32 partial sums the caller reduces in a
-// fixed order (deterministic results). Tiles are 128 rows (the tensor-memory lanes) x BN columns;
+// fixed order (deterministic results); with a single split the kernel applies bias and ReLU and
+// stores the result itself (GemmOut). Tiles are 128 rows (the tensor-memory lanes) x BN columns;
 // rows and columns past M, N and k past K arrive as zeros (tensor-copy out-of-bounds fill).
 //
 // One CTA of 4 warps per tile. Warp 0 allocates BN (at least 32) tensor-memory columns. Thread 0
@@ -25,6 +26,8 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cuda_bf16.h>
 
 #include <cstdint>
 
@@ -108,9 +111,22 @@ __device__ __forceinline__ void tensor_load_2d(void* dst, const CUtensorMap* map
         : "memory");
 }
 
+// Where the accumulator goes. With `part` set, the FP32 partial sums of each K split,
+// part[split][m][n]; otherwise (one split) the finished result: v = acc + bias[n], ReLU when
+// `relu`, stored as bf16 and/or float at (m / mdiv) * s_mq + (m % mdiv) * s_mr + n * s_n (an NCHW
+// image when mdiv is H*W, s_mq the image stride, s_mr 1 and s_n H*W).
+struct GemmOut {
+    float* part;
+    const float* bias;
+    int relu;
+    __nv_bfloat16* out_bf;
+    float* out_f;
+    long long mdiv, s_mq, s_mr, s_n;
+};
+
 template <int BN>
 __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ CUtensorMap mapA,
-                                                      const __grid_constant__ CUtensorMap mapB, float* __restrict__ part,
+                                                      const __grid_constant__ CUtensorMap mapB, GemmOut o,
                                                       int M, int N, int nkb, int kb_per_split, int* err,
                                                       long long wait_ns) {
     using T = Tile<BN>;
@@ -187,15 +203,32 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ CU
 
     const int row = m0 + warp * 32 + lane;
     const bool have = nk > 0 && !err_set(err);
+    long long obase = 0;
+    if (!o.part) obase = (row / o.mdiv) * o.s_mq + (row % o.mdiv) * o.s_mr;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
         uint32_t r[16];
         tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, r);
         if (row < M) {
-            float* dst = part + ((size_t)split * M + row) * N + n0 + c0;
+            if (o.part) {
+                float* dst = o.part + ((size_t)split * M + row) * N + n0 + c0;
 #pragma unroll
-            for (int j = 0; j < 16; j++)
-                if (n0 + c0 + j < N) dst[j] = have ? __uint_as_float(r[j]) : 0.0f;
+                for (int j = 0; j < 16; j++)
+                    if (n0 + c0 + j < N) dst[j] = have ? __uint_as_float(r[j]) : 0.0f;
+            } else {
+                // lanes hold consecutive rows: for each column the warp's stores are contiguous
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int n = n0 + c0 + j;
+                    if (n < N) {
+                        float v = (have ? __uint_as_float(r[j]) : 0.0f) + (o.bias ? o.bias[n] : 0.0f);
+                        if (o.relu) v = fmaxf(v, 0.0f);
+                        const long long idx = obase + n * o.s_n;
+                        if (o.out_bf) o.out_bf[idx] = __float2bfloat16_rn(v);
+                        if (o.out_f) o.out_f[idx] = v;
+                    }
+                }
+            }
         }
     }
     tc_fence_before();
