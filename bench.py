@@ -33,7 +33,7 @@ per-run set-up; --impl reference --ref-gpu times its GPU path the same way.
 all-reduce and its check, without any simulation (a check of the multi-process plumbing).
 --profile-case NS runs one configuration of the workload with an NS x NS raster (the small case the
 ncu captures under profiles/ use: NS = 16 gives one launch of 256 probes, 512 MiB of waves) and
-prints its device time.
+prints its device time; --profile-nx NX runs it on an NX x NX grid instead of 512 x 512.
 """
 from __future__ import annotations
 
@@ -395,8 +395,9 @@ def large_field_live(conf):
 
 def run_profile_case(args):
     """One configuration of the workload on an NS x NS raster (a bounded case for profilers)."""
-    from multem_b200 import api
-    p = _raster(workload(1), args.profile_case)
+    from multem_b200 import api, specimens
+    nx = args.profile_nx
+    p = _raster(workload(1) if nx == 512 else specimens.stem_srtio3(nx=nx, ny=nx, nconf=1, seed=1), args.profile_case)
     e = api.Engine(p)
     e.prepare_confs(1, 1)
     e.run_prepared(1, 1)
@@ -405,7 +406,7 @@ def run_profile_case(args):
     tun = e.tuning()
     n_launch = e.launch_count()
     e.close()
-    print(json.dumps({"case": f"512^2 SrTiO3, {args.profile_case}x{args.profile_case} probes, 1 configuration",
+    print(json.dumps({"case": f"{nx}^2 SrTiO3, {args.profile_case}x{args.profile_case} probes, 1 configuration",
                       "device_ms": t["total_ms"], "launches": n_launch, "tuning": tun,
                       "detector_sums": img.sum(axis=(2, 3)).ravel().tolist()}))
     return 0
@@ -548,6 +549,8 @@ def main():
     ap.add_argument("--rank-timeout", type=int, default=1800, help="bound of a self-started multi-rank run (s)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="NS",
                     help="one configuration with an NS x NS raster, for profilers; prints its device time")
+    ap.add_argument("--profile-nx", type=int, default=512, metavar="NX",
+                    help="grid of the --profile-case run (the same SrTiO3 specimen and slices, NX x NX)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
