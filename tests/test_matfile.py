@@ -126,12 +126,15 @@ def _fake_output(p, rng):
     return d, out
 
 
-@pytest.mark.parametrize("case", ["stem", "ew"])
+@pytest.mark.parametrize("case", ["stem", "ew", "hrtem"])
 @pytest.mark.parametrize("compress", [False, True])
 def test_output_struct_layout(tmp_path, case, compress):
-    p = _cases()[case]
+    p = _cases()[case] if case != "hrtem" else specimens.hrtem_si001(nx=64, ny=64, na=2, nb=2, nc=2)
     if case == "stem":
         p.pn_coh_contrib = 1
+    if case == "hrtem":
+        p.simulation_type, p.pn_model, p.pn_nconf, p.pn_coh_contrib = 32, 3, 2, 1
+        p.illumination_model = 1
     rng = np.random.default_rng(7)
     d, out = _fake_output(p, rng)
     path = tmp_path / "out.mat"
@@ -153,7 +156,11 @@ def test_output_struct_layout(tmp_path, case, compress):
                 assert dets.shape == (1, d.n_detector)
                 for k in range(d.n_detector):
                     np.testing.assert_array_equal(dets[0, k]["image"], out["data"][it][name][k])
-        else:
+        elif case == "ew":
             assert set(data.dtype.names) == {"m2psi_tot", "psi_coh"}
             np.testing.assert_array_equal(e["m2psi_tot"], out["data"][it]["m2psi_tot"])
             np.testing.assert_array_equal(e["psi_coh"], out["data"][it]["psi_coh"])
+        else:
+            assert set(data.dtype.names) == {"m2psi_tot", "m2psi_coh"}
+            np.testing.assert_array_equal(e["m2psi_tot"], out["data"][it]["m2psi_tot"])
+            np.testing.assert_array_equal(e["m2psi_coh"], out["data"][it]["m2psi_coh"])
