@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -132,7 +133,17 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
             d_coh_m2_.alloc((size_t)n_thk * onxy);
         }
         d_ew_m2_.alloc((size_t)n_thk * onxy);
-        d_tmp_.alloc(nxy);
+        // frozen-phonon configurations advance together (one launch per pass for all of them) where
+        // every configuration runs the same sequence of passes: a plane incident wave, one beam
+        // rotation, no source or defocus quadrature; the transmission functions of all of them are
+        // held at once (at most 32 GiB)
+        const bool batchable = !m_.is_convergent_wave() && !m_.is_user_wave() && m_.nrot == 1 &&
+                               m_.si_x.size() * m_.ti_x.size() == 1;
+        const size_t trans_bytes = spec_->slices().size() * nxy * sizeof(float2);
+        int eb = batchable ? std::min(8, m_.number_conf()) : 1;
+        while (eb > 1 && (size_t)eb * trans_bytes > ((size_t)32 << 30)) eb--;
+        ew_batch_ = batchable ? std::max(1, std::min(env_int("MTB_EW_BATCH", eb), m_.number_conf())) : 1;
+        d_tmp_.alloc((size_t)ew_batch_ * nxy);
         niter_ = m_.number_conf() * m_.nrot * (int)(m_.si_x.size() * m_.ti_x.size());
         if (m_.is_convergent_wave()) {
             // convergent beams at iw_x/iw_y, summed (Incident_Wave::operator(), src/incident_wave.cuh:72-90);
@@ -153,7 +164,8 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
             probe_norm_ = aperture_norm();
         }
     }
-    d_psi_.alloc((size_t)batch_ * nxy);
+    d_psi_.alloc((size_t)std::max(batch_, ew_batch_) * nxy);
+    slot_.resize(2 * (size_t)ew_batch_);
     if (m_.grid.bwl) build_bwl();
     if (m_.is_imaging()) build_ctf_tables();
     if (m_.tilted()) {
@@ -162,7 +174,7 @@ Engine::Engine(const mt_system_conf* conf, const mt_input_multislice* in) {
         if (m_.is_scanning() && n_thk > 1) d_tmp_.alloc((size_t)batch_ * nxy);
         if (m_.is_ISTEM() && n_thk > 1) d_tmp2_.alloc((size_t)batch_ * nxy);
     }
-    d_trans_.alloc((size_t)spec_->slices().size() * nxy);
+    d_trans_.alloc((size_t)ew_batch_ * spec_->slices().size() * nxy);
     d_err_.alloc(1);
     MTB_CUDA(cudaMemsetAsync(d_err_.p, 0, sizeof(int), stream_));
     // line-pass variants: MTB_PIPE pins them (bit 0 rows, bit 1 columns: bulk-copy fed) and
@@ -324,20 +336,20 @@ void Engine::build_bwl() {
 // bwl = 1: T <- IFFT(bwl_factor/N * FFT(T)) for the slices of a configuration, as three line passes
 // over all slices at once (a real-space row pass, the column pass with the cut-off, the inverse row
 // pass).
-void Engine::band_limit_trans(const ConfData& cd) {
+void Engine::band_limit_trans(const ConfData& cd, float2* trans) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const int ns = cd.last_slice + 1;
     RowArgs ra{};
-    ra.in = d_trans_.p;
-    ra.out = d_trans_.p;
+    ra.in = trans;
+    ra.out = trans;
     ra.trans = d_one_.p;
     ra.nx = nx;
     ra.nprobe = ns;
     ra.scale = 1.0f;
     rows(ROW_FIRST_REAL, ra);
     ColArgs ca{};
-    ca.in = d_trans_.p;
-    ca.out = d_trans_.p;
+    ca.in = trans;
+    ca.out = trans;
     ca.ny = ny;
     ca.nprobe = ns;
     ca.g = gdev_;
@@ -471,6 +483,15 @@ ProbeDev Engine::probe_params(float c_c_10, int nz_c10, bool tilt_offset) const 
 
 // Host part of one configuration: Spec::move_atoms, slicing, tables; uploads on the stream.
 void Engine::prepare_conf(ConfData& cd, int iconf) {
+    ConfStage st;
+    prepare_conf_host(cd, iconf, st);
+    prepare_conf_device(cd, st);
+}
+
+// Host part of a configuration's set-up: phonon displacement (host generator), slicing, propagator
+// tables and probe defocus into cd's host fields and the staging vectors of st. Runs while the
+// GPU works on earlier configurations; touches no device buffer of cd.
+void Engine::prepare_conf_host(ConfData& cd, int iconf, ConfStage& st) {
     // pn_rng 1: the undisplaced atoms and their slicing once, the displacements on the device
     const bool device_rng = m_.pn_rng == 1 && m_.is_frozen_phonon();
     if (!device_rng)
@@ -482,7 +503,9 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     cd.iconf = iconf;
     cd.n_slice = (int)S.size();
-    std::vector<float4> at;
+    std::vector<float4>& at = st.at;
+    at.clear();
+    st.n_atoms = A.size();
     if (!device_rng || !d_atoms_u_.p) {
         at.resize(A.size());
         for (size_t i = 0; i < A.size(); i++) {
@@ -496,7 +519,8 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
         d_atoms_u_.upload(at.data(), at.size(), stream_);
         d_sigma_.upload(A.sigma.data(), A.size(), stream_);
     }
-    std::vector<int2> rg(S.size());
+    std::vector<int2>& rg = st.rg;
+    rg.resize(S.size());
     cd.slice_ithk.resize(S.size());
     cd.last_slice = -1;
     for (size_t k = 0; k < S.size(); k++) {
@@ -510,13 +534,23 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
     for (size_t t = 0; t < TH.size(); t++) cd.thick_z_back_prop[t] = TH[t].z_back_prop;
     const size_t pl = (size_t)nx + ny;
     const size_t rb = (S.size() + TH.size()) * pl;  // one block per beam rotation
-    std::vector<float2> prop(rb * m_.nrot);
-    for (int r = 0; r < m_.nrot; r++) {
-        float2* q = prop.data() + r * rb;
-        for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), q + k * pl, q + k * pl + nx, false, r);
-        for (size_t t = 0; t < TH.size(); t++)
-            prop_tables(TH[t].z_back_prop, q + (S.size() + t) * pl, q + (S.size() + t) * pl + nx, true, r);
+    // the tables depend on the slice thicknesses and back-propagation distances only, which the
+    // phonon displacements (x and y) do not change: computed once and reused while they match
+    std::vector<float> key;
+    key.reserve(S.size() + TH.size());
+    for (size_t k = 0; k < S.size(); k++) key.push_back(spec_->dz((int)k));
+    for (size_t t = 0; t < TH.size(); t++) key.push_back(TH[t].z_back_prop);
+    if (key != prop_key_ || prop_cache_.size() != rb * m_.nrot) {
+        prop_cache_.assign(rb * m_.nrot, make_float2(0.0f, 0.0f));
+        for (int r = 0; r < m_.nrot; r++) {
+            float2* q = prop_cache_.data() + r * rb;
+            for (size_t k = 0; k < S.size(); k++) prop_tables(spec_->dz((int)k), q + k * pl, q + k * pl + nx, false, r);
+            for (size_t t = 0; t < TH.size(); t++)
+                prop_tables(TH[t].z_back_prop, q + (S.size() + t) * pl, q + (S.size() + t) * pl + nx, true, r);
+        }
+        prop_key_ = std::move(key);
     }
+    st.prop = prop_cache_;
     // incident-wave defocus relative to the first slice (Incident_Wave::operator(),
     // src/incident_wave.cuh:54-72): f_s = c_10 - (zero_defocus_plane - z_m(0)), with c_10 moved
     // by each defocus-spread point (cond_lens.set_defocus(c_10_0 + qt.x), src/tem_simulation.cuh:155-157)
@@ -531,16 +565,22 @@ void Engine::prepare_conf(ConfData& cd, int iconf) {
         cd.probe_c_c_10.push_back(L.c_c_10);
         cd.probe_nz_c10.push_back(!is_zero_f(f_s));
     }
+}
+
+// Device part: the configuration's atoms (uploaded, or displaced on the device), slice ranges and
+// propagator tables into cd's buffers. The uploads wait for the stream's earlier work.
+void Engine::prepare_conf_device(ConfData& cd, ConfStage& st) {
+    const bool device_rng = m_.pn_rng == 1 && m_.is_frozen_phonon();
     if (device_rng) {
-        cd.atoms.alloc(A.size());
-        launch_phonon_displace(d_atoms_u_.p, d_sigma_.p, (int)A.size(), (uint32_t)m_.pn_seed, iconf, m_.pn_x, m_.pn_y,
-                               cd.atoms.p, stream_);
+        cd.atoms.alloc(st.n_atoms);
+        launch_phonon_displace(d_atoms_u_.p, d_sigma_.p, (int)st.n_atoms, (uint32_t)m_.pn_seed, cd.iconf, m_.pn_x,
+                               m_.pn_y, cd.atoms.p, stream_);
     } else {
-        cd.atoms.upload(at.data(), at.size(), stream_);
+        cd.atoms.upload(st.at.data(), st.at.size(), stream_);
     }
-    cd.ranges.upload(rg.data(), rg.size(), stream_);
-    cd.prop.upload(prop.data(), prop.size(), stream_);
-    synchronize();  // host vectors go out of scope
+    cd.ranges.upload(st.rg.data(), st.rg.size(), stream_);
+    cd.prop.upload(st.prop.data(), st.prop.size(), stream_);
+    synchronize();  // the staging vectors may be reused
 }
 
 ConfData* Engine::find_conf(int iconf) {
@@ -600,7 +640,7 @@ void Engine::run_prepared(int c0, int c1) {
             MTB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             capturing_ = true;
             try {
-                for (int c = c0; c <= c1; c++) run_conf(*find_conf(c));
+                run_prepared_range(c0, c1);
             } catch (...) {
                 capturing_ = false;
                 cudaStreamEndCapture(stream_, &g);
@@ -627,7 +667,7 @@ void Engine::run_prepared(int c0, int c1) {
         iter_ += range_graph_.iters;
         add_launches(range_graph_.launches);
     } else {
-        for (int c = c0; c <= c1; c++) run_conf(*find_conf(c));
+        run_prepared_range(c0, c1);
     }
     MTB_CUDA(cudaEventRecord(run_b_, stream_));
     launches_ = launches_issued() - l0;
@@ -701,13 +741,27 @@ void Engine::run_confs(int c0, int c1) {
     long long l0 = launches_issued();
     // every configuration as its slot's CUDA graph: captured twice (once per slot) and replayed
     // while the launch sequence and its arguments match
+    const int B = ew_batch_;
     if (graphs_ && !timing_) {
-        // configuration c is prepared in slot c % 2 (prepare_conf waits for the stream, so the
-        // slot's previous user, c - 2, has finished) and runs as that slot's graph
-        for (int c = c0; c <= c1; c++) {
-            ConfData& cd = slot_[c & 1];
-            prepare_conf(cd, c);
-            run_conf_graph(cd, graph_[c & 1]);
+        // batch k of B configurations is prepared in slot group k % 2 (prepare_conf waits for the
+        // stream, so the group's previous user, batch k - 2, has finished) and runs as that group's
+        // graph
+        // the host part of batch k + 1 runs while batch k's graph executes
+        std::vector<ConfData*> cds(B);
+        std::vector<ConfStage> st(B);
+        auto stage = [&](int c, int k) {
+            const int nb = std::min(B, c1 - c + 1);
+            for (int b = 0; b < nb; b++) prepare_conf_host(slot_[(size_t)(k & 1) * B + b], c + b, st[b]);
+        };
+        stage(c0, 0);
+        for (int c = c0, k = 0; c <= c1; c += B, k++) {
+            const int nb = std::min(B, c1 - c + 1);
+            for (int b = 0; b < nb; b++) {
+                cds[b] = &slot_[(size_t)(k & 1) * B + b];
+                prepare_conf_device(*cds[b], st[b]);
+            }
+            run_conf_graph(cds.data(), nb, graph_[k & 1]);
+            if (c + B <= c1) stage(c + B, k + 1);
         }
         launches_ = launches_issued() - l0;
         synchronize();
@@ -716,23 +770,39 @@ void Engine::run_confs(int c0, int c1) {
     // configuration c is prepared on the host while c-1 runs; c-1's buffers go back to the pool once
     // its last launch has completed
     if (!conf_done_) MTB_CUDA(cudaEventCreateWithFlags(&conf_done_, cudaEventDisableTiming));
-    ConfData prev;
-    bool have_prev = false;
-    for (int c = c0; c <= c1; c++) {
-        ConfData cd;
-        prepare_conf(cd, c);
-        run_conf(cd);
-        if (have_prev) {
+    std::vector<ConfData> prev;
+    for (int c = c0; c <= c1; c += B) {
+        const int nb = std::min(B, c1 - c + 1);
+        std::vector<ConfData> cur(nb);
+        std::vector<ConfData*> cds(nb);
+        for (int b = 0; b < nb; b++) {
+            prepare_conf(cur[b], c + b);
+            cds[b] = &cur[b];
+        }
+        run_conf_batch(cds.data(), nb);
+        if (!prev.empty()) {
             MTB_CUDA(cudaEventSynchronize(conf_done_));
-            prev.release_idle();
+            for (auto& cd : prev) cd.release_idle();
         }
         MTB_CUDA(cudaEventRecord(conf_done_, stream_));
-        prev = std::move(cd);
-        have_prev = true;
+        prev = std::move(cur);
     }
     launches_ = launches_issued() - l0;
     synchronize();
-    prev.release_idle();
+    for (auto& cd : prev) cd.release_idle();
+}
+
+// Configurations c0..c1 (prepared) run in batches of ew_batch_.
+static void for_batches(int c0, int c1, int B, const std::function<void(int, int)>& f) {
+    for (int c = c0; c <= c1; c += B) f(c, std::min(B, c1 - c + 1));
+}
+
+void Engine::run_prepared_range(int c0, int c1) {
+    for_batches(c0, c1, ew_batch_, [&](int c, int nb) {
+        std::vector<ConfData*> cds(nb);
+        for (int b = 0; b < nb; b++) cds[b] = find_conf(c + b);
+        run_conf_batch(cds.data(), nb);
+    });
 }
 
 void Engine::prepare_run() {
@@ -749,11 +819,14 @@ void Engine::record_run() {
     cancel_ = false;
     capturing_ = true;  // no host synchronisation (check_cancel) while the work is recorded
     try {
-        for (int c = m_.fp_iconf_0; c <= m_.pn_nconf; c++) {
-            ConfData* cd = find_conf(c);
-            if (!cd) fail(MT_ERR_INTERNAL, "configuration not prepared before recording");
-            run_conf(*cd);
-        }
+        for_batches(m_.fp_iconf_0, m_.pn_nconf, ew_batch_, [&](int c, int nb) {
+            std::vector<ConfData*> cds(nb);
+            for (int b = 0; b < nb; b++) {
+                cds[b] = find_conf(c + b);
+                if (!cds[b]) fail(MT_ERR_INTERNAL, "configuration not prepared before recording");
+            }
+            run_conf_batch(cds.data(), nb);
+        });
     } catch (...) {
         capturing_ = false;
         throw;
@@ -782,9 +855,14 @@ std::vector<char> Engine::graph_signature(const ConfData& cd) const {
 // run_conf as a CUDA graph: captured once, then replayed for every configuration with the same
 // launch sequence and arguments (same slot buffers, slice count, thickness map and probe defocus).
 // The line-pass autotuner runs before the capture (it times launches and waits for them).
-void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
-    if (tune_) tune(cd);
-    std::vector<char> sig = graph_signature(cd);
+void Engine::run_conf_graph(ConfData* const* cds, int nb, ConfGraph& g) {
+    if (tune_) tune(*cds[0]);
+    std::vector<char> sig;
+    sig.insert(sig.end(), (const char*)&nb, (const char*)&nb + sizeof(nb));
+    for (int b = 0; b < nb; b++) {
+        std::vector<char> s = graph_signature(*cds[b]);
+        sig.insert(sig.end(), s.begin(), s.end());
+    }
     if (!g.exec || sig != g.sig) {
         if (g.exec) {
             MTB_CUDA(cudaGraphExecDestroy(g.exec));
@@ -796,7 +874,7 @@ void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
         MTB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         capturing_ = true;
         try {
-            run_conf(cd);
+            run_conf_batch(cds, nb);
         } catch (...) {
             capturing_ = false;
             cudaStreamEndCapture(stream_, &graph);
@@ -822,22 +900,37 @@ void Engine::run_conf_graph(ConfData& cd, ConfGraph& g) {
 }
 
 void Engine::run_conf(ConfData& cd) {
-    // transmission functions of the slices up to the last output thickness
-    SplatArgs sa{};
-    sa.g = gdev_;
-    sa.atoms = cd.atoms.p;
-    sa.slice_range = cd.ranges.p;
-    sa.tab = d_tab_.p;
-    sa.R_max = d_Rmax_.p;
-    sa.n_types = (int)Z_of_type_.size();
-    sa.nR = m_.nR;
-    sa.w = m_.Vr_factor();
-    sa.wpo = (m_.interaction_model == 3);
-    sa.trans = d_trans_.p;
-    sa.V = nullptr;
-    launch_splat(sa, 0, cd.last_slice + 1, stream_);
-    if (d_bwl_.p) band_limit_trans(cd);
-    if (m_.is_scanning()) run_stem(cd); else run_ew(cd);
+    ConfData* p = &cd;
+    run_conf_batch(&p, 1);
+}
+
+void Engine::run_conf_batch(ConfData* const* cds, int nb) {
+    if (nb < 1 || nb > ew_batch_ || (nb > 1 && m_.is_scanning())) fail(MT_ERR_INTERNAL, "bad configuration batch");
+    const size_t tstride = (size_t)spec_->slices().size() * m_.grid.nx * m_.grid.ny;
+    for (int b = 1; b < nb; b++)
+        if (cds[b]->n_slice != cds[0]->n_slice || cds[b]->last_slice != cds[0]->last_slice ||
+            cds[b]->slice_ithk != cds[0]->slice_ithk)
+            fail(MT_ERR_INTERNAL, "configurations of a batch must share their slicing");
+    for (int b = 0; b < nb; b++) {
+        const ConfData& cd = *cds[b];
+        float2* trans = d_trans_.p + b * tstride;
+        // transmission functions of the slices up to the last output thickness
+        SplatArgs sa{};
+        sa.g = gdev_;
+        sa.atoms = cd.atoms.p;
+        sa.slice_range = cd.ranges.p;
+        sa.tab = d_tab_.p;
+        sa.R_max = d_Rmax_.p;
+        sa.n_types = (int)Z_of_type_.size();
+        sa.nR = m_.nR;
+        sa.w = m_.Vr_factor();
+        sa.wpo = (m_.interaction_model == 3);
+        sa.trans = trans;
+        sa.V = nullptr;
+        launch_splat(sa, 0, cd.last_slice + 1, stream_);
+        if (d_bwl_.p) band_limit_trans(cd, trans);
+    }
+    if (m_.is_scanning()) run_stem(*cds[0]); else run_ew(cds, nb);
 }
 
 // Autotuner of the line passes. For each (nx, ny, allocated probes per launch) the process times,
@@ -931,7 +1024,7 @@ Engine::Tuning Engine::tune_passes(int nprobe, ConfData& cd) {
 }
 
 void Engine::tune(ConfData& cd) {
-    const int nprobe = m_.is_scanning() ? std::min(batch_, m_.n_scan()) : 1;
+    const int nprobe = m_.is_scanning() ? std::min(batch_, m_.n_scan()) : ew_batch_;
     const Tuning t = tune_passes(nprobe, cd);
     pipe_ = t.pipe;
     shape_ = t.shape;
@@ -1150,7 +1243,12 @@ void Engine::run_stem(ConfData& cd) {
     }
 }
 
-void Engine::run_ew(ConfData& cd) {
+// nb configurations of the batch advance together: their waves are the nb "probes" of every pass,
+// each row pass multiplying wave b by its own transmission functions (trans_stride), and the
+// outputs of each thickness are accumulated wave by wave in configuration order, as nb separate
+// configurations would be.
+void Engine::run_ew(ConfData* const* cds, int nb) {
+    const ConfData& cd = *cds[0];
     const int nx = m_.grid.nx, ny = m_.grid.ny;
     const size_t nxy = (size_t)nx * ny;
     const size_t pl = (size_t)nx + ny;
@@ -1161,17 +1259,19 @@ void Engine::run_ew(ConfData& cd) {
 
     RowArgs ra{};
     ra.nx = nx;
-    ra.nprobe = 1;
+    ra.nprobe = nb;
     ra.scale = 1.0f;
+    ra.trans_stride = nb > 1 ? (size_t)spec_->slices().size() * nxy : 0;
     ColArgs ca{};
     ca.ny = ny;
-    ca.nprobe = 1;
+    ca.nprobe = nb;
     ca.g = gdev_;
     ca.n_det = 0;
     ca.P2 = d_bwl_.p;  // band-width limit of every propagation (NULL without bwl)
-    if (tune_) tune(cd);
+    if (tune_) tune(*cds[0]);
     const bool conv = m_.is_convergent_wave();
     const bool user = m_.is_user_wave();
+    if (nb > 1 && (conv || user || m_.nrot != 1)) fail(MT_ERR_INTERNAL, "this incident wave runs one configuration at a time");
     const size_t rblock = (size_t)(cd.n_slice + (int)cd.thick_z_back_prop.size()) * pl;
     // beam rotations of PED / HCTEM (Multislice::PED_HCTEM, src/tem_simulation.cuh:274-300); one
     // pass otherwise
@@ -1220,6 +1320,7 @@ void Engine::run_ew(ConfData& cd) {
             rr.in = d_psi_.p;
             rr.out = d_tmp_.p;
             rr.trans = ramp;
+            rr.trans_stride = 0;  // one ramp for every wave
             rows(ROW_STEP, rr);
             src = d_tmp_.p;
         }
@@ -1231,7 +1332,9 @@ void Engine::run_ew(ConfData& cd) {
         if (m_.is_imaging()) {
             // coherent contribution: the weighted wave of this thickness, imaged once at output
             // (add_scale_psi_coh then set_m2psi_coh, src/wave_function.cuh:166-172, 210-218)
-            if (d_coh_img_.p) launch_axpy_wave(src, (float)w, nxy, d_coh_img_.p + (size_t)ithk * nxy, stream_);
+            if (d_coh_img_.p)
+                for (int b = 0; b < nb; b++)
+                    launch_axpy_wave(src + b * nxy, (float)w, nxy, d_coh_img_.p + (size_t)ithk * nxy, stream_);
             // image formation: transfer function per defocus point, inverse transform, |psi|^2
             // weighted (Microscope_Effects::operator(), src/microscope_effects.cuh:56-85)
             for (size_t j = 0; j < m_.obj_c10.size(); j++) {
@@ -1243,9 +1346,10 @@ void Engine::run_ew(ConfData& cd) {
                 rb.out = d_tmp_.p;
                 rb.scale = 1.0f;
                 rows(ROW_INVERSE, rb);
-                launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e,
-                                     (double)(float)(w * m_.obj_w[j]), 0, nullptr, d_ew_m2_.p + (size_t)ithk * onxy,
-                                     stream_);
+                for (int b = 0; b < nb; b++)
+                    launch_ew_accumulate(d_tmp_.p + b * nxy, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0,
+                                         m_.out_iy_e, (double)(float)(w * m_.obj_w[j]), 0, nullptr,
+                                         d_ew_m2_.p + (size_t)ithk * onxy, stream_);
             }
             continue;
         }
@@ -1264,17 +1368,20 @@ void Engine::run_ew(ConfData& cd) {
         } else {
             cols(COL_LOAD | COL_PROP | COL_STORE, cb);
         }
-        // ED and CBED keep only |psi_hat|^2 (add_scale_crop_shift_m2psi_tot_from_psi, wave_function.cuh:172-184)
-        launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
-                             m_.is_EW() ? d_ew_psi_.p + (size_t)ithk * onxy * 2 : nullptr,
-                             sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
-        // coherent contribution of ED / CBED / PED: the configuration-weighted wave (add_scale_psi_coh,
-        // src/output_multislice.hpp:770-780), kept cropped and shifted like the intensity
-        if (d_ew_cohpsi_.p)
-            launch_ew_accumulate(d_tmp_.p, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, 0,
-                                 d_ew_cohpsi_.p + (size_t)ithk * onxy * 2, nullptr, stream_);
+        for (int b = 0; b < nb; b++) {
+            const float2* wave = d_tmp_.p + b * nxy;
+            // ED and CBED keep only |psi_hat|^2 (add_scale_crop_shift_m2psi_tot_from_psi, wave_function.cuh:172-184)
+            launch_ew_accumulate(wave, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, sc ? 1 : 0,
+                                 m_.is_EW() ? d_ew_psi_.p + (size_t)ithk * onxy * 2 : nullptr,
+                                 sc ? nullptr : d_ew_m2_.p + (size_t)ithk * onxy, stream_);
+            // coherent contribution of ED / CBED / PED: the configuration-weighted wave (add_scale_psi_coh,
+            // src/output_multislice.hpp:770-780), kept cropped and shifted like the intensity
+            if (d_ew_cohpsi_.p)
+                launch_ew_accumulate(wave, nx, ny, m_.out_ix_0, m_.out_ix_e, m_.out_iy_0, m_.out_iy_e, w, 0,
+                                     d_ew_cohpsi_.p + (size_t)ithk * onxy * 2, nullptr, stream_);
+        }
     }
-    iter_ += 1;
+    iter_ += nb;
     }
     }
     check_cancel();

@@ -165,6 +165,10 @@ class Engine {
     bool tune_ = true;               // choose pipe_, shape_, run_batch_ per shape with tune (MTB_PIPE unset)
     int shape_ = 0;                  // pipeline shapes of the step passes (bits 0-1 rows, bits 2-3 cols)
     int run_batch_ = 1;              // probes per launch (<= batch_, the allocated batch)
+    // exit-wave family (EW, ED, HRTEM) with frozen phonons: configurations whose waves advance
+    // through the slices together, one launch per pass for all of them, each with its own
+    // transmission functions (1: one configuration at a time)
+    int ew_batch_ = 1;
     DevBuf<float2> d_psi_;
     DevBuf<float2> d_trans_;
     DevBuf<float2> d_tmp_;
@@ -200,27 +204,42 @@ class Engine {
     void build_types();
     void build_tilt_ramp();
     void prepare_conf(ConfData& cd, int iconf);
+    struct ConfStage {                // host staging of a configuration's device data
+        std::vector<float4> at;
+        std::vector<int2> rg;
+        std::vector<float2> prop;
+        size_t n_atoms = 0;
+    };
+    void prepare_conf_host(ConfData& cd, int iconf, ConfStage& st);
+    std::vector<float> prop_key_;     // slice thicknesses and back-propagation distances of prop_cache_
+    std::vector<float2> prop_cache_;  // propagator tables of every rotation (per slice, then per thickness)
+    void prepare_conf_device(ConfData& cd, ConfStage& st);
     void run_conf(ConfData& cd);
+    // the splats of nb configurations (into consecutive transmission blocks) and their slice loop
+    // (nb > 1: exit-wave family only, configurations with identical slicing)
+    void run_conf_batch(ConfData* const* cds, int nb);
+    void run_prepared_range(int c0, int c1);  // prepared configurations c0..c1 in batches of ew_batch_
     struct Tuning {
         int pipe, shape, nprobe;
     };
     Tuning tune_passes(int nprobe, ConfData& cd);
     void tune(ConfData& cd);         // tune_passes for this engine's shape; sets pipe_, shape_, run_batch_
     void run_stem(ConfData& cd);
-    void run_ew(ConfData& cd);
+    void run_ew(ConfData* const* cds, int nb);
     void prop_tables(float dz, float2* px, float2* py, bool output, int irot = 0) const;
     ProbeDev probe_params(float c_c_10, int nz_c10, bool tilt_offset) const;
     void build_ctf_tables();
     float aperture_norm() const;
     void build_user_wave();
     void build_bwl();
-    void band_limit_trans(const ConfData& cd);
+    void band_limit_trans(const ConfData& cd, float2* trans);
     void check_cancel();
     void zero_accumulators();        // the accumulators' memsets on the stream (no synchronisation)
     ConfData* find_conf(int iconf);
 
-    // CUDA graphs of run_conf, one per configuration slot (run_confs alternates two slots whose
-    // buffers keep their addresses), replayed while the launch sequence and its arguments match
+    // CUDA graphs of run_conf_batch, one per group of configuration slots (run_confs alternates two
+    // groups of ew_batch_ slots whose buffers keep their addresses), replayed while the launch
+    // sequence and its arguments match
     struct ConfGraph {
         cudaGraphExec_t exec = nullptr;
         std::vector<char> sig;  // launch-shaping data the graph was captured with
@@ -229,11 +248,11 @@ class Engine {
     };
     bool graphs_ = true;
     bool capturing_ = false;
-    ConfData slot_[2];
+    std::vector<ConfData> slot_;     // 2 x ew_batch_
     ConfGraph graph_[2];
     ConfGraph range_graph_;  // run_prepared: one graph over a range of prepared configurations
     std::vector<char> graph_signature(const ConfData& cd) const;
-    void run_conf_graph(ConfData& cd, ConfGraph& g);
+    void run_conf_graph(ConfData* const* cds, int nb, ConfGraph& g);
 };
 
 }  // namespace mtb

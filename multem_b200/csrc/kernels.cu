@@ -178,8 +178,7 @@ __global__ void __launch_bounds__(SPLAT_THREADS) splat_kernel(SplatArgs a, int i
                             // the interval of unrolledBinarySearch_c_nR (src/cgpu_fcns.cuh:1498-1518):
                             // the largest i0 in [0, nR-2] with T[i0] <= R2 (0 below the first knot),
                             // from the logarithmic guess and exact comparisons with the knots
-                            int i0 = (int)fmaxf(__fmul_rn(__log2f(R2) - lg0, lgs), 0.0f);
-                            i0 = i0 < nR - 2 ? i0 : nR - 2;
+                            int i0 = (int)fminf(fmaxf(__fmul_rn(__log2f(R2) - lg0, lgs), 0.0f), (float)(nR - 2));
                             while (i0 > 0 && R2 < T[i0]) i0--;
                             while (i0 < nR - 2 && !(R2 < T[i0 + 1])) i0++;
                             const float dx = __fsub_rn(R2, T[i0]);

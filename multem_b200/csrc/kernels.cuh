@@ -44,6 +44,8 @@ struct RowArgs {
     const float2* in;
     float2* out;
     const float2* trans;   // [nx*ny] of the slice
+    size_t trans_stride;   // elements between the transmission functions of consecutive waves of the
+                           // batch (0: one function shared by every wave, as for STEM probes)
     int nx;                // lines per probe
     int nprobe;
     float scale;

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(LineGeom<NY>::THREADS, LinePlan<NY>::B) rows_k
 #pragma unroll
             for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::RL>(i, t)] = cscale(x[i], a.scale);
         } else {
-            const float2* Tr = a.trans + (size_t)ix * NY;
+            const float2* Tr = a.trans + (size_t)b * a.trans_stride + (size_t)ix * NY;
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(&Tr[reg_pos<NY, G::RL>(i, t)]));
             line_fft<NY, true, -1>(x, buf, twF, t, Sync{});
@@ -785,7 +785,8 @@ static bool rows_pipe_try(const RowArgs& a, int grid_ctas, cudaStream_t s) {
     using S = RowPipeShape<NY, V>;
     using RP = RowPipe<NY, S::GT, S::NG, S::PM>;
     if constexpr (RP::OK && MODE != ROW_FIRST_ONE) {
-        if (a.nprobe % S::NG != 0) return false;
+        // the resident transmission rows are shared by every wave of the batch
+        if (a.nprobe % S::NG != 0 || (a.trans_stride != 0 && MODE != ROW_INVERSE)) return false;
         auto kern = rows_pipe_kernel<NY, MODE, S::GT, S::NG, S::PM>;
         static const int cap = max_ctas(kern, S::GT * S::NG, RP::SMEM);
         const int units = (a.nx / RP::LPC) * a.nprobe / S::NG;

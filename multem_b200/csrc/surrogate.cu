@@ -296,10 +296,10 @@ Workspace& workspace(size_t bytes) {
         MTB_CUDA(cudaMemset(w.err, 0, sizeof(int)));
     }
     if (w.bytes < bytes) {
+        const size_t nb = std::max(bytes, 2 * w.bytes);  // grow geometrically
         if (w.p) mtb::dev_free(w.p, w.dev);  // waits for the device: earlier calls may still use it
         w.p = nullptr;
         w.bytes = 0;
-        const size_t nb = std::max(bytes, 2 * w.bytes);
         w.p = static_cast<unsigned char*>(mtb::dev_alloc(nb, &w.dev));
         w.bytes = nb;
     }
