@@ -64,6 +64,13 @@ struct WarpSync {
 struct BlockSync {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
+// Barrier over the T threads of group `grp` (named barrier 1 + grp; barrier 15 is the row pass's
+// CTA-wide barrier).
+template <int T>
+struct GroupSync {
+    int grp;
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(T) : "memory"); }
+};
 
 // ---------------------------------------------------------------------------------------------
 // Contiguous-line pass. LinePlan<NY>::T threads; each line of NY points is owned by TPL = NY/E
@@ -83,7 +90,10 @@ __global__ void __launch_bounds__(LineGeom<NY>::THREADS, LinePlan<NY>::B) rows_k
     float2* buf = lines + li * G::LS;
     const int groups = a.nx / LPC;
     const int items = groups * a.nprobe;
-    using Sync = typename std::conditional<(TPL <= 32), WarpSync, BlockSync>::type;
+    // a line's exchanges synchronise only its own threads: one warp, or a named barrier per line
+    static_assert(TPL <= 32 || LPC <= 15, "one named barrier per line");
+    using Sync = typename std::conditional<(TPL <= 32), WarpSync, GroupSync<TPL>>::type;
+    const Sync sync{li};
 
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
         const int b = item / groups;
@@ -93,7 +103,7 @@ __global__ void __launch_bounds__(LineGeom<NY>::THREADS, LinePlan<NY>::B) rows_k
         if constexpr (MODE == ROW_STEP || MODE == ROW_INVERSE) {
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = a.in[off + reg_pos<NY, G::R1>(i, t)];
-            line_fft<NY, false, +1>(x, buf, twI, t, Sync{});
+            line_fft<NY, false, +1>(x, buf, twI, t, sync);
         } else if constexpr (MODE == ROW_FIRST_REAL) {
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = a.in[off + reg_pos<NY, G::RL>(i, t)];
@@ -108,7 +118,7 @@ __global__ void __launch_bounds__(LineGeom<NY>::THREADS, LinePlan<NY>::B) rows_k
             const float2* Tr = a.trans + (size_t)b * a.trans_stride + (size_t)ix * NY;
 #pragma unroll
             for (int i = 0; i < E; i++) x[i] = cmul(x[i], __ldg(&Tr[reg_pos<NY, G::RL>(i, t)]));
-            line_fft<NY, true, -1>(x, buf, twF, t, Sync{});
+            line_fft<NY, true, -1>(x, buf, twF, t, sync);
 #pragma unroll
             for (int i = 0; i < E; i++) a.out[off + reg_pos<NY, G::R1>(i, t)] = x[i];
         }
@@ -372,13 +382,6 @@ __device__ __forceinline__ void tensor_load_3d(void* dst, const CUtensorMap* map
         : "memory");
 }
 
-// Barrier over the T threads of group `grp` (named barrier 1 + grp; barrier 15 is the row pass's
-// CTA-wide barrier).
-template <int T>
-struct GroupSync {
-    int grp;
-    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(T) : "memory"); }
-};
 
 constexpr size_t kPipeSmemMax = 232448 - 2048;  // opt-in shared memory per CTA less static use
 
