@@ -164,3 +164,31 @@ def test_output_struct_layout(tmp_path, case, compress):
             assert set(data.dtype.names) == {"m2psi_tot", "m2psi_coh"}
             np.testing.assert_array_equal(e["m2psi_tot"], out["data"][it]["m2psi_tot"])
             np.testing.assert_array_equal(e["m2psi_coh"], out["data"][it]["m2psi_coh"])
+
+
+@pytest.mark.parametrize("compress", [False, True])
+def test_damaged_files_are_rejected_cleanly(tmp_path, compress):
+    """Truncated or corrupted files end in MT_ERR_INVALID_ARG (or, where the damage leaves a
+    readable struct, a normal read), never in a crash."""
+    p = _cases()["ew"]
+    good = tmp_path / "good.mat"
+    sio.savemat(good, {"prms": p.to_struct()}, format="5", do_compression=compress)
+    data = good.read_bytes()
+    rng = np.random.default_rng(11)
+    bad = tmp_path / "bad.mat"
+    cuts = sorted(set(int(c) for c in rng.integers(129, len(data), 12))) + [130, 136, 200]
+    for cut in cuts:
+        bad.write_bytes(data[:cut])
+        try:
+            api.MatInput(bad).close()
+        except capi.MtError as e:
+            assert e.status == 1
+    for _ in range(20):
+        b = bytearray(data)
+        for i in rng.integers(128, len(b), 4):
+            b[i] = int(rng.integers(0, 256))
+        bad.write_bytes(bytes(b))
+        try:
+            api.MatInput(bad).close()
+        except capi.MtError as e:
+            assert e.status == 1
