@@ -4,7 +4,8 @@ With several configurations the engine runs up to eight of them per pass (each w
 transmission functions) and adds their outputs thickness by thickness in configuration order, so
 the results must equal those of one configuration at a time (MTB_EW_BATCH=1) bit for bit: for
 real- and Fourier-space exit waves with a tilted beam, several thicknesses, the band-width limit,
-electron diffraction with the coherent contribution and an HRTEM image with it; over batches that
+electron diffraction with the coherent contribution, an HRTEM image with it, and displacements
+drawn on the GPU; over batches that
 divide the configurations and batches that do not (11 configurations: 8 + 3); through the graphs
 of mt_multislice_run and through direct launches (tests/test_gpu_batch.py covers the recorded runs
 of mt_multislice_run_batch)."""
@@ -24,8 +25,10 @@ def _cases():
     ed.pn_coh_contrib = 1
     hr = hrtem_coherent_si001()
     hr.pn_coh_contrib = 1
+    dev = ew_tilt_si001()
+    dev.pn_rng = 1  # displacements drawn on the GPU for every configuration of the batch
     return {"ewrs_tilt_3thick": ew, "ewfs_tilt": ewfs_tilt_si001(), "ewrs_bwl": ew_bwl_si001(), "ed_coh": ed,
-            "hrtem_coh": hr}
+            "hrtem_coh": hr, "ewrs_device_rng": dev}
 
 
 def _arrays(out):
@@ -34,7 +37,7 @@ def _arrays(out):
 
 
 @pytest.mark.parametrize("nconf", [5, 11])
-@pytest.mark.parametrize("name", ["ewrs_tilt_3thick", "ewfs_tilt", "ewrs_bwl", "ed_coh", "hrtem_coh"])
+@pytest.mark.parametrize("name", ["ewrs_tilt_3thick", "ewfs_tilt", "ewrs_bwl", "ed_coh", "hrtem_coh", "ewrs_device_rng"])
 def test_batched_configurations_match_one_at_a_time(name, nconf, monkeypatch):
     p = _cases()[name]
     p.pn_model, p.pn_nconf = 3, nconf
