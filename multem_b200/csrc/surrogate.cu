@@ -42,29 +42,24 @@ __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162f
 
 // A[m][k] = in[b][c][y+ky-1][x+kx-1] for k = c*9 + ky*3 + kx < 9*C (zero outside the image and for
 // the padding k in [9C, ldk)); with `mask`, zero where mask (same layout as in) is not positive.
-// One CTA of 32 x 8 threads per tile of 32 pixels x 64 k: the gather reads consecutive pixels with
-// consecutive threads, the tile is transposed through shared memory, and each pixel's 64 k values
-// leave as 16-byte stores. grid: (ceil(M/32), ceil(ldk/64)).
+// Thread (m, chunk) gathers the 8 values k = 8*chunk .. 8*chunk+7 of pixel m with independent loads
+// (the 32 lanes of a warp take 32 consecutive pixels: each load is contiguous across the warp) and
+// stores them as one 16-byte vector. grid: (ceil(M/32), ceil(ldk/64)), block 32 x 8.
 __global__ void __launch_bounds__(256) im2col_kernel(const __nv_bfloat16* __restrict__ in,
                                                      const __nv_bfloat16* __restrict__ mask,
                                                      __nv_bfloat16* __restrict__ A, int B, int C, int H, int W,
                                                      int ldk) {
-    __shared__ __nv_bfloat16 tile[64][34];
     const int HW = H * W, M = B * HW, K = 9 * C;
-    const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int m = m0 + tx;
-    int b = 0, y = 0, x = 0;
-    if (m < M) {
-        b = m / HW;
-        const int yx = m - b * HW;
-        y = yx / W;
-        x = yx - y * W;
-    }
-    for (int kk = ty; kk < 64; kk += 8) {
-        const int k = k0 + kk;
+    const int m = blockIdx.x * 32 + threadIdx.x;
+    const int k0 = blockIdx.y * 64 + threadIdx.y * 8;
+    if (m >= M || k0 >= ldk) return;  // ldk and k0 are multiples of 8: the 8 values stay in the row
+    const int b = m / HW, yx = m - b * HW, y = yx / W, x = yx - y * W;
+    __align__(16) __nv_bfloat16 v8[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int k = k0 + j;
         __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
-        if (m < M && k < K) {
+        if (k < K) {
             const int c = k / 9, q = k - 9 * c;
             const int yy = y + q / 3 - 1, xx = x + q % 3 - 1;
             if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
@@ -73,17 +68,9 @@ __global__ void __launch_bounds__(256) im2col_kernel(const __nv_bfloat16* __rest
                 if (mask && !(bf(mask[idx]) > 0.0f)) v = __float2bfloat16_rn(0.0f);
             }
         }
-        tile[kk][tx] = v;
+        v8[j] = v;
     }
-    __syncthreads();
-    const int t = ty * 32 + tx, r = t / 8, ch = t % 8;
-    const int mr = m0 + r, k = k0 + ch * 8;
-    if (mr < M && k < ldk) {  // ldk and k are multiples of 8: the 8 values stay inside the row
-        __align__(16) __nv_bfloat16 v8[8];
-#pragma unroll
-        for (int j = 0; j < 8; j++) v8[j] = tile[ch * 8 + j][r];
-        *reinterpret_cast<uint4*>(A + (size_t)mr * ldk + k) = *reinterpret_cast<const uint4*>(v8);
-    }
+    *reinterpret_cast<uint4*>(A + (size_t)m * ldk + k0) = *reinterpret_cast<const uint4*>(v8);
 }
 
 // X[k][p] = in[b][c][y+ky-1][x+kx-1] (the transposed im2col, p = (b, y, x)) for k = c*9 + q < 9C,
