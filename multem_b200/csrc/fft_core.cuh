@@ -83,8 +83,51 @@ constexpr double cx_trig2pi(long long k, long long n, bool c) {
 // ---------------------------------------------------------------------------------------------
 // complex helpers (float2 = (re, im))
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex sums as one packed FP32 instruction each (add/sub .rn.f32x2 on a register pair): the
+// same two IEEE round-to-nearest sums as the scalar form, in half the issue slots.
+__device__ __forceinline__ unsigned long long pack2(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long r) {
+    float2 d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+    return d;
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(d);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(d);
+}
+
+// a + (DIR*i)^Q * b. The quarter turns swap the components of b, so they stay two scalar sums
+// (the same roundings as adding the rotated value); Q = 0 and 2 are packed sums.
+template <int Q, int DIR>
+__device__ __forceinline__ float2 cadd_rot(float2 a, float2 b) {
+    constexpr int q = ((Q % 4) + 4) % 4;
+    if constexpr (q == 0) {
+        return cadd(a, b);
+    } else if constexpr (q == 2) {
+        return csub(a, b);
+    } else if constexpr ((q == 1) == (DIR > 0)) {  // +i * b = (-b.y, b.x)
+        return make_float2(a.x - b.y, a.y + b.x);
+    } else {                                       // -i * b = (b.y, -b.x)
+        return make_float2(a.x + b.y, a.y - b.x);
+    }
+}
+
+// Quarter turns Q (exp(DIR*2*pi*i*K/R) = (DIR*i)^Q) of a compile-time twiddle, or -1.
+template <int K, int R>
+constexpr int twiddle_quarter() {
+    constexpr int k = ((K % R) + R) % R;
+    return (4 * k) % R == 0 ? (4 * k) / R : -1;
+}
 // Complex products with their rounding fixed (one rounded product, one fused multiply-add per
 // component), so that every kernel variant computes bit-identical results whatever the compiler
 // would otherwise contract.
@@ -133,6 +176,20 @@ __device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
     c = csub(m, s);
 }
 
+// a +- w * b for the compile-time twiddle w = exp(DIR*2*pi*i*K/R); quarter turns cost no product.
+template <int K, int R, int DIR>
+__device__ __forceinline__ void tw_butterfly(float2 a, float2 b, float2& p, float2& m) {
+    constexpr int q = twiddle_quarter<K, R>();
+    if constexpr (q >= 0) {
+        p = cadd_rot<q, DIR>(a, b);
+        m = cadd_rot<q + 2, DIR>(a, b);
+    } else {
+        const float2 t = twiddle_const<K, R, DIR>(b);
+        p = cadd(a, t);
+        m = csub(a, t);
+    }
+}
+
 // In-register DFT of length R (natural order in and out), dir = -1 forward, +1 inverse,
 // unnormalised. Radix-4 / radix-3 / radix-2 decimation in time, fully unrolled; trivial twiddles
 // folded.
@@ -148,11 +205,10 @@ __device__ __forceinline__ void dft(float2* v) {
     } else if constexpr (R == 4) {
         float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
         float2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
-        float2 jt3 = twiddle_const<1, 4, DIR>(t3);
         v[0] = cadd(t0, t2);
         v[2] = csub(t0, t2);
-        v[1] = cadd(t1, jt3);
-        v[3] = csub(t1, jt3);
+        v[1] = cadd_rot<1, DIR>(t1, t3);
+        v[3] = cadd_rot<3, DIR>(t1, t3);
     } else if constexpr (R % 4 == 0) {
         // radix-4 DIT: four interleaved sub-DFTs of length R/4
         constexpr int Q = R / 4;
@@ -171,14 +227,13 @@ __device__ __forceinline__ void dft(float2* v) {
         static_for<0, Q>([&](auto kc) {
             constexpr int k = decltype(kc)::value;
             float2 bb = twiddle_const<k, R, DIR>(b[k]);
-            float2 cc = twiddle_const<2 * k, R, DIR>(c[k]);
-            float2 dd = twiddle_const<3 * k, R, DIR>(d[k]);
-            float2 s0 = cadd(a[k], cc), s1 = csub(a[k], cc);
-            float2 s2 = cadd(bb, dd), s3 = twiddle_const<1, 4, DIR>(csub(bb, dd));
+            float2 s0, s1, s2, d3;
+            tw_butterfly<2 * k, R, DIR>(a[k], c[k], s0, s1);
+            tw_butterfly<3 * k, R, DIR>(bb, d[k], s2, d3);
             v[k] = cadd(s0, s2);
             v[k + 2 * Q] = csub(s0, s2);
-            v[k + Q] = cadd(s1, s3);
-            v[k + 3 * Q] = csub(s1, s3);
+            v[k + Q] = cadd_rot<1, DIR>(s1, d3);
+            v[k + 3 * Q] = cadd_rot<3, DIR>(s1, d3);
         });
     } else if constexpr (R % 3 == 0) {
         // radix-3 DIT: X[k + m*Q] = DFT3 over r of w_R^(k*r) * S_r[k], S_r = DFT_Q of v[3i + r]
@@ -214,9 +269,7 @@ __device__ __forceinline__ void dft(float2* v) {
         dft<H, DIR>(o);
         static_for<0, H>([&](auto kc) {
             constexpr int k = decltype(kc)::value;
-            float2 t = twiddle_const<k, R, DIR>(o[k]);
-            v[k] = cadd(e[k], t);
-            v[k + H] = csub(e[k], t);
+            tw_butterfly<k, R, DIR>(e[k], o[k], v[k], v[k + H]);
         });
     }
 }
