@@ -305,8 +305,7 @@ mt_status mt_engine_pass_variants(mt_engine* eng, int* variants);
 /* The autotuner's full choice for the engine's grid (no counterpart in the reference, whose FFT
  * shapes come from cuFFT plans, src/fft.cuh:364-478): the variant of the row and of the column
  * pass of the slice step (0 per-thread loads, 1 bulk-copy fed, 2 and 3 bulk-copy fed in the two
- * alternative pipeline shapes: narrower groups, and early issue with full exchange buffers; for the
- * column pass also 4: each line's threads in one warp set, on swizzled landing tiles) and the
+ * alternative pipeline shapes: narrower groups, and early issue with full exchange buffers) and the
  * probes per launch; valid after a run. */
 mt_status mt_engine_tuning(mt_engine* eng, int* rows_variant, int* cols_variant, int* probes_per_launch);
 /* Device timing (no counterpart in the reference): with timing on, each run records CUDA events on

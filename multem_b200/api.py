@@ -253,8 +253,7 @@ class Engine:
 
     def tuning(self) -> dict:
         """The autotuner's choice: row and column pass variant (0 per-thread loads, 1 bulk-copy fed,
-        2 and 3 bulk-copy fed in the alternative pipeline shapes, 4 for the column pass: each line's
-        threads in one warp set) and probes per launch."""
+        2 and 3 bulk-copy fed in the alternative pipeline shapes) and probes per launch."""
         r, c, b = C.c_int(), C.c_int(), C.c_int()
         capi.check(self.lib.mt_engine_tuning(self.h, C.byref(r), C.byref(c), C.byref(b)))
         return {"rows": r.value, "cols": c.value, "probes_per_launch": b.value}

@@ -985,9 +985,8 @@ Engine::Tuning Engine::tune_passes(int nprobe, ConfData& cd) {
     ca.det_w = col_det_width(nx);
     ca.wait_ns = wait_ns_;
     const int step = COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE;
-    // variant v: 0 per-thread loads, 1 bulk-copy fed, 2, 3 (and 4 for columns) bulk-copy fed in the
-    // alternative pipeline shapes 1, 2 (and 3) (a shape that does not fit this length runs the
-    // default one)
+    // variant v: 0 per-thread loads, 1 bulk-copy fed, 2 and 3 bulk-copy fed in the alternative
+    // pipeline shapes 1 and 2 (a shape that does not fit this length runs the default one)
     auto rows_t = [&](int v, int nb) {
         ra.nprobe = nb;
         ra.err = v ? d_err_.p : nullptr;
@@ -1000,17 +999,15 @@ Engine::Tuning Engine::tune_passes(int nprobe, ConfData& cd) {
         ca.shape = v > 1 ? v - 1 : 0;
         return time_of([&] { launch_cols(nx, step, ca, 0, stream_); });
     };
-    // rows: per-thread loads and three pipeline shapes; columns: one more shape (each line's
-    // threads in one warp set)
-    constexpr int NVR = 4, NVC = 5;
-    float tr[NVR], tc[NVC];
-    for (int v = 0; v < NVC; v++) {
-        if (v < NVR) tr[v] = rows_t(v, nprobe);
+    constexpr int NV = 4;
+    float tr[NV], tc[NV];
+    for (int v = 0; v < NV; v++) {
+        tr[v] = rows_t(v, nprobe);
         tc[v] = cols_t(v, nprobe);
     }
     int vr = 0, vc = 0;
-    for (int v = 1; v < NVC; v++) {
-        if (v < NVR && tr[v] < tr[vr]) vr = v;
+    for (int v = 1; v < NV; v++) {
+        if (tr[v] < tr[vr]) vr = v;
         if (tc[v] < tc[vc]) vc = v;
     }
     Tuning t{(vr ? 1 : 0) | (vc ? 2 : 0), (vr > 1 ? vr - 1 : 0) | ((vc > 1 ? vc - 1 : 0) << 2), nprobe};

@@ -30,8 +30,7 @@ long long launches_issued() { return g_launches; }
 void note_launch() { g_launches++; }
 void add_launches(long long n) { g_launches += n; }
 
-void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr,
-                     int swizzle_bytes) {
+void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr) {
     static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
@@ -45,10 +44,7 @@ void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int 
     const cuuint32_t box[3] = {(cuuint32_t)(2 * w), (cuuint32_t)boxr, 1};
     const cuuint32_t estride[3] = {1, 1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides, box,
-                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                              swizzle_bytes == 128  ? CU_TENSOR_MAP_SWIZZLE_128B
-                              : swizzle_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
-                                                    : CU_TENSOR_MAP_SWIZZLE_NONE,
+                              estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the column-pass tile map");
 }

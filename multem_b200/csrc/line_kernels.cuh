@@ -588,36 +588,23 @@ struct RowPipeShape<NY, 2> {
 //   PM 0: (lengths without a half-line exchange, 1024) the slot doubles as the full exchange
 //         buffer and the next tile is issued once the group's last exchange read is done; the other
 //         groups keep the copy engine busy meanwhile.
-template <int NX, int GT, int NG, int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0,
-          int WPL = GT / 32>
+template <int NX, int GT, int NG, int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0>
 struct ColPipe {
     using G = LineGeom<NX>;
     static constexpr int PM_V = PM;
     static constexpr bool EARLY = PM != 0;
     static constexpr int W = GT / G::TPL;
-    // Thread layout: a line's TPL threads sit in WPL warps (GT/32: spread over the whole group, whose
-    // barrier then orders every exchange; fewer: a set of WPL warps owns CPW whole lines and
-    // synchronises its exchanges by itself). Lane l of warp k of a set holds column l % CPW and line
-    // thread k*(32/CPW) + l/CPW. With fewer than GT/32 warps per line a warp reads up to 32/CPW rows of
-    // its landing tile at once, so the tile lands swizzled (128-byte rows of 16 columns, or 64-byte
-    // rows of 8) to keep those reads free of bank conflicts.
-    static constexpr int CPW = 32 * WPL / G::TPL;
-    static constexpr bool SWZ = WPL < GT / 32;
-    static constexpr int SWZ_BYTES = SWZ ? W * (int)sizeof(float2) : 0;
     static constexpr int LSH = PM == 1 ? HalfLineSmem<NX>::value : G::LS;  // exchange buffer per column
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
     static constexpr size_t LAND0 = (size_t)W * NX;
     static constexpr size_t LAND1 = EARLY ? LAND0 : ((size_t)W * G::LS > LAND0 ? (size_t)W * G::LS : LAND0);
-    // slots on 128-byte boundaries (bulk-copy targets), 1024-byte ones for swizzled tiles
-    static constexpr size_t LAND = SWZ ? (LAND1 + 127) / 128 * 128 : (LAND1 + 15) / 16 * 16;
+    static constexpr size_t LAND = (LAND1 + 15) / 16 * 16;  // slots on 128-byte boundaries (bulk-copy targets)
     static constexpr size_t HBUF = EARLY ? (size_t)W * LSH : 0;
     static constexpr size_t SMEM = sizeof(float2) * (TW + NX + NG * LAND + NG * HBUF);
     // rows per bulk-copy box: the boxes must tile the NX rows exactly (a box reaching past NX would
     // write past the slot and count bytes the barrier does not expect)
     static constexpr int BOXR = (NX <= 256) ? NX : (NX % 256 == 0) ? 256 : (NX % 128 == 0) ? 128 : 0;
     static constexpr bool OK = (PM != 1 || (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)) &&
-                               ((32 * WPL) % G::TPL == 0) && (CPW >= 1) && ((GT / 32) % WPL == 0) &&
-                               (!SWZ || ((W == 16 || W == 8) && ((TW + NX) * sizeof(float2)) % 1024 == 0)) &&
                                (BOXR > 0) && (NX % (BOXR > 0 ? BOXR : 1) == 0) && ((size_t)NX * W <= LAND) &&
                                (GT % G::TPL == 0) && (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) &&
                                (HBUF % 2 == 0) && SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
@@ -627,42 +614,21 @@ struct ColPipe {
 // autotuner may pick for the slice step: 4 groups of 128 threads (narrower tiles), and groups of
 // 128 threads in early-issue mode with full exchange buffers, as many (4, 3 or 2) as shared memory
 // holds.
-#ifndef MTB_COL_WPL
-#define MTB_COL_WPL 2
-#endif
 template <int NX, int V = 0>
 struct ColPipeShape {
     static constexpr int GT = V == 0 ? 256 : 128, NG = V == 0 ? 2 : 4;
     static constexpr int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0;
-    static constexpr int WPL = GT / 32;
 };
 template <int NX>
 struct ColPipeShape<NX, 2> {
     static constexpr int GT = 128, PM = 2;
     static constexpr int NG = ColPipe<NX, 128, 4, 2>::OK ? 4 : ColPipe<NX, 128, 3, 2>::OK ? 3 : 2;
-    static constexpr int WPL = GT / 32;
-};
-// shape 3: the default groups with each line's threads in one warp set (swizzled landing tiles)
-// (MTB_COL_WPL warps per line: 2 by default)
-template <int NX>
-struct ColPipeShape<NX, 3> {
-    static constexpr int GT = 256, NG = 2;
-    static constexpr int PM = (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK) ? 1 : 0;
-    static constexpr int WPL = MTB_COL_WPL;
 };
 
-// Barrier over the 32*WPL threads of one warp set (named barriers 3 and up; 1 + group is the
-// group's barrier).
-template <int WPL>
-struct SetSync {
-    int id;
-    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(32 * WPL) : "memory"); }
-};
-
-template <int NX, int FLAGS, int LDY, int GT, int NG, int PM, int WPL>
+template <int NX, int FLAGS, int LDY, int GT, int NG, int PM>
 __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const __grid_constant__ CUtensorMap map) {
     using G = LineGeom<NX>;
-    using P = ColPipe<NX, GT, NG, PM, WPL>;
+    using P = ColPipe<NX, GT, NG, PM>;
     constexpr bool EARLY = PM != 0, HALF = PM == 1;
     constexpr int E = G::E, W = P::W, NWARP = GT / 32;
     constexpr bool PROP = FLAGS & COL_PROP, DET = FLAGS & COL_DETECT;
@@ -681,9 +647,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     float2* s_px = sm + P::TW;
     float2* land0 = s_px + NX;  // NG landing buffers, [row][W] each
     const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
-    constexpr int CPW = P::CPW, NSET = GT / 32 / WPL;
-    const int wset = gtid / (32 * WPL), wk = (gtid / 32) % WPL, lane = gtid % 32;
-    const int c = wset * CPW + lane % CPW, t = wk * (32 / CPW) + lane / CPW;
+    const int c = gtid % W, t = gtid / W;
     float2* land = land0 + grp * P::LAND;
     float2* buf = EARLY ? land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH : land + (size_t)c * G::LS;
     (void)HALF;
@@ -692,11 +656,6 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     }
     if (threadIdx.x == 0) {
         s_skip = err_set(a.err);  // an earlier pass timed out: the CTA returns (one decision for all)
-        if (P::SWZ && (smem_u32(land0) & 1023u)) {
-            // swizzled tiles need 1024-byte aligned landing buffers: refuse rather than misread
-            atomicOr(a.err, 1);
-            s_skip = 1;
-        }
         for (int i = 0; i < NG; i++) mbar_init(&full[i], 1);
         mbar_fence_init();
     }
@@ -726,11 +685,6 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
 
     using GSync = typename std::conditional<(GT == 32), WarpSync, GroupSync<GT>>::type;
     const GSync gsync{grp};
-    // the exchanges of a line synchronise the warps that hold it: the group, a warp set or a warp
-    static_assert(3 + NG * NSET <= 15 || WPL == 1 || WPL == GT / 32, "named barriers for the warp sets");
-    using XSync = typename std::conditional<(WPL == GT / 32), GSync,
-                                            typename std::conditional<(WPL == 1), WarpSync, SetSync<WPL>>::type>::type;
-    const XSync xsync{WPL == GT / 32 ? grp : 3 + grp * NSET + wset};
     for (int k = grp; k < K; k += NG) {
         const int item = blockIdx.x + k * gridDim.x;
         const int b = item / tiles, ct = item % tiles;
@@ -739,25 +693,14 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
         float2* dst = a.out + off;
         mbar_wait(&full[grp], (unsigned)(k / NG) & 1u, a.err, a.wait_ns);
         float2 x[E];
-        if constexpr (P::SWZ) {
-            // swizzled tile: the 16-byte chunk j of row r sits at chunk j ^ (r % 8) (128-byte rows)
-            // or j ^ ((r / 2) % 4) (64-byte rows)
 #pragma unroll
-            for (int i = 0; i < E; i++) {
-                const int r = reg_pos<NX, G::R1>(i, t);
-                const int sw = W == 16 ? (r & 7) : ((r >> 1) & 3);
-                x[i] = land[(size_t)r * W + ((((c >> 1) ^ sw) << 1) | (c & 1))];
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < E; i++) x[i] = land[(size_t)reg_pos<NX, G::R1>(i, t) * W + c];
-        }
+        for (int i = 0; i < E; i++) x[i] = land[(size_t)reg_pos<NX, G::R1>(i, t) * W + c];
         gsync();  // the whole group has read its landing buffer
         if constexpr (EARLY) {
             if (gtid == 0 && k + NG < K) issue(k + NG);
         }
-        if constexpr (HALF) line_fft_half<NX, false, -1>(x, buf, twP, t, xsync);
-        else line_fft<NX, false, -1>(x, buf, twP, t, xsync);
+        if constexpr (HALF) line_fft_half<NX, false, -1>(x, buf, twP, t, gsync);
+        else line_fft<NX, false, -1>(x, buf, twP, t, gsync);
         if constexpr (PROP) {
             const float2 py = a.Py[iy];
 #pragma unroll
@@ -791,9 +734,9 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
         }
         if constexpr (INV) {
             if constexpr (HALF) {
-                line_fft_half<NX, true, +1>(x, buf, twR, t, xsync);
+                line_fft_half<NX, true, +1>(x, buf, twR, t, gsync);
             } else {
-                line_fft<NX, true, +1>(x, buf, twR, t, xsync);
+                line_fft<NX, true, +1>(x, buf, twR, t, gsync);
                 if constexpr (!EARLY) {
                     gsync();  // every exchange read of the slot is done
                     if (gtid == 0 && k + NG < K) issue(k + NG);
@@ -818,8 +761,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
 
 // Tensor map for cols_pipe_kernel over a probe batch at `base` (cuTensorMapEncodeTiled through
 // the runtime's driver entry point, so the library needs no link to the driver library).
-void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr,
-                     int swizzle_bytes = 0);
+void encode_tile_map(CUtensorMap* map, const float2* base, int nx, int ldy, int nprobe, int w, int boxr);
 
 // ---------------------------------------------------------------------------------------------
 // launch helpers (the per-kernel occupancy caps are function-local statics, initialised once and
@@ -901,15 +843,15 @@ void rows_dispatch_mode(RowMode mode, const RowArgs& a, int grid_ctas, cudaStrea
 template <int NX, int FLAGS, int LDY, int V>
 static bool cols_pipe_try(const ColArgs& a, int grid_ctas, cudaStream_t s) {
     using S = ColPipeShape<NX, V>;
-    using CP = ColPipe<NX, S::GT, S::NG, S::PM, S::WPL>;
+    using CP = ColPipe<NX, S::GT, S::NG, S::PM>;
     if constexpr (CP::OK && (FLAGS & COL_LOAD)) {
-        auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG, S::PM, S::WPL>;
+        auto kern = cols_pipe_kernel<NX, FLAGS, LDY, S::GT, S::NG, S::PM>;
         static const int cap = max_ctas(kern, S::GT * S::NG, CP::SMEM);
         const int items = (a.ny / CP::W) * a.nprobe;
         int grid = grid_ctas > 0 ? grid_ctas : cap;
         if (grid > items) grid = items;
         CUtensorMap map;
-        encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP::W, CP::BOXR, CP::SWZ_BYTES);
+        encode_tile_map(&map, a.in, NX, a.ny, a.nprobe, CP::W, CP::BOXR);
         kern<<<grid, S::GT * S::NG, CP::SMEM, s>>>(a, map);
         note_launch();
         MTB_CUDA(cudaGetLastError());
@@ -927,7 +869,6 @@ static void cols_launch_ld(const ColArgs& a, int grid_ctas, cudaStream_t s) {
         if constexpr (FLAGS == (COL_LOAD | COL_PROP | COL_INVERSE | COL_STORE)) {
             if (a.shape == 1 && cols_pipe_try<NX, FLAGS, LDY, 1>(a, grid_ctas, s)) return;
             if (a.shape == 2 && cols_pipe_try<NX, FLAGS, LDY, 2>(a, grid_ctas, s)) return;
-            if (a.shape == 3 && cols_pipe_try<NX, FLAGS, LDY, 3>(a, grid_ctas, s)) return;
         }
         if (cols_pipe_try<NX, FLAGS, LDY, 0>(a, grid_ctas, s)) return;
     }

@@ -29,7 +29,7 @@ def _stem(p, pipe, monkeypatch):
     return np.stack([np.stack(d["image_tot"]) for d in r["data"]])
 
 
-@pytest.mark.parametrize("nx,ns", [(512, 4), (512, 3), (128, 4), (256, 4), (384, 4), (1024, 4)])
+@pytest.mark.parametrize("nx,ns", [(512, 4), (512, 3), (64, 4), (128, 4), (256, 4), (384, 4), (1024, 4)])
 def test_stem_pipelined_matches_per_thread_kernels(nx, ns, monkeypatch):
     p = specimens.stem_srtio3(nx=nx, ny=nx, na=4, nb=4, nc=6, ns=ns, nconf=1, seed=3)
     ref = _stem(p, 0, monkeypatch)
@@ -60,12 +60,11 @@ def test_exit_wave_pipelined_matches_per_thread_kernels(nx, monkeypatch):
     np.testing.assert_array_equal(out[3], out[0])
 
 
-@pytest.mark.parametrize("shape", [1, 2, 3])
-@pytest.mark.parametrize("nx", [128, 256, 384, 512, 1024, 2048])
+@pytest.mark.parametrize("shape", [1, 2])
+@pytest.mark.parametrize("nx", [64, 128, 256, 384, 512, 1024, 2048])
 def test_alternative_pipeline_shapes_match(nx, shape, monkeypatch):
     """The autotuner's alternative pipeline shapes of the slice step (shape 1: one-warp row groups,
-    4 x 128 column groups; shape 2: early issue with full exchange buffers; shape 3, columns only:
-    each line's threads in one warp set, on 128-byte swizzled landing tiles) give the waves of the
+    4 x 128 column groups; shape 2: early issue with full exchange buffers) give the waves of the
     per-thread-load kernels bit for bit."""
     p = specimens.stem_srtio3(nx=nx, ny=nx, na=4, nb=4, nc=6 if nx < 2048 else 2, ns=4, nconf=1, seed=3)
     ref = _stem(p, 0, monkeypatch)
@@ -84,5 +83,5 @@ def test_autotuner_reports_its_choice():
     e.run()
     t = e.tuning()
     e.close()
-    assert t["rows"] in (0, 1, 2, 3) and t["cols"] in (0, 1, 2, 3, 4)
+    assert t["rows"] in (0, 1, 2, 3) and t["cols"] in (0, 1, 2, 3)
     assert t["probes_per_launch"] in (128, 256)
