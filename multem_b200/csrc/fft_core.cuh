@@ -295,7 +295,7 @@ template <> struct LinePlan<2048> { static constexpr int E = 32, T = 256, B = 2,
 template <int N, bool REV, int S>
 struct StageRadix {
     static constexpr int NSTAGE = LinePlan<N>::NS;
-    static constexpr int value = LinePlan<N>::R[REV ? (NSTAGE - 1 - S) : S];
+    static constexpr int value = S < NSTAGE ? LinePlan<N>::R[REV ? (NSTAGE - 1 - S) : S] : 1;  // 1 past the last stage
 };
 
 // Product of the radices before stage s.
@@ -321,14 +321,18 @@ struct LineSmem {
 };
 
 // Per-stage twiddle table in shared memory: tw[(m*R + r)*TPL + t] = exp(-2*pi*i*r*k/(Ns*R)),
-// k = (t + TPL*m) % Ns. The inverse direction uses the conjugate.
+// k = (t + TPL*m) % Ns (N entries, one per thread and register), or, where the stage has fewer
+// distinct twiddles than points (Ns*R < N: the middle stage of a three-stage plan), the compact
+// tw[r*Ns + k] (Ns*R entries, 8x fewer for 2048 = 32 x 8 x 8; consecutive threads still read
+// consecutive entries). The inverse direction uses the conjugate.
 template <int N, bool REV, int S>
 struct TwTable {
     static constexpr int E = LinePlan<N>::E;
     static constexpr int TPL = N / E;
     static constexpr int R = StageRadix<N, REV, S>::value;
     static constexpr int NSV = StageNs<N, REV, S>::value;
-    static constexpr int SIZE = (NSV > 1) ? E * TPL : 0;  // = N entries
+    static constexpr bool COMPACT = (NSV > 1) && (NSV * R < E * TPL);
+    static constexpr int SIZE = (NSV > 1) ? (COMPACT ? NSV * R : E * TPL) : 0;
 };
 
 template <int N, bool REV, int S>
@@ -336,11 +340,17 @@ __device__ void fill_twiddles(float2* tw, int tid, int nthreads) {
     using TT = TwTable<N, REV, S>;
     if constexpr (TT::SIZE > 0) {
         for (int i = tid; i < TT::SIZE; i += nthreads) {
-            int t = i % TT::TPL;
-            int mr = i / TT::TPL;
-            int r = mr % TT::R;
-            int m = mr / TT::R;
-            int k = (t + TT::TPL * m) % TT::NSV;
+            int r, k;
+            if constexpr (TT::COMPACT) {
+                r = i / TT::NSV;
+                k = i % TT::NSV;
+            } else {
+                const int t = i % TT::TPL;
+                const int mr = i / TT::TPL;
+                const int m = mr / TT::R;
+                r = mr % TT::R;
+                k = (t + TT::TPL * m) % TT::NSV;
+            }
             double s, c;
             sincospi(-2.0 * (double)(r * k) / (double)(TT::NSV * TT::R), &s, &c);
             tw[i] = make_float2((float)c, (float)s);
@@ -358,9 +368,11 @@ __device__ __forceinline__ void stage_compute(float2* x, int t, const float2* tw
     static_for<0, E / R>([&](auto mc) {
         constexpr int m = decltype(mc)::value;
         if constexpr (NSV > 1) {
+            const int kc = (t + TPL * m) % NSV;  // the butterfly's k (compact tables)
+            (void)kc;
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                float2 w = tw[(m * R + r) * TPL + t];
+                float2 w = TwTable<N, REV, S>::COMPACT ? tw[r * NSV + kc] : tw[(m * R + r) * TPL + t];
                 x[m * R + r] = (DIR < 0) ? cmul(x[m * R + r], w) : cmulc(x[m * R + r], w);
             }
         }

@@ -407,11 +407,14 @@ struct RowPipe {
     static constexpr int LPC = GT / TPL;
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
     static constexpr size_t LAND = (size_t)LPC * NY;
-    static constexpr size_t SLOT = PM != 0 ? LAND : ((size_t)LPC * G::LS > LAND ? (size_t)LPC * G::LS : LAND);
+    // slots and per-group buffers in whole 16-byte units (bulk-copy targets follow them)
+    static constexpr size_t SLOT0 = PM != 0 ? LAND : ((size_t)LPC * G::LS > LAND ? (size_t)LPC * G::LS : LAND);
+    static constexpr size_t SLOT = (SLOT0 + 1) / 2 * 2;
     static constexpr size_t LBUF = PM == 1 ? (size_t)HalfLineSmem<NY>::value : (size_t)G::LS;  // per line
-    static constexpr size_t HBUF = PM != 0 ? (size_t)LPC * LBUF : 0;
+    static constexpr size_t HBUF = PM != 0 ? ((size_t)LPC * LBUF + 1) / 2 * 2 : 0;
     static constexpr size_t SMEM = sizeof(float2) * (TW + LAND + NG * SLOT + NG * HBUF);
     static constexpr bool OK = (GT % TPL == 0) && (GT % 32 == 0) && (SLOT % 2 == 0) && (HBUF % 2 == 0) &&
+                               (TW % 2 == 0) &&
                                SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14) &&
                                (PM != 1 || (HalfExchange<NY, false>::OK && HalfExchange<NY, true>::OK));
 };
@@ -606,6 +609,7 @@ struct ColPipe {
     static constexpr int BOXR = (NX <= 256) ? NX : (NX % 256 == 0) ? 256 : (NX % 128 == 0) ? 128 : 0;
     static constexpr bool OK = (PM != 1 || (HalfExchange<NX, false>::OK && HalfExchange<NX, true>::OK)) &&
                                (BOXR > 0) && (NX % (BOXR > 0 ? BOXR : 1) == 0) && ((size_t)NX * W <= LAND) &&
+                               (((TW + NX) * sizeof(float2)) % 128 == 0) &&
                                (GT % G::TPL == 0) && (GT % 32 == 0) && (W % 2 == 0) && (2 * W <= 256) &&
                                (HBUF % 2 == 0) && SMEM <= kPipeSmemMax && (GT == 32 || NG <= 14);
 };
