@@ -186,26 +186,28 @@ __device__ __forceinline__ void write_det_partials(const ColArgs& a, int b, int 
     }
 }
 
-// A thread's contribution to the detector sums from its E pixels of column iy, in the layout the
+// A thread's contribution to detector d's sum from its E pixels of column iy, in the layout the
 // last stage leaves (sum_square_over_Det, src/cgpu_fcns.cuh:1796-1814): |psi_hat|^2 where
-// g2_min <= |g|^2 < g2_max (rings), or weighted by each sensitivity map (matrix detectors).
+// g2_min <= |g|^2 < g2_max (rings), or weighted by the detector's sensitivity map (matrix
+// detectors). One detector at a time keeps one FP64 accumulator live; the pixels are added in the
+// same order for every detector.
 template <int NX>
-__device__ __forceinline__ void det_pixels(const ColArgs& a, const float2 (&x)[LineGeom<NX>::E], int t, int iy,
-                                           double* acc) {
+__device__ __forceinline__ double det_pixels(const ColArgs& a, const float2 (&x)[LineGeom<NX>::E], int t, int iy,
+                                             int d) {
     using G = LineGeom<NX>;
+    double acc = 0.0;
     if (a.det_mat) {
         const size_t nxy = (size_t)a.g.nx * a.g.ny;
+        const float* m = a.det_mat + (size_t)d * nxy + iy;
 #pragma unroll
         for (int i = 0; i < G::E; i++) {
             const int ix = reg_pos<NX, G::RL>(i, t);
             const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
-            const float* m = a.det_mat + (size_t)ix * a.g.ny + iy;
-#pragma unroll
-            for (int d = 0; d < kMaxDet; d++)
-                if (d < a.n_det) acc[d] += (double)__fmul_rn(__ldg(m + d * nxy), v2);
+            acc += (double)__fmul_rn(__ldg(m + (size_t)ix * a.g.ny), v2);
         }
-        return;
+        return acc;
     }
+    const float g2_min = a.det_g2_min[d], g2_max = a.det_g2_max[d];
     const float gy = __fsub_rn(__fmul_rn((float)ig_shift(iy, a.g.nyh, a.g.ny), a.g.dgy), 0.0f);
     const float gy2 = __fmul_rn(gy, gy);
 #pragma unroll
@@ -214,10 +216,9 @@ __device__ __forceinline__ void det_pixels(const ColArgs& a, const float2 (&x)[L
         const float gx = __fmul_rn((float)ig_shift(ix, a.g.nxh, a.g.nx), a.g.dgx);
         const float g2 = __fadd_rn(__fmul_rn(gx, gx), gy2);
         const float v2 = __fadd_rn(__fmul_rn(x[i].x, x[i].x), __fmul_rn(x[i].y, x[i].y));
-#pragma unroll
-        for (int d = 0; d < kMaxDet; d++)
-            if (d < a.n_det && a.det_g2_min[d] <= g2 && g2 < a.det_g2_max[d]) acc[d] += (double)v2;
+        if (g2_min <= g2 && g2 < g2_max) acc += (double)v2;
     }
+    return acc;
 }
 
 // Coherent part of STEM (Output_Multislice::add_scale_psi_coh, src/output_multislice.hpp:770-780):
@@ -303,15 +304,11 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
             }
         }
         if constexpr (DET) {
-            double acc[kMaxDet];
-#pragma unroll
-            for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
-            det_pixels<NX>(a, x, t, iy, acc);
             if (a.coh) coh_add<NX>(a, b, x, t, iy);
             // deterministic block reduction: warp shuffles, then warps in order
-#pragma unroll
-            for (int d = 0; d < kMaxDet; d++) {
-                double v = acc[d];
+#pragma unroll 1
+            for (int d = 0; d < a.n_det; d++) {
+                double v = det_pixels<NX>(a, x, t, iy, d);
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
                 if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5][d] = v;
             }
@@ -716,15 +713,11 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
             }
         }
         if constexpr (DET) {
-            double acc[kMaxDet];
-#pragma unroll
-            for (int d = 0; d < kMaxDet; d++) acc[d] = 0.0;
-            det_pixels<NX>(a, x, t, iy, acc);
             if (a.coh) coh_add<NX>(a, b, x, t, iy);
             // deterministic group reduction: warp shuffles, then the group's warps in order
-#pragma unroll
-            for (int d = 0; d < kMaxDet; d++) {
-                double v = acc[d];
+#pragma unroll 1
+            for (int d = 0; d < a.n_det; d++) {
+                double v = det_pixels<NX>(a, x, t, iy, d);
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
                 if ((gtid & 31) == 0) s_red[grp][gtid >> 5][d] = v;
             }
