@@ -39,6 +39,24 @@ struct LineGeom {
     static constexpr int TW_F = TwTable<N, true, 0>::SIZE + TwTable<N, true, 1>::SIZE + (NSG > 2 ? TwTable<N, true, 2>::SIZE : 0);
 };
 
+// Line stride of the column passes' full exchange buffers. A warp's lanes hold W adjacent columns
+// (lines) and 32/W consecutive line threads, and an 8-byte shared access is served one half-warp
+// (16 lanes, one 128-byte wavefront) at a time: its 16 lanes hold W lines x 16/W threads. The
+// exchanges address consecutive threads' points 1 mod 16 points apart, so the lines' starts must step
+// by 16/W points mod 16 for a half-warp to hit the 16 8-byte bank slots once each. The padded line
+// of LineGeom (1 mod 16) does that for W = 16; for 8-column tiles of 1024-point lines it conflicted
+// 2-way per half-warp, for 4- and 2-column tiles up to 4-way.
+template <int NX, int W>
+constexpr int col_ls() {
+    constexpr int base = LineGeom<NX>::LS;
+    if constexpr (W > 8) {
+        return base;
+    } else {
+        constexpr int r = (16 / W) % 16;
+        return base + ((r - base % 16) % 16 + 16) % 16;
+    }
+}
+
 template <int N>
 __device__ __forceinline__ void setup_twiddles(float2* base, const float2** twI, const float2** twF) {
     constexpr int NSG = LinePlan<N>::NS;
@@ -270,7 +288,7 @@ __global__ void __launch_bounds__(LineGeom<NX>::THREADS, LinePlan<NX>::B) cols_k
     __syncthreads();
 
     const int c = threadIdx.x % W, t = threadIdx.x / W;
-    float2* buf = lines + c * G::LS;
+    float2* buf = lines + c * col_ls<NX, W>();
     const int ldy = LDY ? LDY : a.ny;
     const int tiles = ldy / W;
     const int items = tiles * a.nprobe;
@@ -335,7 +353,7 @@ template <int NX, int FLAGS>
 static size_t cols_smem() {
     using G = LineGeom<NX>;
     constexpr bool PROP = FLAGS & COL_PROP;
-    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + (PROP ? NX : 0) + G::LPC * G::LS);
+    return sizeof(float2) * (size_t)(G::TW_I + G::TW_F + (PROP ? NX : 0) + G::LPC * col_ls<NX, G::LPC>());
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -594,10 +612,10 @@ struct ColPipe {
     static constexpr int PM_V = PM;
     static constexpr bool EARLY = PM != 0;
     static constexpr int W = GT / G::TPL;
-    static constexpr int LSH = PM == 1 ? HalfLineSmem<NX>::value : G::LS;  // exchange buffer per column
+    static constexpr int LSH = PM == 1 ? HalfLineSmem<NX>::value : col_ls<NX, W>();  // exchange buffer per column
     static constexpr size_t TW = (size_t)G::TW_I + G::TW_F;
     static constexpr size_t LAND0 = (size_t)W * NX;
-    static constexpr size_t LAND1 = EARLY ? LAND0 : ((size_t)W * G::LS > LAND0 ? (size_t)W * G::LS : LAND0);
+    static constexpr size_t LAND1 = EARLY ? LAND0 : ((size_t)W * LSH > LAND0 ? (size_t)W * LSH : LAND0);
     static constexpr size_t LAND = (LAND1 + 15) / 16 * 16;  // slots on 128-byte boundaries (bulk-copy targets)
     static constexpr size_t HBUF = EARLY ? (size_t)W * LSH : 0;
     static constexpr size_t SMEM = sizeof(float2) * (TW + NX + NG * LAND + NG * HBUF);
@@ -650,7 +668,7 @@ __global__ void __launch_bounds__(GT * NG, 1) cols_pipe_kernel(ColArgs a, const 
     const int grp = threadIdx.x / GT, gtid = threadIdx.x % GT;
     const int c = gtid % W, t = gtid / W;
     float2* land = land0 + grp * P::LAND;
-    float2* buf = EARLY ? land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH : land + (size_t)c * G::LS;
+    float2* buf = EARLY ? land0 + NG * P::LAND + grp * P::HBUF + (size_t)c * P::LSH : land + (size_t)c * P::LSH;
     (void)HALF;
     if constexpr (PROP) {
         for (int i = threadIdx.x; i < NX; i += blockDim.x) s_px[i] = a.Px[i];
