@@ -10,12 +10,16 @@
 //     remaining prime factor; twiddles computed in double and rounded once to the working type;
 //     unnormalised in both directions, sign convention exp(sign * 2*pi*i*j*k/n) as in FFTW.
 //   * 2-D/batched transforms: rows (contiguous) then columns (gathered in blocks of 16 into a
-//     contiguous scratch buffer), each split over std::threads (plan_with_nthreads).
+//     contiguous scratch buffer), each split over plan_with_nthreads threads of one persistent
+//     worker pool (started on first use, as FFTW's threads are, rather than per execute).
 //
 // Wisdom calls are accepted and do nothing. Nothing in the product links this file; it exists
 // only so that oracle/_ref can be compiled from the reference sources.
 #include <cmath>
 #include <complex>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
@@ -25,6 +29,61 @@
 namespace {
 
 int g_nthreads = 1;
+
+// Persistent workers: run(n, f) calls f(0) on the caller and f(1..n-1) on workers, and returns when
+// all are done. One parallel region at a time (callers from several threads take turns).
+class Pool {
+public:
+    void run(int n, const std::function<void(int)>& f) {
+        std::lock_guard<std::mutex> call(call_mu_);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            while ((int)th_.size() < n - 1) {
+                const int id = (int)th_.size() + 1;
+                th_.emplace_back([this, id] { loop(id); });
+            }
+            task_ = &f;
+            active_ = n;
+            pending_ = n - 1;
+            ++gen_;
+        }
+        start_.notify_all();
+        f(0);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+        task_ = nullptr;
+    }
+
+private:
+    void loop(int id) {
+        unsigned long seen = 0;
+        for (;;) {
+            const std::function<void(int)>* t = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                start_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (id >= active_) continue;
+                t = task_;
+            }
+            (*t)(id);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::mutex call_mu_, mu_;
+    std::condition_variable start_, done_;
+    std::vector<std::thread> th_;
+    const std::function<void(int)>* task_ = nullptr;
+    int active_ = 0, pending_ = 0;
+    unsigned long gen_ = 0;
+};
+
+// never destroyed: the workers live until the process exits, like FFTW's
+Pool& pool() {
+    static Pool* p = new Pool();
+    return *p;
+}
 
 template <class T>
 struct Fft1d {
@@ -143,14 +202,11 @@ struct Plan {
     void parallel(int count, F fn) const {
         int nt = std::max(1, std::min(nthreads, count));
         if (nt == 1) { fn(0, count); return; }
-        std::vector<std::thread> th;
-        int chunk = (count + nt - 1) / nt;
-        for (int t = 0; t < nt; ++t) {
-            int b = t * chunk, e = std::min(count, b + chunk);
-            if (b >= e) break;
-            th.emplace_back([=] { fn(b, e); });
-        }
-        for (auto& x : th) x.join();
+        const int chunk = (count + nt - 1) / nt;
+        pool().run(nt, [&](int t) {
+            const int b = t * chunk, e = std::min(count, b + chunk);
+            if (b < e) fn(b, e);
+        });
     }
 
     void exec_one(C* d) const {
